@@ -1,0 +1,337 @@
+#!/usr/bin/env python
+"""Benchmark of the HYOWON PM step (particle-mesh force + KDK update) on B200.
+
+Workload (default): the 512^3-particle / 1024^3-mesh configuration, L = 1000
+Mpc/h, flat LCDM (Om 0.3, OL 0.7), 1LPT at z = 49 from seeded white noise
+(seed 7) shaped by a BBKS spectrum with sigma_8 = 0.8, steps uniform in ln a
+(64 steps to z = 0). A "step" is one KDK step (one force evaluation). Synthetic
+inputs: no public dataset is involved.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp64|fp32]
+                    [--config c1|c2|c3] [--impl ours|reference]
+
+Prints one JSON line (rank 0). `value` = particle-steps/s over the K timed steps
+with the state resident in HBM, timed with CUDA events on the library's stream
+(max over ranks); `e2e` = the same metric through the public C ABI with host
+buffers: upload of the IC state from pinned host memory, K calls of
+hyowon_pm_kdk_step (host scalars in, max-drift read back), download of the final
+state, all inside the timed region. Multi-GPU runs are independent replicas
+(the PM step does not shard across GPUs in this build).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def setup_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def algorithmic_bytes(form, n_particles, n_mesh):
+    """Algorithmic HBM bytes of one KDK step (particles sorted, gather reading
+    the mesh once, Green's function fused between the transforms):
+    B = Np (9 bx + 6 bp) + Ng^3 (b_dep + [b_dep + b_fft if the int->float
+    conversion is its own pass] + 5 b_fft)."""
+    G = n_mesh ** 3
+    if form == "fp64":
+        return n_particles * (9 * 8 + 6 * 8) + G * (8 + 5 * 8)
+    return n_particles * (9 * 4 + 6 * 4) + G * (8 + (8 + 4) + 5 * 4)
+
+
+def gather_bytes(form, n_particles, n_mesh):
+    """Algorithmic bytes of one gather + K2 launch: positions and momenta read,
+    momenta and accelerations written, the potential mesh read once."""
+    bx = 8 if form == "fp64" else 4
+    bp = 8 if form == "fp64" else 4
+    return n_particles * (3 * bx + 3 * bp + 3 * bp + 3 * bp) + n_mesh ** 3 * bx
+
+
+def run_reference(args, world, rank):
+    """The reference's own CPU implementation (oracle/_ref) on the host cores."""
+    if rank != 0:
+        return
+    from hyowon_b200 import ic
+    from oracle.bindings import Reference
+    from oracle.lpt_oracle import lpt_ics
+    cfg_name = args.config
+    c = ic.CONFIGS[cfg_name]
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    ref = Reference()
+    a0, dl = ic.config_schedule(cfg_name)
+    # Bounded sample of the workload: the first steps of the schedule; the c3
+    # workload (31 GB of host RAM in the reference) is sampled one step at a time.
+    n_side = c["n_side"]
+    noise = ic.white_noise(n_side, c["seed"])
+    st = lpt_ics(noise, n_side, c["box"], a0)
+    for k in ("ax", "ay", "az"):
+        st[k] = np.zeros_like(st["x"])
+    m_p = ic.particle_mass(c["box"], n_side)
+    steps = max(1, min(args.steps, 2 if cfg_name == "c3" else args.steps))
+    _, secs = ref.kdk_run(c["box"], c["mesh"], st, a0, 1.0, dl, steps, m_p)
+    value = n_side ** 3 * steps / secs
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": value,
+        "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": steps, "warmup": 0,
+        "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg_name, "particles": n_side ** 3, "mesh": c["mesh"],
+                   "box": c["box"]},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{steps} KDK step(s) of {cfg_name} after the initial force"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(cfg_name):
+    """Times the reference (oracle/_ref) on a bounded sample: KDK steps of the
+    c2-sized problem when the full configuration would exceed ~30 s."""
+    try:
+        from hyowon_b200 import ic
+        from oracle.bindings import Reference
+        from oracle.lpt_oracle import lpt_ics
+        ref = Reference()
+    except Exception as e:  # pragma: no cover
+        return {"value": None, "unit": "particle-steps/s", "cores": os.cpu_count(),
+                "kind": "reference", "sample": f"unavailable: {e}"}
+    name = "c2" if cfg_name == "c3" else cfg_name
+    c = ic.CONFIGS[name]
+    a0, dl = ic.config_schedule(name)
+    st = lpt_ics(ic.white_noise(c["n_side"], c["seed"]), c["n_side"], c["box"], a0)
+    for k in ("ax", "ay", "az"):
+        st[k] = np.zeros_like(st["x"])
+    steps = 3 if name == "c2" else 8
+    _, secs = ref.kdk_run(c["box"], c["mesh"], st, a0, 1.0, dl, steps,
+                          ic.particle_mass(c["box"], c["n_side"]))
+    return {"value": c["n_side"] ** 3 * steps / secs, "unit": "particle-steps/s",
+            "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"{steps} KDK steps of {name} ({c['n_side']}^3 particles, "
+                      f"{c['mesh']}^3 mesh) on all host threads"}
+
+
+def main():
+    args = parse()
+    world, rank, local = setup_dist()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import hyowon_b200 as hb
+    from hyowon_b200 import ic
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", ""))
+
+    c = ic.CONFIGS[args.config]
+    n_side, N, L = c["n_side"], c["mesh"], c["box"]
+    n = n_side ** 3
+    a0, dl = ic.config_schedule(args.config)
+    stepper = hb.TimeStepper(a0, 1.0, dl)
+    K1, D, K2 = stepper.factors()
+    total_steps = args.warmup + args.steps
+    if total_steps > K1.size:
+        reps = math.ceil(total_steps / K1.size)
+        K1, D, K2 = np.tile(K1, reps), np.tile(D, reps), np.tile(K2, reps)
+    m_p = ic.particle_mass(L, n_side)
+    noise = ic.white_noise(n_side, c["seed"] + rank)
+
+    solver = hb.PMSolver(hb.MeshGeometry(L, N), hb.PMForceMethod.pure_pm(False), args.form)
+    ic.lpt_on_device(solver, noise, n_side, a0, m_p)
+    ics = solver.download(acc=False) if not args.no_e2e else None
+    solver.solve_forces()
+    solver.set_timing(True)
+
+    # -- device-resident throughput -------------------------------------------
+    solver.run(K1[:args.warmup], D[:args.warmup], K2[:args.warmup])
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        solver.run(K1[args.warmup:total_steps], D[args.warmup:total_steps],
+                   K2[args.warmup:total_steps])
+        wall = time.perf_counter() - t0
+    timing = solver.last_timing()
+    dev_ms = timing["total"]
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([dev_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    ms_per_step = dev_ms / args.steps
+    value = world * n * args.steps / (dev_ms * 1e-3)
+
+    # per-phase times of the last timed step (CUDA events on the library stream)
+    phases = {k: timing[k] for k in ("sort", "deposit", "fft_forward", "green", "fft_inverse",
+                                     "gather")}
+    launches = int(timing["launches"])
+
+    # -- roofline of the dominant kernel of ours: the gather + K2 ---------------
+    hbm, peak_kind = peaks()
+    gb = gather_bytes(args.form, n, N)
+    achieved = gb / (phases["gather"] * 1e-3) / 1e9 if phases["gather"] > 0 else None
+    roofline = {"bound": "hbm", "kernel": "gather_kick", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
+                "traffic": None, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": gb}
+    step_bytes = algorithmic_bytes(args.form, n, N)
+    step_roofline = {"algorithmic_bytes_per_step": step_bytes,
+                     "achieved_GBs": step_bytes / (ms_per_step * 1e-3) / 1e9,
+                     "frac": step_bytes / (ms_per_step * 1e-3) / 1e9 / hbm}
+
+    # -- end to end through the C ABI with host buffers -------------------------
+    e2e = None
+    if not args.no_e2e:
+        import torch
+        pinned = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+                  for k in ("x", "y", "z", "px", "py", "pz", "ax", "ay", "az")}
+        for k in ("x", "y", "z", "px", "py", "pz"):
+            pinned[k][:] = ics[k]
+        e2e_solver = solver
+        t0 = time.perf_counter()
+        e2e_solver.upload(pinned["x"], pinned["y"], pinned["z"], pinned["px"], pinned["py"],
+                          pinned["pz"], uniform_mass=m_p)
+        for s in range(args.steps):
+            e2e_solver.kdk_step(K1[s], D[s], K2[s])
+        out = e2e_solver.download()
+        e2e_secs = time.perf_counter() - t0
+        h2d = 6 * 8 * n
+        d2h = 9 * 8 * n + 8 * args.steps
+        e2e = {"value": world * n * args.steps / e2e_secs, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": h2d / args.steps + 24,
+               "d2h_bytes_per_step": d2h / args.steps,
+               "note": "upload IC state + K kdk_step calls + download final state"}
+        del out
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args.config)
+
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+i64",
+            "data": "synthetic",
+            "config": {"workload": args.config, "form": args.form, "particles": n, "mesh": N,
+                       "box": L, "z_start": c["z_start"], "seed": c["seed"],
+                       "l2": "inputs larger than L2 (meshes and particle arrays >> 126 MB)",
+                       "parallelism": f"replicas{world}"},
+            "phases_ms_last_step": phases,
+            "roofline": roofline,
+            "step_roofline": step_roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "wall_s_timed_region": wall,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,54 @@
+// pm_fp32.h -- the precision form of the PM step (internal interface).
+//
+// Positions are 32-bit periodic fixed-point lattice coordinates u, with
+// x = u * L / 2^32; the cell of u on an N mesh is floor(u*N / 2^32) and its CIC
+// fraction the low 32 bits of u*N. Mass is deposited as int64 fixed-point
+// offsets from the mean cell mass (deterministic integer atomics), converted to
+// FP32 for the R2C transform; the Green's multiply, C2R and gather run in FP32;
+// momenta are FP32; the drift p*D is formed in FP64 and rounded once into the
+// fixed-point position.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+struct hyowon_pm_s;
+
+namespace hyowon {
+
+int status_or_cuda(hyowon_pm_s* h, int rc);
+
+namespace fp32 {
+
+struct State;
+
+int create(State** out, double L, int N, int method, int deconvolve, double r_s,
+           const double* lap, const double* win, double four_pi_G, cudaStream_t s);
+void destroy(State* st);
+const std::string& last_error(State* st);
+
+int upload(State* st, uint32_t n, const double* x, const double* y, const double* z,
+           const double* px, const double* py, const double* pz, const double* masses,
+           double uniform_mass, double total_mass, double mass_tol, cudaStream_t s);
+// Same as upload from device-resident binary64 arrays (LPT initial conditions).
+int upload_device(State* st, uint32_t n, double* const pos[3], double* const mom[3],
+                  double uniform_mass, double total_mass, double mass_tol, cudaStream_t s);
+void validate(State* st, cudaStream_t s, unsigned int* d_status);
+int sort_current(State* st, cudaStream_t s, unsigned int* d_status);
+int enqueue_force(State* st, cudaStream_t s, unsigned int* d_status, bool kick, double K2,
+                  cudaEvent_t* ev);
+int kdk_step(State* st, cudaStream_t s, unsigned int* d_status,
+             unsigned long long* d_maxdrift, double K1, double D, double K2,
+             cudaEvent_t* ev);
+// Host bookkeeping after a kdk_step: `published` when the drift was published,
+// `ok` when the whole step succeeded.
+void commit_step(State* st, bool published, bool ok);
+int download(State* st, cudaStream_t s, double* x, double* y, double* z, double* px,
+             double* py, double* pz, double* ax, double* ay, double* az);
+int download_potential(State* st, cudaStream_t s, double* phi);
+int download_mass_mesh(State* st, cudaStream_t s, unsigned int* d_status, double* mesh);
+
+}  // namespace fp32
+}  // namespace hyowon

@@ -1,0 +1,523 @@
+// pm_fp64.cu -- binary64 PM kernels: cell key, K1 kick + drift, CIC deposit,
+// Green's function, centred-gradient gather fused with the K2 kick.
+//
+// Compiled with --fmad=false: every product and sum below rounds exactly as
+// the reference's -ffp-contract=off build does, in the reference's operation
+// order (cited per kernel). Summation across particles (the deposit) uses
+// atomics and therefore differs from the reference's plane-ordered sum only in
+// rounding.
+#include <cuda_runtime.h>
+
+#include "pm_kernels.h"
+
+namespace hyowon {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned blocks_for(uint64_t n, int threads = kThreads) {
+    return static_cast<unsigned>((n + threads - 1) / threads);
+}
+
+__device__ __forceinline__ uint32_t cell_index(int ix, int iy, int iz, int N) {
+    return (static_cast<uint32_t>(ix) * static_cast<uint32_t>(N) + static_cast<uint32_t>(iy))
+               * static_cast<uint32_t>(N)
+        + static_cast<uint32_t>(iz);
+}
+
+__global__ void k_validate_inputs(uint32_t n, const double* __restrict__ x,
+                                  const double* __restrict__ y,
+                                  const double* __restrict__ z,
+                                  const double* __restrict__ mass,
+                                  unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool bad = !isfinite(x[i]) || !isfinite(y[i]) || !isfinite(z[i]);
+    if (mass) bad |= !isfinite(mass[i]) || mass[i] < 0.0;
+    if (bad) raise_status(status, ST_NONFINITE_INPUT);
+}
+
+// Cell key + bucket rank for the current positions.
+__global__ void k_key(uint32_t n, const double* __restrict__ x, const double* __restrict__ y,
+                      const double* __restrict__ z, Axis a, uint32_t* __restrict__ key,
+                      uint32_t* __restrict__ rank, uint32_t* __restrict__ count, int shift,
+                      unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int bx, by, bz;
+    double fx, fy, fz;
+    const bool ok = cic_coord_f64(x[i], a, bx, fx) & cic_coord_f64(y[i], a, by, fy)
+        & cic_coord_f64(z[i], a, bz, fz);
+    if (!ok) {
+        raise_status(status, isfinite(x[i]) && isfinite(y[i]) && isfinite(z[i])
+                                 ? ST_CELL_ESCAPE
+                                 : ST_NONFINITE_INPUT);
+        bx = by = bz = 0;
+    }
+    const uint32_t b = cell_index(bx, by, bz, a.N) >> shift;
+    key[i] = b;
+    rank[i] = atomicAdd(&count[b], 1u);
+}
+
+// K1 kick + drift (particle_update.hpp:20-116, leapfrog_integrator.cpp:170-225)
+// writing the candidate state, its sort key and the drift telemetry.
+__global__ void k_kick_drift_key(uint32_t n, const double* __restrict__ x,
+                                 const double* __restrict__ y, const double* __restrict__ z,
+                                 const double* __restrict__ px, const double* __restrict__ py,
+                                 const double* __restrict__ pz, const double* __restrict__ ax,
+                                 const double* __restrict__ ay, const double* __restrict__ az,
+                                 double K1, double D, Axis a, double* __restrict__ xo,
+                                 double* __restrict__ yo, double* __restrict__ zo,
+                                 double* __restrict__ pxo, double* __restrict__ pyo,
+                                 double* __restrict__ pzo, uint32_t* __restrict__ key,
+                                 uint32_t* __restrict__ rank, uint32_t* __restrict__ count,
+                                 int shift, unsigned long long* max_drift_bits,
+                                 unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double drift_norm = 0.0;
+    if (i < n) {
+        const double qx = px[i] + ax[i] * K1;
+        const double qy = py[i] + ay[i] * K1;
+        const double qz = pz[i] + az[i] * K1;
+        const double dx = qx * D;
+        const double dy = qy * D;
+        const double dz = qz * D;
+        // add_periodic_displacement: wrap(wrap(x) + minimum_image(d)).
+        const double nx = wrap_f64(wrap_f64(x[i], a.L) + minimum_image_f64(dx, a.L), a.L);
+        const double ny = wrap_f64(wrap_f64(y[i], a.L) + minimum_image_f64(dy, a.L), a.L);
+        const double nz = wrap_f64(wrap_f64(z[i], a.L) + minimum_image_f64(dz, a.L), a.L);
+        bool ok = isfinite(qx) && isfinite(qy) && isfinite(qz) && isfinite(dx)
+            && isfinite(dy) && isfinite(dz) && isfinite(nx) && isfinite(ny) && isfinite(nz);
+        int bx = 0, by = 0, bz = 0;
+        if (ok) {
+            double fx, fy, fz;
+            if (!(cic_coord_f64(nx, a, bx, fx) & cic_coord_f64(ny, a, by, fy)
+                  & cic_coord_f64(nz, a, bz, fz))) {
+                raise_status(status, ST_CELL_ESCAPE);
+                bx = by = bz = 0;
+            }
+            drift_norm = hypot(hypot(D * qx, D * qy), D * qz);
+        } else {
+            raise_status(status, ST_KICK_DRIFT);
+        }
+        xo[i] = nx;
+        yo[i] = ny;
+        zo[i] = nz;
+        pxo[i] = qx;
+        pyo[i] = qy;
+        pzo[i] = qz;
+        const uint32_t b = cell_index(bx, by, bz, a.N) >> shift;
+        key[i] = b;
+        rank[i] = atomicAdd(&count[b], 1u);
+    }
+    // Non-negative doubles order like their bit patterns.
+    unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(drift_norm));
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+        bits = other > bits ? other : bits;
+    }
+    if ((threadIdx.x & 31) == 0 && bits != 0ull) atomicMax(max_drift_bits, bits);
+}
+
+// CIC deposit (src/mesh/mass_assignment_deposit.inc:193-240): each particle adds
+// mass*wx*wy*wz (that product order) to its 8 cells.
+__global__ void k_deposit(uint32_t n, const double* __restrict__ x,
+                          const double* __restrict__ y, const double* __restrict__ z,
+                          const double* __restrict__ mass, double uniform_mass, Axis a,
+                          double* __restrict__ mesh, unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+    int ix, iy, iz;
+    double tx, ty, tz;
+    if (!(cic_coord_f64(x[i], a, ix, tx) & cic_coord_f64(y[i], a, iy, ty)
+          & cic_coord_f64(z[i], a, iz, tz))) {
+        raise_status(status, ST_CELL_ESCAPE);
+        return;
+    }
+    const double m = mass ? mass[i] : uniform_mass;
+    const double wx[2] = {1.0 - tx, tx};
+    const double wy[2] = {1.0 - ty, ty};
+    const double wz[2] = {1.0 - tz, tz};
+    const int N = a.N;
+    const int gy[2] = {iy, iy + 1 == N ? 0 : iy + 1};
+    const int gz[2] = {iz, iz + 1 == N ? 0 : iz + 1};
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox) {
+        const int gx = ox == 0 ? ix : (ix + 1 == N ? 0 : ix + 1);
+        const double mx = m * wx[ox];
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy) {
+            const double mxy = mx * wy[oy];
+#pragma unroll
+            for (int oz = 0; oz < 2; ++oz) {
+                atomicAdd(&mesh[cell_index(gx, gy[oy], gz[oz], N)], mxy * wz[oz]);
+            }
+        }
+    }
+}
+
+// Pure-PM Green's function (src/mesh/green_function.cpp:165-207) applied to the
+// r2c of the mass mesh. `scale` folds in the density normalisation 1/dx^3 and
+// the 1/N^3 of the inverse transform; the mean subtraction of
+// DensityNormalization only changes the k=0 mode, which the kernel zeroes. The
+// k=0 thread also checks CIC mass conservation against the reference bound
+// (src/math/cic_mass_conservation.cpp:26-59): Re(delta_0) is the mesh mass.
+__global__ void k_green(int N, double2* __restrict__ modes, const double* __restrict__ lap,
+                        const double* __restrict__ win, double four_pi_G, double scale,
+                        int deconvolve, double input_mass, double mass_tolerance,
+                        unsigned int* status) {
+    const int Hz = N / 2 + 1;
+    const uint64_t total = static_cast<uint64_t>(N) * N * Hz;
+    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int iz = static_cast<int>(idx % Hz);
+    const uint64_t t = idx / Hz;
+    const int iy = static_cast<int>(t % N);
+    const int ix = static_cast<int>(t / N);
+    double2 v = modes[idx];
+    if (idx == 0) {
+        const double deposited = v.x;
+        if (!(fabs(deposited - input_mass) <= mass_tolerance)) raise_status(status, ST_MASS);
+        modes[0] = make_double2(0.0, 0.0);
+        return;
+    }
+    const double Dk = lap[ix] + lap[iy] + lap[iz];
+    double f = four_pi_G / Dk;
+    if (deconvolve) {
+        const double wt = win[ix] * win[iy] * win[iz];
+        f /= (wt * wt);
+    }
+    f *= scale;
+    v.x *= f;
+    v.y *= f;
+    modes[idx] = v;
+}
+
+// TreePM long-range Green's function (green_function.cpp:174-200):
+// 4 pi G/(-k^2) * exp(-k^2 r_s^2) / W^2, with the same folded scale.
+__global__ void k_green_spectral(int N, double L, double2* __restrict__ modes,
+                                 const double* __restrict__ win, double four_pi_G,
+                                 double scale, double r_s, double input_mass,
+                                 double mass_tolerance, unsigned int* status) {
+    const int Hz = N / 2 + 1;
+    const uint64_t total = static_cast<uint64_t>(N) * N * Hz;
+    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int iz = static_cast<int>(idx % Hz);
+    const uint64_t t = idx / Hz;
+    const int iy = static_cast<int>(t % N);
+    const int ix = static_cast<int>(t / N);
+    double2 v = modes[idx];
+    if (idx == 0) {
+        if (!(fabs(v.x - input_mass) <= mass_tolerance)) raise_status(status, ST_MASS);
+        modes[0] = make_double2(0.0, 0.0);
+        return;
+    }
+    const double two_pi = 2.0 * 3.141592653589793;
+    const int mx = ix <= N / 2 ? ix : ix - N;
+    const int my = iy <= N / 2 ? iy : iy - N;
+    const int mz = iz <= N / 2 ? iz : iz - N;
+    const double kx = two_pi * static_cast<double>(mx) / L;
+    const double ky = two_pi * static_cast<double>(my) / L;
+    const double kz = two_pi * static_cast<double>(mz) / L;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    double f = four_pi_G / (-k2);
+    f *= exp(-k2 * r_s * r_s);
+    const double wt = win[ix] * win[iy] * win[iz];
+    f /= (wt * wt);
+    f *= scale;
+    v.x *= f;
+    v.y *= f;
+    modes[idx] = v;
+}
+
+// out_k = -i k_axis phi_k with the Nyquist component zeroed
+// (src/gravity/pm_solver.cpp:775-797).
+__global__ void k_spectral_axis(int N, double L, int axis, const double2* __restrict__ phi,
+                                double2* __restrict__ out) {
+    const int Hz = N / 2 + 1;
+    const uint64_t total = static_cast<uint64_t>(N) * N * Hz;
+    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int iz = static_cast<int>(idx % Hz);
+    const uint64_t t = idx / Hz;
+    const int iy = static_cast<int>(t % N);
+    const int ix = static_cast<int>(t / N);
+    const int i = axis == 0 ? ix : (axis == 1 ? iy : iz);
+    double k = 0.0;
+    if (!(N % 2 == 0 && i == N / 2)) {
+        const int m = i <= N / 2 ? i : i - N;
+        k = 2.0 * 3.141592653589793 * static_cast<double>(m) / L;
+    }
+    const double2 p = phi[idx];
+    out[idx] = make_double2(p.y * k, -p.x * k);
+}
+
+// Plain CIC interpolation added to out (mass_assignment_gather.inc:402-450).
+__global__ void k_interp_add(uint32_t n, const double* __restrict__ field,
+                             const double* __restrict__ x, const double* __restrict__ y,
+                             const double* __restrict__ z, Axis a, double* __restrict__ out,
+                             unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+    int ix, iy, iz;
+    double tx, ty, tz;
+    if (!(cic_coord_f64(x[i], a, ix, tx) & cic_coord_f64(y[i], a, iy, ty)
+          & cic_coord_f64(z[i], a, iz, tz))) {
+        raise_status(status, ST_CELL_ESCAPE);
+        return;
+    }
+    const int N = a.N;
+    const double wx[2] = {1.0 - tx, tx};
+    const double wy[2] = {1.0 - ty, ty};
+    const double wz[2] = {1.0 - tz, tz};
+    double s = 0.0;
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox) {
+        const int gx = ox == 0 ? ix : (ix + 1 == N ? 0 : ix + 1);
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy) {
+            const int gy = oy == 0 ? iy : (iy + 1 == N ? 0 : iy + 1);
+#pragma unroll
+            for (int oz = 0; oz < 2; ++oz) {
+                const int gz = oz == 0 ? iz : (iz + 1 == N ? 0 : iz + 1);
+                const double w = wx[ox] * wy[oy] * wz[oz];
+                s += __ldg(&field[cell_index(gx, gy, gz, N)]) * w;
+            }
+        }
+    }
+    const double r = out[i] + s;
+    if (!isfinite(r)) raise_status(status, ST_FORCE);
+    out[i] = r;
+}
+
+// interpolate_centered_gradient3_add_full_mesh
+// (src/mesh/mass_assignment_gradient.cpp:117-206) into zeroed accelerations,
+// fused with the K2 kick (leapfrog_integrator.cpp:240-278). Loads the 32
+// distinct potential values of the 4x4x4 stencil footprint once.
+__global__ void __launch_bounds__(kThreads)
+k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restrict__ x,
+              const double* __restrict__ y, const double* __restrict__ z,
+              const double* __restrict__ px, const double* __restrict__ py,
+              const double* __restrict__ pz, double* __restrict__ ax,
+              double* __restrict__ ay, double* __restrict__ az, int do_kick, double K2,
+              double* __restrict__ pxo, double* __restrict__ pyo,
+              double* __restrict__ pzo, Axis a, unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+    int ix, iy, iz;
+    double tx, ty, tz;
+    if (!(cic_coord_f64(x[i], a, ix, tx) & cic_coord_f64(y[i], a, iy, ty)
+          & cic_coord_f64(z[i], a, iz, tz))) {
+        raise_status(status, ST_CELL_ESCAPE);
+        return;
+    }
+    const int N = a.N;
+    const int xs[4] = {ix == 0 ? N - 1 : ix - 1, ix, ix + 1 == N ? 0 : ix + 1,
+                       ix + 2 >= N ? ix + 2 - N : ix + 2};
+    const int ys[4] = {iy == 0 ? N - 1 : iy - 1, iy, iy + 1 == N ? 0 : iy + 1,
+                       iy + 2 >= N ? iy + 2 - N : iy + 2};
+    const int zs[4] = {iz == 0 ? N - 1 : iz - 1, iz, iz + 1 == N ? 0 : iz + 1,
+                       iz + 2 >= N ? iz + 2 - N : iz + 2};
+#define PHI(a_, b_, c_) __ldg(&phi[cell_index(xs[a_], ys[b_], zs[c_], N)])
+    double c[2][2][2], xm[2][2], xp[2][2], ym[2][2], yp[2][2], zm[2][2], zp[2][2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            xm[u][v] = PHI(0, u + 1, v + 1);
+            xp[u][v] = PHI(3, u + 1, v + 1);
+            ym[u][v] = PHI(u + 1, 0, v + 1);
+            yp[u][v] = PHI(u + 1, 3, v + 1);
+            zm[u][v] = PHI(u + 1, v + 1, 0);
+            zp[u][v] = PHI(u + 1, v + 1, 3);
+#pragma unroll
+            for (int w = 0; w < 2; ++w) c[u][v][w] = PHI(u + 1, v + 1, w + 1);
+        }
+    }
+#undef PHI
+    const double wx[2] = {1.0 - tx, tx};
+    const double wy[2] = {1.0 - ty, ty};
+    const double wz[2] = {1.0 - tz, tz};
+    const double two_dx = 2.0 * a.dx;
+    double gx_sum = 0.0, gy_sum = 0.0, gz_sum = 0.0;
+    bool lost = false;
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox) {
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy) {
+#pragma unroll
+            for (int oz = 0; oz < 2; ++oz) {
+                const double w = wx[ox] * wy[oy] * wz[oz];
+                const bool w_lost = wx[ox] != 0.0 && wy[oy] != 0.0 && wz[oz] != 0.0 && w == 0.0;
+                const double dxv = (ox == 0 ? c[1][oy][oz] : xp[oy][oz])
+                    - (ox == 0 ? xm[oy][oz] : c[0][oy][oz]);
+                const double dyv = (oy == 0 ? c[ox][1][oz] : yp[ox][oz])
+                    - (oy == 0 ? ym[ox][oz] : c[ox][0][oz]);
+                const double dzv = (oz == 0 ? c[ox][oy][1] : zp[ox][oy])
+                    - (oz == 0 ? zm[ox][oy] : c[ox][oy][0]);
+                const double gx = -dxv / two_dx;
+                const double gy = -dyv / two_dx;
+                const double gz = -dzv / two_dx;
+                const bool w_nonzero = w != 0.0 || w_lost;
+                lost |= w_nonzero
+                    && ((dxv != 0.0 && gx == 0.0) || (dyv != 0.0 && gy == 0.0)
+                        || (dzv != 0.0 && gz == 0.0));
+                lost |= w_lost && (gx != 0.0 || gy != 0.0 || gz != 0.0);
+                const double cx = w * gx;
+                const double cy = w * gy;
+                const double cz = w * gz;
+                lost |= w != 0.0
+                    && ((gx != 0.0 && cx == 0.0) || (gy != 0.0 && cy == 0.0)
+                        || (gz != 0.0 && cz == 0.0));
+                gx_sum += cx;
+                gy_sum += cy;
+                gz_sum += cz;
+            }
+        }
+    }
+    if (lost) raise_status(status, ST_UNDERFLOW);
+    // The evolution path adds into zeroed accelerations (leapfrog_integrator.cpp:75-83).
+    const double gax = 0.0 + gx_sum;
+    const double gay = 0.0 + gy_sum;
+    const double gaz = 0.0 + gz_sum;
+    if (!(isfinite(gax) && isfinite(gay) && isfinite(gaz))) raise_status(status, ST_FORCE);
+    ax[i] = gax;
+    ay[i] = gay;
+    az[i] = gaz;
+    if (do_kick) {
+        const double qx = px[i] + gax * K2;
+        const double qy = py[i] + gay * K2;
+        const double qz = pz[i] + gaz * K2;
+        if (!(isfinite(qx) && isfinite(qy) && isfinite(qz))) raise_status(status, ST_KICK2);
+        pxo[i] = qx;
+        pyo[i] = qy;
+        pzo[i] = qz;
+    }
+}
+
+// K2 kick alone, for force paths that do not end in the fused gather.
+__global__ void k_kick_only(uint32_t n, const double* __restrict__ px,
+                            const double* __restrict__ py, const double* __restrict__ pz,
+                            const double* __restrict__ ax, const double* __restrict__ ay,
+                            const double* __restrict__ az, double K2,
+                            double* __restrict__ pxo, double* __restrict__ pyo,
+                            double* __restrict__ pzo, unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+    const double qx = px[i] + ax[i] * K2;
+    const double qy = py[i] + ay[i] * K2;
+    const double qz = pz[i] + az[i] * K2;
+    if (!(isfinite(qx) && isfinite(qy) && isfinite(qz))) raise_status(status, ST_KICK2);
+    pxo[i] = qx;
+    pyo[i] = qy;
+    pzo[i] = qz;
+}
+
+__global__ void k_cell_coords(uint32_t n, const double* __restrict__ pos, Axis a,
+                              int64_t* __restrict__ base, double* __restrict__ frac,
+                              unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int b = -1;
+    double f = 0.0;
+    if (!cic_coord_f64(pos[i], a, b, f)) {
+        raise_status(status, ST_CELL_ESCAPE);
+        b = -1;
+    }
+    base[i] = b;
+    frac[i] = f;
+}
+
+}  // namespace
+
+void launch_validate_inputs_f64(uint32_t n, const double* x, const double* y,
+                                const double* z, const double* mass, unsigned int* status,
+                                cudaStream_t s) {
+    if (n == 0) return;
+    k_validate_inputs<<<blocks_for(n), kThreads, 0, s>>>(n, x, y, z, mass, status);
+}
+
+void launch_key_f64(uint32_t n, const ParticlesF64& p, Axis a, const SortWork& w,
+                    unsigned int* status, cudaStream_t s) {
+    if (n == 0) return;
+    k_key<<<blocks_for(n), kThreads, 0, s>>>(n, p.x, p.y, p.z, a, w.key, w.rank, w.count,
+                                             w.shift, status);
+}
+
+void launch_kick_drift_key_f64(uint32_t n, const ParticlesF64& cur, const double* ax,
+                               const double* ay, const double* az, double K1, double D,
+                               Axis a, const ParticlesF64& cand, const SortWork& w,
+                               unsigned long long* max_drift_bits, unsigned int* status,
+                               cudaStream_t s) {
+    if (n == 0) return;
+    k_kick_drift_key<<<blocks_for(n), kThreads, 0, s>>>(
+        n, cur.x, cur.y, cur.z, cur.px, cur.py, cur.pz, ax, ay, az, K1, D, a, cand.x, cand.y,
+        cand.z, cand.px, cand.py, cand.pz, w.key, w.rank, w.count, w.shift, max_drift_bits,
+        status);
+}
+
+void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,
+                        double uniform_mass, Axis a, double* mesh, unsigned int* status,
+                        cudaStream_t s) {
+    if (n == 0) return;
+    k_deposit<<<blocks_for(n), kThreads, 0, s>>>(n, p.x, p.y, p.z, mass, uniform_mass, a,
+                                                 mesh, status);
+}
+
+void launch_green_f64(int N, double2* modes, const double* lap, const double* win,
+                      double four_pi_G, double scale, int deconvolve, double input_mass,
+                      double mass_tolerance, unsigned int* status, cudaStream_t s) {
+    const uint64_t total = static_cast<uint64_t>(N) * N * (N / 2 + 1);
+    k_green<<<blocks_for(total), kThreads, 0, s>>>(N, modes, lap, win, four_pi_G, scale,
+                                                   deconvolve, input_mass, mass_tolerance,
+                                                   status);
+}
+
+void launch_green_spectral_f64(int N, double L, double2* modes, const double* win,
+                               double four_pi_G, double scale, double r_s,
+                               double input_mass, double mass_tolerance,
+                               unsigned int* status, cudaStream_t s) {
+    const uint64_t total = static_cast<uint64_t>(N) * N * (N / 2 + 1);
+    k_green_spectral<<<blocks_for(total), kThreads, 0, s>>>(
+        N, L, modes, win, four_pi_G, scale, r_s, input_mass, mass_tolerance, status);
+}
+
+void launch_spectral_axis_f64(int N, double L, int axis, const double2* phi_k,
+                              double2* out_k, cudaStream_t s) {
+    const uint64_t total = static_cast<uint64_t>(N) * N * (N / 2 + 1);
+    k_spectral_axis<<<blocks_for(total), kThreads, 0, s>>>(N, L, axis, phi_k, out_k);
+}
+
+void launch_interp_add_f64(uint32_t n, const double* field, const ParticlesF64& p,
+                           Axis a, double* out, unsigned int* status, cudaStream_t s) {
+    if (n == 0) return;
+    k_interp_add<<<blocks_for(n), kThreads, 0, s>>>(n, field, p.x, p.y, p.z, a, out, status);
+}
+
+void launch_gather_kick_f64(uint32_t n, const double* phi, const ParticlesF64& p,
+                            double* ax, double* ay, double* az, int do_kick, double K2,
+                            double* pxo, double* pyo, double* pzo, Axis a,
+                            unsigned int* status, cudaStream_t s) {
+    if (n == 0) return;
+    k_gather_kick<<<blocks_for(n), kThreads, 0, s>>>(n, phi, p.x, p.y, p.z, p.px, p.py, p.pz,
+                                                     ax, ay, az, do_kick, K2, pxo, pyo, pzo,
+                                                     a, status);
+}
+
+void launch_kick_only_f64(uint32_t n, const ParticlesF64& p, const double* ax,
+                          const double* ay, const double* az, double K2, double* pxo,
+                          double* pyo, double* pzo, unsigned int* status, cudaStream_t s) {
+    if (n == 0) return;
+    k_kick_only<<<blocks_for(n), kThreads, 0, s>>>(n, p.px, p.py, p.pz, ax, ay, az, K2, pxo,
+                                                   pyo, pzo, status);
+}
+
+void launch_cell_coords_f64(uint32_t n, const double* pos, Axis a, int64_t* base,
+                            double* frac, unsigned int* status, cudaStream_t s) {
+    if (n == 0) return;
+    k_cell_coords<<<blocks_for(n), kThreads, 0, s>>>(n, pos, a, base, frac, status);
+}
+
+}  // namespace hyowon

@@ -1,0 +1,1009 @@
+// pm_handle.cu -- the C ABI of include/hyowon_pm.h: device state, cuFFT plans
+// and the orchestration of one force solve / one KDK step on one stream.
+//
+// Step structure (binary64 form), for particle state P, accelerations A:
+//   1. kick_drift_key: P' = K1-kick + drift of P into the spare buffer set,
+//      cell-bucket key + histogram (rank) per particle;
+//   2. exclusive scan of the bucket histogram;
+//   3. scatter P' -> P in bucket order (skipped on a device error: nothing is
+//      published, as LeapfrogIntegrator's preflight, leapfrog_integrator.cpp:170-190);
+//   4. deposit, D2Z, Green (+ density normalisation, 1/N^3, mass check), Z2D;
+//   5. gather_kick: A = -grad(phi) at P, p'' = p' + A*K2 into the spare
+//      momentum buffer, published by a pointer swap after the status check.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "hyowon_pm.h"
+#include "pm_fp32.h"
+#include "pm_kernels.h"
+#include "pm_lpt.h"
+
+namespace hyowon {
+void launch_scatter_multi(uint32_t n, const uint32_t* key, const uint32_t* rank,
+                          const uint32_t* offset, int n_f64, const double* const* src,
+                          double* const* dst, int n_u32, const uint32_t* const* src_u,
+                          uint32_t* const* dst_u, const unsigned int* status,
+                          cudaStream_t s);
+}
+
+using namespace hyowon;
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// include/cosmo_nbody/cosmology/units.hpp:12-25, evaluated in that order.
+double gravitational_constant() {
+    const double G_SI = 6.67430e-11;
+    const double Mpc_in_m = 3.085677581491367e22;
+    const double Msun_in_kg = 1.98847e30;
+    const double MassUnit_in_kg = 1e10 * Msun_in_kg;
+    const double V = 1000.0;
+    return G_SI * MassUnit_in_kg / (Mpc_in_m * V * V);
+}
+
+struct Error {
+    int code;
+    std::string msg;
+};
+
+}  // namespace
+
+struct hyowon_pm_s {
+    double L = 0.0;
+    int N = 0;
+    int method = HYOWON_PURE_PM;
+    int deconvolve = 0;
+    double r_s = 0.0;
+    int precision = HYOWON_FP64;
+    Axis axis{};
+    double four_pi_G = 0.0;
+    double field_scale = 0.0;  // (1/dx^3) * (1/N^3)
+
+    cudaStream_t stream = nullptr;
+    cufftHandle plan_r2c = 0;
+    cufftHandle plan_c2r = 0;
+    bool plans = false;
+    void* fft_work = nullptr;
+
+    double* mesh = nullptr;      // real N^3: mass, then potential
+    double2* modes = nullptr;    // half spectrum
+    double2* phi_k = nullptr;    // spectral method: kept copy of phi_k
+    double* lap = nullptr;       // 1-D discrete Laplacian symbol (N)
+    double* win = nullptr;       // 1-D CIC window W(k) (N)
+
+    uint32_t n = 0;
+    uint32_t cap = 0;
+    double* pos[2][3] = {};
+    double* mom[2][3] = {};
+    uint32_t* id[2] = {};
+    double* mass[2] = {};
+    int pc = 0, mc = 0, ic = 0;
+    double* acc[3] = {};
+    bool acc_valid = false;
+    bool sorted = false;
+    bool has_state = false;
+    double uniform_mass = 0.0;
+    bool has_masses = false;
+    double input_mass = 0.0;
+    double mass_tol = 0.0;
+
+    SortWork sort{};
+    uint32_t sort_cap_buckets = 0;
+
+    unsigned int* d_status = nullptr;
+    unsigned long long* d_maxdrift = nullptr;
+    unsigned int* h_status = nullptr;           // pinned
+    unsigned long long* h_maxdrift = nullptr;   // pinned
+
+    fp32::State* f32 = nullptr;  // precision form (pm_fp32.cu)
+
+    bool timing = false;
+    cudaEvent_t ev[8] = {};
+    cudaEvent_t call_ev[2] = {};
+    double last_times[8] = {};
+    uint64_t launches = 0;  // kernels launched by this library (cuFFT excluded)
+
+    std::string err;
+};
+
+namespace {
+
+int fail(hyowon_pm_t h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_fail(hyowon_pm_t h, cudaError_t e, const char* where) {
+    return fail(h, e == cudaErrorMemoryAllocation ? HYOWON_ENOMEM : HYOWON_ECUDA,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+    } while (0)
+
+#define CKFFT(call)                                                             \
+    do {                                                                        \
+        cufftResult r_ = (call);                                                \
+        if (r_ != CUFFT_SUCCESS)                                                \
+            return fail(h, HYOWON_ECUDA, std::string(#call) + ": cufft error " \
+                                             + std::to_string(static_cast<int>(r_))); \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+// Maps device status bits onto the reference's exception classes.
+int status_to_code(hyowon_pm_t h, unsigned int st) {
+    if (st == 0) return HYOWON_OK;
+    if (st & ST_NONFINITE_INPUT)
+        return fail(h, HYOWON_EINVAL, "particle positions and masses must be finite (masses non-negative)");
+    if (st & ST_CELL_ESCAPE)
+        return fail(h, HYOWON_ELOGIC, "CIC bounded coordinate escaped the mesh domain");
+    if (st & ST_KICK_DRIFT)
+        return fail(h, HYOWON_EOVERFLOW, "Leapfrog K1/drift update is not finite and representable");
+    if (st & ST_MASS)
+        return fail(h, HYOWON_ERUNTIME, "CIC deposited mass violates the binary64 forward-error bound");
+    if (st & ST_CAPACITY)
+        return fail(h, HYOWON_ERUNTIME, "fixed-point mass cell capacity exceeded");
+    if (st & ST_FORCE)
+        return fail(h, HYOWON_EOVERFLOW, "PM backend produced a non-finite force");
+    if (st & ST_KICK2)
+        return fail(h, HYOWON_EOVERFLOW, "Leapfrog K2 update is not finite and representable");
+    if (st & ST_UNDERFLOW)
+        return fail(h, HYOWON_EUNDERFLOW, "CIC centered-gradient gather lost a non-zero product");
+    return fail(h, HYOWON_ERUNTIME, "unknown device status");
+}
+
+ParticlesF64 set_view(hyowon_pm_t h, int pset, int mset) {
+    return ParticlesF64{h->pos[pset][0], h->pos[pset][1], h->pos[pset][2],
+                        h->mom[mset][0], h->mom[mset][1], h->mom[mset][2]};
+}
+
+void free_particles(hyowon_pm_t h) {
+    for (int s = 0; s < 2; ++s) {
+        for (int a = 0; a < 3; ++a) {
+            cudaFree(h->pos[s][a]);
+            cudaFree(h->mom[s][a]);
+            h->pos[s][a] = h->mom[s][a] = nullptr;
+        }
+        cudaFree(h->id[s]);
+        cudaFree(h->mass[s]);
+        h->id[s] = nullptr;
+        h->mass[s] = nullptr;
+    }
+    for (int a = 0; a < 3; ++a) {
+        cudaFree(h->acc[a]);
+        h->acc[a] = nullptr;
+    }
+    cudaFree(h->sort.key);
+    cudaFree(h->sort.rank);
+    h->sort.key = h->sort.rank = nullptr;
+    h->cap = 0;
+}
+
+int ensure_capacity(hyowon_pm_t h, uint32_t n, bool masses) {
+    if (n <= h->cap && (!masses || h->mass[0])) return HYOWON_OK;
+    free_particles(h);
+    for (int s = 0; s < 2; ++s) {
+        for (int a = 0; a < 3; ++a) {
+            CK(dalloc(&h->pos[s][a], n));
+            CK(dalloc(&h->mom[s][a], n));
+        }
+        CK(dalloc(&h->id[s], n));
+        if (masses) CK(dalloc(&h->mass[s], n));
+    }
+    for (int a = 0; a < 3; ++a) CK(dalloc(&h->acc[a], n));
+    CK(dalloc(&h->sort.key, n));
+    CK(dalloc(&h->sort.rank, n));
+    h->cap = n;
+    return HYOWON_OK;
+}
+
+// Buckets of 2^shift consecutive cells, about eight particles per bucket.
+int ensure_sort_buckets(hyowon_pm_t h, uint32_t n) {
+    const uint64_t cells = static_cast<uint64_t>(h->N) * h->N * h->N;
+    int shift = 0;
+    while (shift < 30 && (cells >> (shift + 1)) * 8 >= static_cast<uint64_t>(n) && (cells >> (shift + 1)) > 0)
+        ++shift;
+    const uint32_t nb = static_cast<uint32_t>((cells + (1ull << shift) - 1) >> shift);
+    h->sort.shift = shift;
+    h->sort.n_buckets = nb;
+    if (nb > h->sort_cap_buckets) {
+        cudaFree(h->sort.count);
+        cudaFree(h->sort.offset);
+        cudaFree(h->sort.scan_tmp);
+        CK(dalloc(&h->sort.count, nb + 1));
+        CK(dalloc(&h->sort.offset, nb + 1));
+        CK(dalloc(&h->sort.scan_tmp, scan_tmp_elements(nb + 1)));
+        h->sort_cap_buckets = nb;
+    }
+    return HYOWON_OK;
+}
+
+// Input mass and the CIC mass-conservation bound of
+// src/math/cic_mass_conservation.cpp:26-59, with a small allowance for the
+// rounding of the FFT's k=0 sum that stands in for the exact mesh-mass sum.
+void set_input_mass(hyowon_pm_t h, double total, uint32_t n) {
+    h->input_mass = total;
+    const long double eps = std::numeric_limits<double>::epsilon();
+    const long double nu = (32.0L * n + 1.0L) * eps;
+    const long double gamma = nu / (1.0L - nu);
+    h->mass_tol = static_cast<double>((gamma + 64.0L * eps) * total * (1.0L + 4.0L * gamma));
+}
+
+int read_status(hyowon_pm_t h, unsigned int* st) {
+    CK(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *st = *h->h_status;
+    return HYOWON_OK;
+}
+
+// Permutes the current particle state into bucket order (used after upload).
+int sort_current(hyowon_pm_t h) {
+    const uint32_t n = h->n;
+    CK(cudaMemsetAsync(h->sort.count, 0, sizeof(uint32_t) * (h->sort.n_buckets + 1), h->stream));
+    ++h->launches;
+    launch_key_f64(n, set_view(h, h->pc, h->mc), h->axis, h->sort, h->d_status, h->stream);
+    h->launches += launch_exclusive_scan(h->sort.count, h->sort.offset, h->sort.n_buckets + 1, h->sort.scan_tmp,
+                          h->stream);
+    const double* src[8];
+    double* dst[8];
+    int k = 0;
+    for (int a = 0; a < 3; ++a) {
+        src[k] = h->pos[h->pc][a];
+        dst[k++] = h->pos[1 - h->pc][a];
+    }
+    for (int a = 0; a < 3; ++a) {
+        src[k] = h->mom[h->mc][a];
+        dst[k++] = h->mom[1 - h->mc][a];
+    }
+    if (h->has_masses) {
+        src[k] = h->mass[h->ic];
+        dst[k++] = h->mass[1 - h->ic];
+    }
+    const uint32_t* su[1] = {h->id[h->ic]};
+    uint32_t* du[1] = {h->id[1 - h->ic]};
+    ++h->launches;
+    launch_scatter_multi(n, h->sort.key, h->sort.rank, h->sort.offset, k, src, dst, 1, su, du,
+                         h->d_status, h->stream);
+    unsigned int st = 0;
+    int rc = read_status(h, &st);
+    if (rc) return rc;
+    if (st) return status_to_code(h, st);
+    h->pc = 1 - h->pc;
+    h->mc = 1 - h->mc;
+    h->ic = 1 - h->ic;
+    h->sorted = true;
+    return HYOWON_OK;
+}
+
+void record(hyowon_pm_t h, int i) {
+    if (h->timing) cudaEventRecord(h->ev[i], h->stream);
+}
+
+// Deposit -> FFT -> Green -> inverse FFT -> gather (+ K2 into the spare momenta).
+// Leaves the status check to the caller.
+int enqueue_force(hyowon_pm_t h, bool kick, double K2) {
+    const uint32_t n = h->n;
+    const int N = h->N;
+    const size_t cells = static_cast<size_t>(N) * N * N;
+    if (h->precision == HYOWON_FP32_FIXED) {
+        return fp32::enqueue_force(h->f32, h->stream, h->d_status, kick, K2, h->timing ? h->ev : nullptr);
+    }
+    const ParticlesF64 p = set_view(h, h->pc, h->mc);
+    record(h, 1);
+    CK(cudaMemsetAsync(h->mesh, 0, sizeof(double) * cells, h->stream));
+    ++h->launches;
+    launch_deposit_f64(n, p, h->has_masses ? h->mass[h->ic] : nullptr, h->uniform_mass, h->axis,
+                       h->mesh, h->d_status, h->stream);
+    record(h, 2);
+    CKFFT(cufftExecD2Z(h->plan_r2c, h->mesh, reinterpret_cast<cufftDoubleComplex*>(h->modes)));
+    record(h, 3);
+    double* const pxo = h->mom[1 - h->mc][0];
+    double* const pyo = h->mom[1 - h->mc][1];
+    double* const pzo = h->mom[1 - h->mc][2];
+    if (h->method == HYOWON_PURE_PM) {
+        ++h->launches;
+        launch_green_f64(N, h->modes, h->lap, h->win, h->four_pi_G, h->field_scale, h->deconvolve,
+                         h->input_mass, h->mass_tol, h->d_status, h->stream);
+        record(h, 4);
+        CKFFT(cufftExecZ2D(h->plan_c2r, reinterpret_cast<cufftDoubleComplex*>(h->modes), h->mesh));
+        record(h, 5);
+        ++h->launches;
+        launch_gather_kick_f64(n, h->mesh, p, h->acc[0], h->acc[1], h->acc[2], kick ? 1 : 0, K2,
+                               pxo, pyo, pzo, h->axis, h->d_status, h->stream);
+        record(h, 6);
+        return HYOWON_OK;
+    }
+    // TreePM long range: Green's function once, then per axis -ik, C2R and a
+    // plain CIC gather added to the zeroed acceleration.
+    ++h->launches;
+    launch_green_spectral_f64(N, h->L, h->modes, h->win, h->four_pi_G, h->field_scale, h->r_s,
+                              h->input_mass, h->mass_tol, h->d_status, h->stream);
+    CK(cudaMemcpyAsync(h->phi_k, h->modes, sizeof(double2) * static_cast<size_t>(N) * N * (N / 2 + 1),
+                       cudaMemcpyDeviceToDevice, h->stream));
+    record(h, 4);
+    for (int a = 0; a < 3; ++a) {
+        CK(cudaMemsetAsync(h->acc[a], 0, sizeof(double) * n, h->stream));
+        ++h->launches;
+        launch_spectral_axis_f64(N, h->L, a, h->phi_k, h->modes, h->stream);
+        CKFFT(cufftExecZ2D(h->plan_c2r, reinterpret_cast<cufftDoubleComplex*>(h->modes), h->mesh));
+        ++h->launches;
+        launch_interp_add_f64(n, h->mesh, p, h->axis, h->acc[a], h->d_status, h->stream);
+    }
+    record(h, 5);
+    if (kick) {
+        ++h->launches;
+        launch_kick_only_f64(n, p, h->acc[0], h->acc[1], h->acc[2], K2, pxo, pyo, pzo, h->d_status,
+                             h->stream);
+    }
+    record(h, 6);
+    return HYOWON_OK;
+}
+
+void collect_timing(hyowon_pm_t h) {
+    if (!h->timing) return;
+    cudaEventSynchronize(h->ev[6]);
+    float t = 0.f;
+    for (int i = 0; i < 6; ++i) {
+        cudaEventElapsedTime(&t, h->ev[i], h->ev[i + 1]);
+        h->last_times[i + 1] = t;
+    }
+}
+
+// Whole-call device time and launch count (hyowon_pm_last_timing).
+struct CallTimer {
+    hyowon_pm_t h;
+    uint64_t launches0;
+    explicit CallTimer(hyowon_pm_t hh) : h(hh), launches0(hh->launches) {
+        if (h->timing) cudaEventRecord(h->call_ev[0], h->stream);
+    }
+    ~CallTimer() {
+        if (!h->timing) return;
+        cudaEventRecord(h->call_ev[1], h->stream);
+        cudaEventSynchronize(h->call_ev[1]);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, h->call_ev[0], h->call_ev[1]);
+        h->last_times[0] = t;
+        h->last_times[7] = static_cast<double>(h->launches - launches0);
+    }
+};
+
+// Force solve at the current positions; accelerations become valid.
+int solve_force(hyowon_pm_t h) {
+    if (!h->sorted) {
+        int rc = h->precision == HYOWON_FP32_FIXED ? fp32::sort_current(h->f32, h->stream, h->d_status)
+                                                   : sort_current(h);
+        if (rc) return h->precision == HYOWON_FP32_FIXED ? status_or_cuda(h, rc) : rc;
+        h->sorted = true;
+    }
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
+    record(h, 0);
+    int rc = enqueue_force(h, false, 0.0);
+    if (rc) return rc;
+    unsigned int st = 0;
+    rc = read_status(h, &st);
+    if (rc) return rc;
+    collect_timing(h);
+    if (st) {
+        h->acc_valid = false;
+        return status_to_code(h, st);
+    }
+    h->acc_valid = true;
+    return HYOWON_OK;
+}
+
+}  // namespace
+
+namespace hyowon {
+// Used by the precision form to report CUDA failures through the handle.
+int status_or_cuda(hyowon_pm_t h, int rc) {
+    if (rc == HYOWON_OK) return rc;
+    if (h->f32 && !fp32::last_error(h->f32).empty()) h->err = fp32::last_error(h->f32);
+    return rc;
+}
+}  // namespace hyowon
+
+namespace {
+
+int kdk_step_impl(hyowon_pm_t h, double K1, double D, double K2, double* max_drift) {
+    if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
+    if (!std::isfinite(K1) || !std::isfinite(D) || !std::isfinite(K2))
+        return fail(h, HYOWON_EOVERFLOW, "Leapfrog K1/drift update is not finite and representable");
+    if (!h->acc_valid) {
+        int rc = solve_force(h);
+        if (rc) return rc;
+    }
+    if (h->precision == HYOWON_FP32_FIXED) {
+        int rc = fp32::kdk_step(h->f32, h->stream, h->d_status, h->d_maxdrift, K1, D, K2,
+                                h->timing ? h->ev : nullptr);
+        if (rc) return status_or_cuda(h, rc);
+        unsigned int st = 0;
+        rc = read_status(h, &st);
+        if (rc) return rc;
+        collect_timing(h);
+        const bool published = (st & ST_BLOCKS_PUBLISH) == 0;
+        fp32::commit_step(h->f32, published, st == 0);
+        if (st) {
+            h->acc_valid = false;
+            return status_to_code(h, st);
+        }
+        if (max_drift) {
+            CK(cudaMemcpy(h->h_maxdrift, h->d_maxdrift, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+            double d;
+            std::memcpy(&d, h->h_maxdrift, sizeof(double));
+            *max_drift = d;
+        }
+        return HYOWON_OK;
+    }
+    const uint32_t n = h->n;
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
+    CK(cudaMemsetAsync(h->d_maxdrift, 0, sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->sort.count, 0, sizeof(uint32_t) * (h->sort.n_buckets + 1), h->stream));
+    record(h, 0);
+    // 1. candidate = K1 kick + drift of the current state, into the spare set.
+    const ParticlesF64 cur = set_view(h, h->pc, h->mc);
+    const ParticlesF64 cand = set_view(h, 1 - h->pc, 1 - h->mc);
+    ++h->launches;
+    launch_kick_drift_key_f64(n, cur, h->acc[0], h->acc[1], h->acc[2], K1, D, h->axis, cand,
+                              h->sort, h->d_maxdrift, h->d_status, h->stream);
+    // 2-3. sort the candidate back into the current set (publication).
+    h->launches += launch_exclusive_scan(h->sort.count, h->sort.offset, h->sort.n_buckets + 1, h->sort.scan_tmp,
+                          h->stream);
+    {
+        const double* src[8];
+        double* dst[8];
+        int k = 0;
+        src[k] = cand.x; dst[k++] = cur.x;
+        src[k] = cand.y; dst[k++] = cur.y;
+        src[k] = cand.z; dst[k++] = cur.z;
+        src[k] = cand.px; dst[k++] = cur.px;
+        src[k] = cand.py; dst[k++] = cur.py;
+        src[k] = cand.pz; dst[k++] = cur.pz;
+        if (h->has_masses) {
+            src[k] = h->mass[h->ic];
+            dst[k++] = h->mass[1 - h->ic];
+        }
+        const uint32_t* su[1] = {h->id[h->ic]};
+        uint32_t* du[1] = {h->id[1 - h->ic]};
+        ++h->launches;
+        launch_scatter_multi(n, h->sort.key, h->sort.rank, h->sort.offset, k, src, dst, 1, su, du,
+                             h->d_status, h->stream);
+    }
+    // The scatter is the publication point; later kernels skip on error too.
+    const int ic_after = 1 - h->ic;
+    const int ic_before = h->ic;
+    h->ic = ic_after;
+    int rc = enqueue_force(h, true, K2);
+    if (rc) return rc;
+    unsigned int st = 0;
+    rc = read_status(h, &st);
+    if (rc) return rc;
+    collect_timing(h);
+    if (st & ST_BLOCKS_PUBLISH) {
+        // Nothing was published: state is that of the step's start.
+        h->ic = ic_before;
+        return status_to_code(h, st);
+    }
+    if (st) {
+        // Positions drifted and momenta K1-kicked are published; the force or
+        // the K2 kick failed, so momenta stay at p' and acceleration is invalid.
+        h->acc_valid = false;
+        return status_to_code(h, st);
+    }
+    h->mc = 1 - h->mc;  // publish p''
+    h->acc_valid = true;
+    if (max_drift) {
+        CK(cudaMemcpy(h->h_maxdrift, h->d_maxdrift, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        double d;
+        std::memcpy(&d, h->h_maxdrift, sizeof(double));
+        *max_drift = d;
+    }
+    return HYOWON_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hyowon_pm_create(double box_size, uint64_t mesh_size, int method, int deconvolve_cic,
+                     double split_scale, int precision, hyowon_pm_t* out) {
+    if (!out) return HYOWON_EINVAL;
+    *out = nullptr;
+    if (!std::isfinite(box_size) || box_size <= 0.0 || mesh_size < 2 || mesh_size > 2048)
+        return HYOWON_EINVAL;
+    if (method != HYOWON_PURE_PM && method != HYOWON_TREEPM_LONG_RANGE) return HYOWON_EINVAL;
+    if (precision != HYOWON_FP64 && precision != HYOWON_FP32_FIXED) return HYOWON_EINVAL;
+    if (method == HYOWON_TREEPM_LONG_RANGE && (!std::isfinite(split_scale) || split_scale <= 0.0))
+        return HYOWON_EINVAL;
+    hyowon_pm_t h = new (std::nothrow) hyowon_pm_s();
+    if (!h) return HYOWON_ENOMEM;
+    h->L = box_size;
+    h->N = static_cast<int>(mesh_size);
+    h->method = method;
+    h->deconvolve = method == HYOWON_TREEPM_LONG_RANGE ? 1 : (deconvolve_cic ? 1 : 0);
+    h->r_s = split_scale;
+    h->precision = precision;
+    const int N = h->N;
+    h->axis.L = box_size;
+    h->axis.dx = box_size / static_cast<double>(N);
+    h->axis.upper = std::nextafter(static_cast<double>(N), 0.0);
+    h->axis.N = N;
+    h->four_pi_G = 4.0 * kPi * gravitational_constant();
+    const double dx = h->axis.dx;
+    const double inv_vol = 1.0 / (dx * dx * dx);
+    const double norm = 1.0 / (static_cast<double>(N) * static_cast<double>(N) * static_cast<double>(N));
+    h->field_scale = inv_vol * norm;
+
+    auto bail = [&](int code) {
+        hyowon_pm_destroy(h);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(HYOWON_ECUDA);
+    if (cudaMallocHost(reinterpret_cast<void**>(&h->h_status), sizeof(unsigned int)) != cudaSuccess
+        || cudaMallocHost(reinterpret_cast<void**>(&h->h_maxdrift), sizeof(unsigned long long)) != cudaSuccess
+        || dalloc(&h->d_status, 1) != cudaSuccess || dalloc(&h->d_maxdrift, 1) != cudaSuccess)
+        return bail(HYOWON_ENOMEM);
+    for (auto& e : h->ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) return bail(HYOWON_ECUDA);
+    }
+    for (auto& e : h->call_ev) {
+        if (cudaEventCreate(&e) != cudaSuccess) return bail(HYOWON_ECUDA);
+    }
+
+    // Green's-function 1-D tables on the host with the reference's formulas
+    // (src/mesh/green_function.cpp:59-87,137-163) so the device symbol is
+    // bit-identical to the reference's.
+    std::vector<double> lap(N), win(N);
+    {
+        const double inv = 1.0 / dx;
+        const double inv2 = inv * inv;
+        const double nn = static_cast<double>(N);
+        for (int i = 0; i < N; ++i) {
+            const long long mode = i <= N / 2 ? i : static_cast<long long>(i) - N;
+            const double s = std::sin(kPi * static_cast<double>(mode) / nn);
+            lap[i] = -4.0 * inv2 * s * s;
+            const long double arg = 3.141592653589793238462643383279502884L
+                * static_cast<long double>(mode) / static_cast<long double>(N);
+            if (arg == 0.0L) {
+                win[i] = 1.0;
+            } else {
+                long double mag = std::fabs(std::sin(arg) / arg);
+                if (mag > 1.0L) mag = 1.0L;
+                win[i] = static_cast<double>(mag * mag);
+            }
+        }
+    }
+    if (dalloc(&h->lap, N) != cudaSuccess || dalloc(&h->win, N) != cudaSuccess) return bail(HYOWON_ENOMEM);
+    cudaMemcpy(h->lap, lap.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
+    cudaMemcpy(h->win, win.data(), sizeof(double) * N, cudaMemcpyHostToDevice);
+
+    if (precision == HYOWON_FP32_FIXED) {
+        int rc = fp32::create(&h->f32, h->L, N, method, h->deconvolve, split_scale, lap.data(),
+                              win.data(), h->four_pi_G, h->stream);
+        if (rc) {
+            if (h->f32) h->err = fp32::last_error(h->f32);
+            return bail(rc);
+        }
+        *out = h;
+        return HYOWON_OK;
+    }
+
+    const size_t cells = static_cast<size_t>(N) * N * N;
+    const size_t half = static_cast<size_t>(N) * N * (N / 2 + 1);
+    if (dalloc(&h->mesh, cells) != cudaSuccess || dalloc(&h->modes, half) != cudaSuccess)
+        return bail(HYOWON_ENOMEM);
+    if (method == HYOWON_TREEPM_LONG_RANGE && dalloc(&h->phi_k, half) != cudaSuccess)
+        return bail(HYOWON_ENOMEM);
+    size_t ws1 = 0, ws2 = 0;
+    if (cufftCreate(&h->plan_r2c) != CUFFT_SUCCESS || cufftCreate(&h->plan_c2r) != CUFFT_SUCCESS)
+        return bail(HYOWON_ECUDA);
+    h->plans = true;
+    cufftSetAutoAllocation(h->plan_r2c, 0);
+    cufftSetAutoAllocation(h->plan_c2r, 0);
+    if (cufftMakePlan3d(h->plan_r2c, N, N, N, CUFFT_D2Z, &ws1) != CUFFT_SUCCESS
+        || cufftMakePlan3d(h->plan_c2r, N, N, N, CUFFT_Z2D, &ws2) != CUFFT_SUCCESS)
+        return bail(HYOWON_ECUDA);
+    if (cudaMalloc(&h->fft_work, std::max<size_t>(1, std::max(ws1, ws2))) != cudaSuccess)
+        return bail(HYOWON_ENOMEM);
+    cufftSetWorkArea(h->plan_r2c, h->fft_work);
+    cufftSetWorkArea(h->plan_c2r, h->fft_work);
+    cufftSetStream(h->plan_r2c, h->stream);
+    cufftSetStream(h->plan_c2r, h->stream);
+    *out = h;
+    return HYOWON_OK;
+}
+
+int hyowon_pm_destroy(hyowon_pm_t h) {
+    if (!h) return HYOWON_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->f32) fp32::destroy(h->f32);
+    if (h->plans) {
+        cufftDestroy(h->plan_r2c);
+        cufftDestroy(h->plan_c2r);
+    }
+    cudaFree(h->fft_work);
+    cudaFree(h->mesh);
+    cudaFree(h->modes);
+    cudaFree(h->phi_k);
+    cudaFree(h->lap);
+    cudaFree(h->win);
+    free_particles(h);
+    cudaFree(h->sort.count);
+    cudaFree(h->sort.offset);
+    cudaFree(h->sort.scan_tmp);
+    cudaFree(h->d_status);
+    cudaFree(h->d_maxdrift);
+    if (h->h_status) cudaFreeHost(h->h_status);
+    if (h->h_maxdrift) cudaFreeHost(h->h_maxdrift);
+    for (auto& e : h->ev) {
+        if (e) cudaEventDestroy(e);
+    }
+    for (auto& e : h->call_ev) {
+        if (e) cudaEventDestroy(e);
+    }
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return HYOWON_OK;
+}
+
+const char* hyowon_pm_last_error(hyowon_pm_t h) {
+    if (!h) return "null handle";
+    return h->err.c_str();
+}
+
+int hyowon_pm_upload(hyowon_pm_t h, uint64_t n64, const double* x, const double* y, const double* z,
+                     const double* px, const double* py, const double* pz, const double* masses,
+                     double uniform_mass) {
+    if (!h) return HYOWON_EINVAL;
+    if (n64 == 0 || n64 > 0xFFFFFFF0ull) return fail(h, HYOWON_EINVAL, "particle count must be in [1, 2^32-16]");
+    if (!x || !y || !z) return fail(h, HYOWON_EINVAL, "position arrays must be non-null");
+    if (!masses && (!std::isfinite(uniform_mass) || uniform_mass <= 0.0))
+        return fail(h, HYOWON_EINVAL, "PMSolver uniform mass must be finite and positive");
+    const uint32_t n = static_cast<uint32_t>(n64);
+    h->has_state = false;
+    h->acc_valid = false;
+    h->sorted = false;
+    // Input mass (pm_solver.cpp:87-118): uniform = correctly rounded m*n;
+    // explicit masses summed in a wide accumulator.
+    double total = 0.0;
+    if (masses) {
+        long double s = 0.0L, c = 0.0L;
+        for (uint32_t i = 0; i < n; ++i) {
+            const double m = masses[i];
+            if (!std::isfinite(m) || m < 0.0)
+                return fail(h, HYOWON_EINVAL, "PMSolver explicit masses must be finite and non-negative");
+            const long double t = s + m;
+            c += (std::fabs(s) >= std::fabs(static_cast<long double>(m))) ? (s - t) + m : (m - t) + s;
+            s = t;
+        }
+        total = static_cast<double>(s + c);
+    } else {
+        total = uniform_mass * static_cast<double>(n);
+    }
+    if (!std::isfinite(total) || total <= 0.0)
+        return fail(h, HYOWON_ERUNTIME, "PMSolver exact input mass identity must be finite and positive");
+    set_input_mass(h, total, n);
+    h->uniform_mass = masses ? 0.0 : uniform_mass;
+    h->has_masses = masses != nullptr;
+    h->n = n;
+    if (h->precision == HYOWON_FP32_FIXED) {
+        int rc = fp32::upload(h->f32, n, x, y, z, px, py, pz, masses, uniform_mass, total,
+                              h->mass_tol, h->stream);
+        if (rc) return status_or_cuda(h, rc);
+        CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
+        fp32::validate(h->f32, h->stream, h->d_status);
+        unsigned int st = 0;
+        rc = read_status(h, &st);
+        if (rc) return rc;
+        if (st) return status_to_code(h, st);
+        h->has_state = true;
+        return HYOWON_OK;
+    }
+    int rc = ensure_capacity(h, n, masses != nullptr);
+    if (rc) return rc;
+    rc = ensure_sort_buckets(h, n);
+    if (rc) return rc;
+    h->pc = h->mc = h->ic = 0;
+    CK(cudaMemcpyAsync(h->pos[0][0], x, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->pos[0][1], y, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->pos[0][2], z, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    const double* moms[3] = {px, py, pz};
+    for (int a = 0; a < 3; ++a) {
+        if (moms[a]) {
+            CK(cudaMemcpyAsync(h->mom[0][a], moms[a], sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+        } else {
+            CK(cudaMemsetAsync(h->mom[0][a], 0, sizeof(double) * n, h->stream));
+        }
+    }
+    if (masses) CK(cudaMemcpyAsync(h->mass[0], masses, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    ++h->launches;
+    launch_iota_u32(n, h->id[0], h->stream);
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
+    ++h->launches;
+    launch_validate_inputs_f64(n, h->pos[0][0], h->pos[0][1], h->pos[0][2],
+                               masses ? h->mass[0] : nullptr, h->d_status, h->stream);
+    unsigned int st = 0;
+    rc = read_status(h, &st);
+    if (rc) return rc;
+    if (st) return status_to_code(h, st);
+    h->has_state = true;
+    return HYOWON_OK;
+}
+
+int hyowon_pm_lpt_ics(hyowon_pm_t h, uint64_t n_side, const double* noise, uint64_t n_nodes,
+                      const double* ln_k, const double* ln_p, const double* ln_p_y2,
+                      double momentum_factor, double uniform_mass) {
+    if (!h) return HYOWON_EINVAL;
+    if (n_side < 2 || n_side > 2048 || !noise || n_nodes < 2 || !ln_k || !ln_p || !ln_p_y2)
+        return fail(h, HYOWON_EINVAL, "LPT requires n_side in [2,2048], noise and a spline table");
+    if (!std::isfinite(uniform_mass) || uniform_mass <= 0.0 || !std::isfinite(momentum_factor))
+        return fail(h, HYOWON_EINVAL, "LPT uniform mass and momentum factor must be finite (mass positive)");
+    const uint64_t n64 = n_side * n_side * n_side;
+    if (n64 > 0xFFFFFFF0ull) return fail(h, HYOWON_EINVAL, "particle count exceeds 2^32-16");
+    const uint32_t n = static_cast<uint32_t>(n64);
+    const int N = static_cast<int>(n_side);
+    h->has_state = h->acc_valid = h->sorted = false;
+    double* d_noise = nullptr;
+    double* tab = nullptr;
+    CK(dalloc(&d_noise, n64));
+    CK(dalloc(&tab, 3 * n_nodes));
+    int rc = HYOWON_OK;
+    double* tmp_pos[3] = {};
+    double* tmp_mom[3] = {};
+    const char* err = nullptr;
+    if (cudaMemcpy(d_noise, noise, sizeof(double) * n64, cudaMemcpyHostToDevice) != cudaSuccess
+        || cudaMemcpy(tab, ln_k, sizeof(double) * n_nodes, cudaMemcpyHostToDevice) != cudaSuccess
+        || cudaMemcpy(tab + n_nodes, ln_p, sizeof(double) * n_nodes, cudaMemcpyHostToDevice) != cudaSuccess
+        || cudaMemcpy(tab + 2 * n_nodes, ln_p_y2, sizeof(double) * n_nodes, cudaMemcpyHostToDevice) != cudaSuccess) {
+        rc = fail(h, HYOWON_ECUDA, "LPT input copy failed");
+    }
+    if (rc == HYOWON_OK && h->precision == HYOWON_FP64) {
+        rc = ensure_capacity(h, n, false);
+        if (rc == HYOWON_OK) rc = ensure_sort_buckets(h, n);
+        for (int a = 0; a < 3; ++a) {
+            tmp_pos[a] = h->pos[0][a];
+            tmp_mom[a] = h->mom[0][a];
+        }
+    } else if (rc == HYOWON_OK) {
+        for (int a = 0; a < 3 && rc == HYOWON_OK; ++a) {
+            if (dalloc(&tmp_pos[a], n) != cudaSuccess || dalloc(&tmp_mom[a], n) != cudaSuccess)
+                rc = fail(h, HYOWON_ENOMEM, "LPT staging allocation failed");
+        }
+    }
+    if (rc == HYOWON_OK) {
+        cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream);
+        const int lrc = lpt_ics_device(N, h->L, d_noise, tab, tab + n_nodes, tab + 2 * n_nodes,
+                                       static_cast<int>(n_nodes), momentum_factor, tmp_pos,
+                                       tmp_mom, h->d_status, h->stream, &err);
+        if (lrc) rc = fail(h, lrc, err ? err : "LPT failed");
+    }
+    unsigned int st = 0;
+    if (rc == HYOWON_OK) rc = read_status(h, &st);
+    if (rc == HYOWON_OK && st)
+        rc = fail(h, HYOWON_EINVAL, "LPT spectrum table does not cover the mesh wavenumbers");
+    h->n = n;
+    h->uniform_mass = uniform_mass;
+    h->has_masses = false;
+    set_input_mass(h, uniform_mass * static_cast<double>(n), n);
+    if (rc == HYOWON_OK) {
+        if (h->precision == HYOWON_FP64) {
+            h->pc = h->mc = h->ic = 0;
+            ++h->launches;
+            launch_iota_u32(n, h->id[0], h->stream);
+            if (cudaStreamSynchronize(h->stream) != cudaSuccess) rc = fail(h, HYOWON_ECUDA, "iota failed");
+        } else {
+            rc = status_or_cuda(h, fp32::upload_device(h->f32, n, tmp_pos, tmp_mom, uniform_mass,
+                                                       h->input_mass, h->mass_tol, h->stream));
+        }
+    }
+    if (h->precision != HYOWON_FP64) {
+        for (int a = 0; a < 3; ++a) {
+            cudaFree(tmp_pos[a]);
+            cudaFree(tmp_mom[a]);
+        }
+    }
+    cudaFree(d_noise);
+    cudaFree(tab);
+    if (rc == HYOWON_OK) h->has_state = true;
+    return rc;
+}
+
+int hyowon_pm_download(hyowon_pm_t h, double* x, double* y, double* z, double* px, double* py,
+                       double* pz, double* ax, double* ay, double* az) {
+    if (!h) return HYOWON_EINVAL;
+    if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
+    if ((ax || ay || az) && !h->acc_valid)
+        return fail(h, HYOWON_ELOGIC, "accelerations are not valid (no successful force solve)");
+    if (h->precision == HYOWON_FP32_FIXED) {
+        int rc = fp32::download(h->f32, h->stream, x, y, z, px, py, pz, ax, ay, az);
+        return status_or_cuda(h, rc);
+    }
+    const uint32_t n = h->n;
+    // The spare position buffer is dead between calls: use it as staging.
+    double* stage = h->pos[1 - h->pc][0];
+    double* outs[9] = {x, y, z, px, py, pz, ax, ay, az};
+    const double* srcs[9] = {h->pos[h->pc][0], h->pos[h->pc][1], h->pos[h->pc][2],
+                             h->mom[h->mc][0], h->mom[h->mc][1], h->mom[h->mc][2],
+                             h->acc[0], h->acc[1], h->acc[2]};
+    for (int a = 0; a < 9; ++a) {
+        if (!outs[a]) continue;
+        ++h->launches;
+        launch_unpermute_f64(n, h->id[h->ic], srcs[a], stage, h->stream);
+        CK(cudaMemcpyAsync(outs[a], stage, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return HYOWON_OK;
+}
+
+int hyowon_pm_compute_forces(hyowon_pm_t h, double* ax, double* ay, double* az) {
+    if (!h) return HYOWON_EINVAL;
+    if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
+    int rc;
+    {
+        CallTimer timer(h);
+        rc = solve_force(h);
+    }
+    if (rc) return rc;
+    if (!ax && !ay && !az) return HYOWON_OK;
+    const uint32_t n = h->n;
+    double* outs[3] = {ax, ay, az};
+    std::vector<double> forces[3];
+    for (int a = 0; a < 3; ++a) {
+        if (outs[a]) forces[a].resize(n);
+    }
+    rc = hyowon_pm_download(h, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                            ax ? forces[0].data() : nullptr, ay ? forces[1].data() : nullptr,
+                            az ? forces[2].data() : nullptr);
+    if (rc) return rc;
+    // validate_force_commit (pm_solver.cpp:281-326) before any add.
+    for (int a = 0; a < 3; ++a) {
+        if (!outs[a]) continue;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (!std::isfinite(outs[a][i]) || !std::isfinite(outs[a][i] + forces[a][i]))
+                return fail(h, HYOWON_EOVERFLOW, "PMSolver force commit is not representable");
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        if (!outs[a]) continue;
+        for (uint32_t i = 0; i < n; ++i) outs[a][i] += forces[a][i];
+    }
+    return HYOWON_OK;
+}
+
+int hyowon_pm_forces_host(hyowon_pm_t h, uint64_t n, const double* x, const double* y,
+                          const double* z, const double* masses, double uniform_mass, double* ax,
+                          double* ay, double* az) {
+    int rc = hyowon_pm_upload(h, n, x, y, z, nullptr, nullptr, nullptr, masses, uniform_mass);
+    if (rc) return rc;
+    return hyowon_pm_compute_forces(h, ax, ay, az);
+}
+
+int hyowon_pm_kdk_step(hyowon_pm_t h, double K1, double D, double K2, double* max_drift) {
+    if (!h) return HYOWON_EINVAL;
+    CallTimer timer(h);
+    return kdk_step_impl(h, K1, D, K2, max_drift);
+}
+
+int hyowon_pm_run(hyowon_pm_t h, uint64_t n_steps, const double* K1, const double* D,
+                  const double* K2, double* max_drift) {
+    if (!h) return HYOWON_EINVAL;
+    if (n_steps > 0 && (!K1 || !D || !K2)) return fail(h, HYOWON_EINVAL, "factor arrays must be non-null");
+    CallTimer timer(h);
+    for (uint64_t s = 0; s < n_steps; ++s) {
+        int rc = kdk_step_impl(h, K1[s], D[s], K2[s], max_drift ? &max_drift[s] : nullptr);
+        if (rc) {
+            h->err = "step " + std::to_string(s) + ": " + h->err;
+            return rc;
+        }
+    }
+    return HYOWON_OK;
+}
+
+int hyowon_pm_info(hyowon_pm_t h, uint64_t* n_particles, uint64_t* mesh_size, int* precision,
+                   int* method) {
+    if (!h) return HYOWON_EINVAL;
+    if (n_particles) *n_particles = h->n;
+    if (mesh_size) *mesh_size = static_cast<uint64_t>(h->N);
+    if (precision) *precision = h->precision;
+    if (method) *method = h->method;
+    return HYOWON_OK;
+}
+
+int hyowon_pm_download_potential(hyowon_pm_t h, double* phi) {
+    if (!h || !phi) return HYOWON_EINVAL;
+    if (h->method != HYOWON_PURE_PM) return fail(h, HYOWON_ELOGIC, "potential is kept only for pure PM");
+    if (!h->acc_valid) return fail(h, HYOWON_ELOGIC, "no valid force solve");
+    if (h->precision == HYOWON_FP32_FIXED) return status_or_cuda(h, fp32::download_potential(h->f32, h->stream, phi));
+    const size_t cells = static_cast<size_t>(h->N) * h->N * h->N;
+    CK(cudaMemcpy(phi, h->mesh, sizeof(double) * cells, cudaMemcpyDeviceToHost));
+    return HYOWON_OK;
+}
+
+int hyowon_pm_download_mass_mesh(hyowon_pm_t h, double* mesh) {
+    if (!h || !mesh) return HYOWON_EINVAL;
+    if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
+    if (!h->sorted) {
+        int rc = h->precision == HYOWON_FP32_FIXED ? status_or_cuda(h, fp32::sort_current(h->f32, h->stream, h->d_status))
+                                                   : sort_current(h);
+        if (rc) return rc;
+        h->sorted = true;
+    }
+    if (h->precision == HYOWON_FP32_FIXED)
+        return status_or_cuda(h, fp32::download_mass_mesh(h->f32, h->stream, h->d_status, mesh));
+    const size_t cells = static_cast<size_t>(h->N) * h->N * h->N;
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
+    CK(cudaMemsetAsync(h->mesh, 0, sizeof(double) * cells, h->stream));
+    ++h->launches;
+    launch_deposit_f64(h->n, set_view(h, h->pc, h->mc), h->has_masses ? h->mass[h->ic] : nullptr,
+                       h->uniform_mass, h->axis, h->mesh, h->d_status, h->stream);
+    unsigned int st = 0;
+    int rc = read_status(h, &st);
+    if (rc) return rc;
+    if (st) return status_to_code(h, st);
+    CK(cudaMemcpy(mesh, h->mesh, sizeof(double) * cells, cudaMemcpyDeviceToHost));
+    h->acc_valid = false;  // the potential buffer was overwritten
+    return HYOWON_OK;
+}
+
+int hyowon_pm_cell_coords(hyowon_pm_t h, int64_t* base, double* frac) {
+    if (!h || !base || !frac) return HYOWON_EINVAL;
+    if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
+    if (h->precision == HYOWON_FP32_FIXED) return fail(h, HYOWON_ELOGIC, "cell coordinates of the binary64 form only");
+    const uint32_t n = h->n;
+    int64_t* db = nullptr;
+    double* df = nullptr;
+    double* stage = nullptr;
+    CK(dalloc(&db, static_cast<size_t>(n)));
+    CK(dalloc(&df, static_cast<size_t>(n)));
+    CK(dalloc(&stage, static_cast<size_t>(n)));
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
+    int rc = HYOWON_OK;
+    for (int a = 0; a < 3 && rc == HYOWON_OK; ++a) {
+        ++h->launches;
+        launch_unpermute_f64(n, h->id[h->ic], h->pos[h->pc][a], stage, h->stream);
+        ++h->launches;
+        launch_cell_coords_f64(n, stage, h->axis, db, df, h->d_status, h->stream);
+        if (cudaMemcpyAsync(base + static_cast<size_t>(a) * n, db, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess
+            || cudaMemcpyAsync(frac + static_cast<size_t>(a) * n, df, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess
+            || cudaStreamSynchronize(h->stream) != cudaSuccess)
+            rc = fail(h, HYOWON_ECUDA, "cell coordinate copy failed");
+    }
+    cudaFree(db);
+    cudaFree(df);
+    cudaFree(stage);
+    return rc;
+}
+
+int hyowon_pm_set_timing(hyowon_pm_t h, int enabled) {
+    if (!h) return HYOWON_EINVAL;
+    h->timing = enabled != 0;
+    return HYOWON_OK;
+}
+
+int hyowon_pm_last_timing(hyowon_pm_t h, double* times) {
+    if (!h || !times) return HYOWON_EINVAL;
+    for (int i = 0; i < 8; ++i) times[i] = h->last_times[i];
+    return HYOWON_OK;
+}
+
+}  // extern "C"

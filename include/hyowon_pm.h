@@ -1,0 +1,164 @@
+/*
+ * hyowon_pm.h -- C ABI of the B200 particle-mesh gravity step and
+ * kick-drift-kick update for HYOWON.
+ *
+ * One opaque handle owns everything on the device: the particle state
+ * (positions, momenta, accelerations, ids, optional masses), the mass / potential
+ * meshes, the cuFFT plans and their workspace, and one CUDA stream. Particle
+ * state stays device-resident across steps; the host synchronises it only
+ * through hyowon_pm_upload / hyowon_pm_download. Every call is synchronous at
+ * return, must come from one host thread per handle, and returns a status code
+ * (HYOWON_OK = 0). hyowon_pm_last_error() gives the message of the last failure.
+ *
+ * Reference interfaces each entry replaces are cited per function
+ * (paths relative to the HYOWON source tree).
+ */
+#ifndef HYOWON_PM_H
+#define HYOWON_PM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The C++ wrapper (hyowon_b200/csrc/gpu_pm_solver.hpp) maps
+ * them onto the exception types the reference throws for the same condition
+ * (src/gravity/pm_solver.cpp:509-525,281-326; src/time/leapfrog_integrator.cpp:183-261). */
+enum hyowon_status {
+    HYOWON_OK = 0,
+    HYOWON_EINVAL = 1,      /* std::invalid_argument: sizes, non-finite inputs   */
+    HYOWON_ELOGIC = 2,      /* std::logic_error: state / cell-assignment escape  */
+    HYOWON_EOVERFLOW = 3,   /* std::overflow_error: non-finite force or update   */
+    HYOWON_EUNDERFLOW = 4,  /* std::underflow_error                              */
+    HYOWON_ERUNTIME = 5,    /* std::runtime_error: mass conservation, capacity   */
+    HYOWON_ECUDA = 6,       /* CUDA / cuFFT failure                              */
+    HYOWON_ENOMEM = 7       /* device allocation failed                          */
+};
+
+/* PM force discretisation (include/cosmo_nbody/mesh/pm_force_method.hpp:16-67). */
+enum hyowon_method {
+    HYOWON_PURE_PM = 0,          /* discrete Laplacian + centred-gradient gather */
+    HYOWON_TREEPM_LONG_RANGE = 1 /* continuum -k^2, Gaussian split, spectral -ik */
+};
+
+/* Arithmetic form of the step. */
+enum hyowon_precision {
+    HYOWON_FP64 = 0,        /* binary64 throughout: the drop-in form             */
+    HYOWON_FP32_FIXED = 1   /* u32 fixed-point positions, int64 fixed-point mass
+                               deposit, FP32 FFT/Green/gather, FP64 drift        */
+};
+
+typedef struct hyowon_pm_s* hyowon_pm_t;
+
+/* Replaces the PMSolver constructor (src/gravity/pm_solver.cpp:378-386,
+ * include/cosmo_nbody/gravity/pm_solver.hpp:52-56) together with
+ * MeshGeometry(L, N_g) (include/cosmo_nbody/mesh/mesh_geometry.hpp:18-62) and
+ * PMForceMethod::pure_pm / treepm_long_range. split_scale is r_s for
+ * HYOWON_TREEPM_LONG_RANGE and ignored otherwise. */
+int hyowon_pm_create(double box_size, uint64_t mesh_size, int method,
+                     int deconvolve_cic, double split_scale, int precision,
+                     hyowon_pm_t* out);
+
+int hyowon_pm_destroy(hyowon_pm_t h);
+
+/* Message of the last failing call on h (never NULL). */
+const char* hyowon_pm_last_error(hyowon_pm_t h);
+
+/* Loads the ParticleStore SoA (include/cosmo_nbody/core/particle_store.hpp:33-124)
+ * into device memory: positions (any finite value; wrapped on device), canonical
+ * momenta p = a^2 dx/dt, and either per-particle masses (masses != NULL) or one
+ * uniform mass. Momenta may be NULL (zero). Accelerations become invalid until
+ * the next force solve. */
+int hyowon_pm_upload(hyowon_pm_t h, uint64_t n, const double* x, const double* y,
+                     const double* z, const double* px, const double* py,
+                     const double* pz, const double* masses, double uniform_mass);
+
+/* First-order LPT initial conditions generated on the device, replacing the
+ * particle state: from white noise w[n_side^3] (host, unit variance per lattice
+ * cell, row-major), delta_k = r2c(w) * sqrt(P(k) n_side^3 / L^3),
+ * psi = c2r(i k delta_k / k^2) / n_side^3 (Nyquist derivative zeroed),
+ * x = wrap(q + psi), p = momentum_factor * psi on the corner lattice
+ * q = (i,j,k) L / n_side, particle index (i n_side + j) n_side + k
+ * (src/ic/lpt_displacement.cpp:150-384, src/ic/initial_conditions.cpp:295-313,
+ * src/ic/random_field.cpp:119-129). P(k) at the start epoch is a natural cubic
+ * spline through (ln_k[i], ln_p[i]) with second derivatives ln_p_y2[i]
+ * (src/ic/linear_power_spectrum.cpp:649-664); momentum_factor = a^2 H(a) f1(a).
+ * All particles get uniform_mass. */
+int hyowon_pm_lpt_ics(hyowon_pm_t h, uint64_t n_side, const double* noise,
+                      uint64_t n_nodes, const double* ln_k, const double* ln_p,
+                      const double* ln_p_y2, double momentum_factor,
+                      double uniform_mass);
+
+/* Copies the device state back in the caller's original particle order. Any
+ * pointer may be NULL to skip that component. Positions are returned as
+ * stored (the drift wraps them to [0,L)); accelerations are those of the last
+ * force solve (HYOWON_ELOGIC if none). */
+int hyowon_pm_download(hyowon_pm_t h, double* x, double* y, double* z, double* px,
+                       double* py, double* pz, double* ax, double* ay, double* az);
+
+/* PMSolver::compute_forces (src/gravity/pm_solver.cpp:494-567) on the device
+ * state: solves the force at the current positions, stores it as the valid
+ * acceleration field, and ADDS it to the host arrays ax/ay/az when they are
+ * non-NULL (in original particle order), after validating that every sum is
+ * finite (validate_force_commit, src/gravity/pm_solver.cpp:281-326). */
+int hyowon_pm_compute_forces(hyowon_pm_t h, double* ax, double* ay, double* az);
+
+/* The stateless drop-in of PMSolver::compute_forces on HOST spans: uploads the
+ * positions (and masses), solves, adds the force to ax/ay/az. Equivalent to
+ * upload + compute_forces; the handle's previous particle state is replaced. */
+int hyowon_pm_forces_host(hyowon_pm_t h, uint64_t n, const double* x, const double* y,
+                          const double* z, const double* masses, double uniform_mass,
+                          double* ax, double* ay, double* az);
+
+/* One LeapfrogIntegrator::step (src/time/leapfrog_integrator.cpp:143-279) on
+ * the device state: K1 kick + drift with periodic wrap, force at a_end, K2 kick.
+ * K1, D, K2 are DriftKickIntegrator::kick_factor(a_begin,a_half),
+ * drift_factor(a_begin,a_end), kick_factor(a_half,a_end)
+ * (src/cosmology/drift_kick_factors.cpp:91-141), computed on the host. If the
+ * acceleration field is not valid a force solve runs first
+ * (ensure_force_at, :134-141). max_drift (may be NULL) receives
+ * max_i ||D p_half,i||, last_step_max_drift_displacement (:214-225).
+ * A non-finite K1/drift candidate publishes nothing (HYOWON_EOVERFLOW). */
+int hyowon_pm_kdk_step(hyowon_pm_t h, double K1, double D, double K2,
+                       double* max_drift);
+
+/* n_steps consecutive KDK steps with per-step factors K1[i], D[i], K2[i]
+ * (the SimulationRunner step loop, src/runtime/simulation_runner.cpp:1348-1351,
+ * without host work between steps). max_drift may be NULL or hold n_steps. */
+int hyowon_pm_run(hyowon_pm_t h, uint64_t n_steps, const double* K1, const double* D,
+                  const double* K2, double* max_drift);
+
+/* Particle count and mesh size of the handle. */
+int hyowon_pm_info(hyowon_pm_t h, uint64_t* n_particles, uint64_t* mesh_size,
+                   int* precision, int* method);
+
+/* Copies the real-space potential of the last force solve (pure PM, FP64 or
+ * FP32 widened to double, row-major (ix*N+iy)*N+iz, including the 1/N^3 of the
+ * inverse transform) to host memory phi[N^3]. Diagnostic / parity access. */
+int hyowon_pm_download_potential(hyowon_pm_t h, double* phi);
+
+/* Copies the deposited CIC mass mesh of the last force solve (mass per cell,
+ * before density normalisation; FP32_FIXED converts its fixed-point cells to
+ * mass) to host memory mesh[N^3]. */
+int hyowon_pm_download_mass_mesh(hyowon_pm_t h, double* mesh);
+
+/* Per-axis cell assignment of the device positions: base[3*n] (int64, axis-major:
+ * x block then y then z) and frac[3*n] in original particle order, computed by
+ * the same device function the sort key uses (src/mesh/cic_coordinate.hpp:95-121). */
+int hyowon_pm_cell_coords(hyowon_pm_t h, int64_t* base, double* frac);
+
+/* Device timing, measured with CUDA events on the handle's stream. When
+ * enabled, times[0] is the device time of the whole last hyowon_pm_run /
+ * kdk_step / compute_forces call, and times[1..6] the phases of its last step:
+ * sort (kick/drift, scan, scatter), deposit, forward FFT, Green, inverse FFT,
+ * gather (+K2), in milliseconds. times[7] = kernels this library launched
+ * during that call (cuFFT's own kernels excluded). times has 8 entries. */
+int hyowon_pm_set_timing(hyowon_pm_t h, int enabled);
+int hyowon_pm_last_timing(hyowon_pm_t h, double* times);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,233 @@
+"""ctypes bindings for the CPU checker libraries (TEST INFRASTRUCTURE ONLY).
+
+* ``Oracle`` wraps ``oracle/liboracle.so`` -- this repository's C restatement of
+  HYOWON's PM hot path (oracle/pm_oracle.c).
+* ``Reference`` wraps ``oracle/_ref/libhyowon_ref.so`` -- the reference's own
+  sources compiled unmodified (oracle/ref/Makefile) behind a small harness.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, as the checker. The product library never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libhyowon_ref.so")
+
+_c_double = ctypes.c_double
+_c_u64 = ctypes.c_uint64
+_c_int = ctypes.c_int
+
+
+def _dp(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], (a.dtype, a.flags)
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def build_oracle() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def build_reference(ref_root: str = "/root/reference") -> bool:
+    """Compile the reference's hot path into oracle/_ref when its tree exists."""
+    if not os.path.isdir(ref_root):
+        return os.path.exists(REF_SO)
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"),
+                    f"REF_ROOT={ref_root}"], check=True)
+    return True
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code: int, where: str, message: str = ""):
+        super().__init__(f"{where}: status {code} {message}".strip())
+        self.code = code
+
+
+class Oracle:
+    """The C restatement (oracle/pm_oracle.c)."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            build_oracle()
+        self.lib = ctypes.CDLL(path)
+        self.lib.orc_gravitational_constant.restype = ctypes.c_double
+        self.lib.orc_wrap.restype = ctypes.c_double
+        self.lib.orc_wrap.argtypes = [_c_double, _c_double]
+        self.lib.orc_minimum_image.restype = ctypes.c_double
+        self.lib.orc_minimum_image.argtypes = [_c_double, _c_double]
+
+    def _check(self, rc, where):
+        if rc != 0:
+            raise OracleError(rc, where)
+
+    def G(self) -> float:
+        return self.lib.orc_gravitational_constant()
+
+    def cic_coords(self, L, N, pos):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        base = np.zeros(pos.size, dtype=np.int64)
+        frac = np.zeros(pos.size, dtype=np.float64)
+        rc = self.lib.orc_cic_coords(_c_double(L), _c_u64(N), _c_u64(pos.size), _dp(pos),
+                                     _ip(base, ctypes.c_int64), _dp(frac))
+        self._check(rc, "orc_cic_coords")
+        return base, frac
+
+    def x_plane_bins(self, L, N, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        offsets = np.zeros(N + 1, dtype=np.uint64)
+        order = np.zeros(x.size, dtype=np.uint32)
+        rc = self.lib.orc_x_plane_bins(_c_double(L), _c_u64(N), _c_u64(x.size), _dp(x),
+                                       _ip(offsets, ctypes.c_uint64), _ip(order, ctypes.c_uint32))
+        self._check(rc, "orc_x_plane_bins")
+        return offsets, order
+
+    def deposit(self, L, N, x, y, z, masses=None, uniform_mass=1.0):
+        mesh = np.zeros(N * N * N, dtype=np.float64)
+        rc = self.lib.orc_deposit(_c_double(L), _c_u64(N), _c_u64(x.size), _dp(x), _dp(y),
+                                  _dp(z), _dp(masses), _c_double(uniform_mass), _dp(mesh))
+        self._check(rc, "orc_deposit")
+        return mesh
+
+    def potential(self, L, N, x, y, z, masses=None, uniform_mass=1.0, deconvolve=False):
+        dens = np.zeros(N * N * N, dtype=np.float64)
+        phi = np.zeros(N * N * N, dtype=np.float64)
+        rc = self.lib.orc_potential(_c_double(L), _c_u64(N), _c_int(int(deconvolve)),
+                                    _c_u64(x.size), _dp(x), _dp(y), _dp(z), _dp(masses),
+                                    _c_double(uniform_mass), _dp(dens), _dp(phi))
+        self._check(rc, "orc_potential")
+        return dens, phi
+
+    def gradient_gather_add(self, L, N, phi, x, y, z, ax, ay, az):
+        rc = self.lib.orc_gradient_gather_add(_c_double(L), _c_u64(N), _dp(phi), _c_u64(x.size),
+                                              _dp(x), _dp(y), _dp(z), _dp(ax), _dp(ay), _dp(az))
+        self._check(rc, "orc_gradient_gather_add")
+
+    def pm_forces(self, L, N, x, y, z, masses=None, uniform_mass=1.0, deconvolve=False,
+                  ax=None, ay=None, az=None):
+        n = x.size
+        ax = np.zeros(n) if ax is None else ax
+        ay = np.zeros(n) if ay is None else ay
+        az = np.zeros(n) if az is None else az
+        rc = self.lib.orc_pm_forces(_c_double(L), _c_u64(N), _c_int(int(deconvolve)), _c_u64(n),
+                                    _dp(x), _dp(y), _dp(z), _dp(masses), _c_double(uniform_mass),
+                                    _dp(ax), _dp(ay), _dp(az))
+        self._check(rc, "orc_pm_forces")
+        return ax, ay, az
+
+    def kdk_step(self, L, N, state, K1, D, K2, masses=None, uniform_mass=1.0,
+                 deconvolve=False):
+        """state: dict of float64 arrays x,y,z,px,py,pz,ax,ay,az (updated in place)."""
+        md = ctypes.c_double(0.0)
+        s = state
+        rc = self.lib.orc_kdk_step(
+            _c_double(L), _c_u64(N), _c_int(int(deconvolve)), _c_u64(s["x"].size),
+            _dp(s["x"]), _dp(s["y"]), _dp(s["z"]), _dp(s["px"]), _dp(s["py"]), _dp(s["pz"]),
+            _dp(s["ax"]), _dp(s["ay"]), _dp(s["az"]), _dp(masses), _c_double(uniform_mass),
+            _c_double(K1), _c_double(D), _c_double(K2), ctypes.byref(md))
+        self._check(rc, "orc_kdk_step")
+        return md.value
+
+
+class Reference:
+    """The reference's own compiled sources (oracle/_ref/libhyowon_ref.so)."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (oracle/ref/Makefile)")
+        self.lib = ctypes.CDLL(path)
+        self.lib.ref_last_error.restype = ctypes.c_char_p
+
+    def _check(self, rc, where):
+        if rc != 0:
+            raise OracleError(rc, where, self.lib.ref_last_error().decode())
+
+    def cic_coords(self, L, N, pos):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        base = np.zeros(pos.size, dtype=np.int64)
+        frac = np.zeros(pos.size, dtype=np.float64)
+        rc = self.lib.ref_cic_coords(_c_double(L), _c_u64(N), _c_u64(pos.size), _dp(pos),
+                                     _ip(base, ctypes.c_int64), _dp(frac))
+        self._check(rc, "ref_cic_coords")
+        return base, frac
+
+    def deposit(self, L, N, x, y, z, masses=None, uniform_mass=1.0):
+        mesh = np.zeros(N * N * N, dtype=np.float64)
+        rc = self.lib.ref_deposit(_c_double(L), _c_u64(N), _c_u64(x.size), _dp(x), _dp(y), _dp(z),
+                                  _dp(masses), _c_double(uniform_mass), _dp(mesh))
+        self._check(rc, "ref_deposit")
+        return mesh
+
+    def potential(self, L, N, x, y, z, masses=None, uniform_mass=1.0, deconvolve=False):
+        dens = np.zeros(N * N * N)
+        phi = np.zeros(N * N * N)
+        rc = self.lib.ref_potential(_c_double(L), _c_u64(N), _c_int(int(deconvolve)),
+                                    _c_u64(x.size), _dp(x), _dp(y), _dp(z), _dp(masses),
+                                    _c_double(uniform_mass), _dp(dens), _dp(phi))
+        self._check(rc, "ref_potential")
+        return dens, phi
+
+    def pm_forces(self, L, N, x, y, z, masses=None, uniform_mass=1.0, deconvolve=False,
+                  method=0, r_s=0.0, ax=None, ay=None, az=None):
+        n = x.size
+        ax = np.zeros(n) if ax is None else ax
+        ay = np.zeros(n) if ay is None else ay
+        az = np.zeros(n) if az is None else az
+        rc = self.lib.ref_pm_forces(_c_double(L), _c_u64(N), _c_int(method),
+                                    _c_int(int(deconvolve)), _c_double(r_s), _c_u64(n),
+                                    _dp(x), _dp(y), _dp(z), _dp(masses), _c_double(uniform_mass),
+                                    _dp(ax), _dp(ay), _dp(az))
+        self._check(rc, "ref_pm_forces")
+        return ax, ay, az
+
+    def schedule(self, a_start, a_final, delta_ln_a, omega_m=0.3, omega_l=0.7, max_steps=100000):
+        out = np.zeros(6 * max_steps)
+        n = ctypes.c_uint64(0)
+        rc = self.lib.ref_schedule(_c_double(omega_m), _c_double(omega_l), _c_double(a_start),
+                                   _c_double(a_final), _c_double(delta_ln_a), _c_u64(max_steps),
+                                   _dp(out), ctypes.byref(n))
+        self._check(rc, "ref_schedule")
+        return out[: 6 * n.value].reshape(n.value, 6)
+
+    def hubble(self, a, omega_m=0.3, omega_l=0.7):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        H = np.zeros_like(a)
+        rc = self.lib.ref_hubble(_c_double(omega_m), _c_double(omega_l), _c_u64(a.size), _dp(a), _dp(H))
+        self._check(rc, "ref_hubble")
+        return H
+
+    def growth(self, a, omega_m=0.3, omega_l=0.7):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        D1 = np.zeros_like(a)
+        f1 = np.zeros_like(a)
+        rc = self.lib.ref_growth(_c_double(omega_m), _c_double(omega_l), _c_u64(a.size), _dp(a),
+                                 _dp(D1), _dp(f1))
+        self._check(rc, "ref_growth")
+        return D1, f1
+
+    def kdk_run(self, L, N, state, a_start, a_final, delta_ln_a, steps, uniform_mass,
+                deconvolve=False, omega_m=0.3, omega_l=0.7):
+        """Runs `steps` KDK steps in place on state (x..pz); fills ax..az.
+        Returns (per-step max drift, seconds of the step loop)."""
+        s = state
+        md = np.zeros(max(steps, 1))
+        sec = ctypes.c_double(0.0)
+        rc = self.lib.ref_kdk_run(
+            _c_double(L), _c_u64(N), _c_int(int(deconvolve)), _c_double(omega_m),
+            _c_double(omega_l), _c_double(a_start), _c_double(a_final), _c_double(delta_ln_a),
+            _c_u64(steps), _c_u64(s["x"].size), _dp(s["x"]), _dp(s["y"]), _dp(s["z"]),
+            _dp(s["px"]), _dp(s["py"]), _dp(s["pz"]), _c_double(uniform_mass), _dp(s["ax"]),
+            _dp(s["ay"]), _dp(s["az"]), _dp(md), ctypes.byref(sec))
+        self._check(rc, "ref_kdk_run")
+        return md[:steps], sec.value

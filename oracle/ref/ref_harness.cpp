@@ -1,0 +1,296 @@
+// ref_harness.cpp -- test infrastructure. Drives the REFERENCE's own hot-path
+// classes, compiled unmodified from the reference source tree by
+// oracle/ref/Makefile, and exposes them through a small extern "C" surface so
+// that the oracle restatement (oracle/pm_oracle.c) can be pinned against them
+// and golden fixtures can be produced (tests/golden/make_golden.py). It is also
+// the "reference" CPU baseline that bench.py times.
+//
+// Every entry returns 0 on success or a nonzero code naming the reference
+// exception type that was thrown (see ref_error_code); ref_last_error() gives
+// its message. Nothing here is shipped in the product library.
+#include "cosmo_nbody/config/memory_policy.hpp"
+#include "cosmo_nbody/config/simulation_parameters.hpp"
+#include "cosmo_nbody/core/particle_store.hpp"
+#include "cosmo_nbody/cosmology/cosmology_model.hpp"
+#include "cosmo_nbody/cosmology/drift_kick_factors.hpp"
+#include "cosmo_nbody/gravity/pm_solver.hpp"
+#include "cosmo_nbody/math/density_normalization.hpp"
+#include "cosmo_nbody/mesh/fft_backend.hpp"
+#include "cosmo_nbody/mesh/green_function.hpp"
+#include "cosmo_nbody/mesh/mass_assignment.hpp"
+#include "cosmo_nbody/mesh/mesh_field.hpp"
+#include "cosmo_nbody/mesh/mesh_geometry.hpp"
+#include "cosmo_nbody/mesh/pm_force_method.hpp"
+#include "cosmo_nbody/time/leapfrog_integrator.hpp"
+#include "cosmo_nbody/time/time_stepper.hpp"
+#include "mesh/cic_coordinate.hpp"
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <optional>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace cosmo_nbody;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F&& body) {
+    try {
+        body();
+        g_last_error.clear();
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_last_error = e.what();
+        return 1;
+    } catch (const std::overflow_error& e) {
+        g_last_error = e.what();
+        return 3;
+    } catch (const std::underflow_error& e) {
+        g_last_error = e.what();
+        return 4;
+    } catch (const std::logic_error& e) {
+        g_last_error = e.what();
+        return 2;
+    } catch (const std::runtime_error& e) {
+        g_last_error = e.what();
+        return 5;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return 9;
+    }
+}
+
+std::optional<double> uniform_or_none(const double* masses, double uniform_mass) {
+    if (masses) return std::nullopt;
+    return uniform_mass;
+}
+
+std::span<const double> mass_span(const double* masses, std::uint64_t n) {
+    return masses ? std::span<const double>(masses, n) : std::span<const double>{};
+}
+
+config::CosmologyParams flat_lcdm(double omega_m, double omega_l) {
+    config::CosmologyParams p;
+    p.h = 0.7;
+    p.omega_m = omega_m;
+    p.omega_lambda = omega_l;
+    p.omega_b = 0.0;
+    p.sigma8 = 0.8;
+    p.n_s = 0.965;
+    return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_last_error.c_str(); }
+
+// Per-axis CIC cell assignment (src/mesh/cic_coordinate.hpp:95-121).
+int ref_cic_coords(double L, std::uint64_t N, std::uint64_t n, const double* pos,
+                   std::int64_t* base, double* frac) {
+    return guarded([&] {
+        mesh::MeshGeometry geom(L, N);
+        mesh::detail::CICCoordinateAxis axis(L, geom.cell_size(), N);
+        for (std::uint64_t i = 0; i < n; ++i) {
+            const auto c = axis(pos[i]);
+            base[i] = c.base;
+            frac[i] = c.fraction;
+        }
+    });
+}
+
+// CICMassAssignment::deposit (src/mesh/mass_assignment_deposit.inc:15-334).
+int ref_deposit(double L, std::uint64_t N, std::uint64_t n, const double* x,
+                const double* y, const double* z, const double* masses,
+                double uniform_mass, double* mesh_out) {
+    return guarded([&] {
+        mesh::MeshGeometry geom(L, N);
+        mesh::CICMassAssignment cic(geom, config::MemoryPolicyParams{});
+        mesh::RealField field(geom.padded_real_size());
+        cic.deposit(std::span<const double>(x, n), std::span<const double>(y, n),
+                    std::span<const double>(z, n), mass_span(masses, n),
+                    uniform_or_none(masses, uniform_mass), field);
+        std::memcpy(mesh_out, field.data(), sizeof(double) * field.size());
+    });
+}
+
+// The pure-PM potential exactly as PMSolver::compute_forces_in_place forms it
+// (src/gravity/pm_solver.cpp:649-816): deposit, density normalisation,
+// r2c, GreenFunction::apply, c2r (normalised). density_out (optional)
+// receives the normalised source, phi_out the real-space potential.
+int ref_potential(double L, std::uint64_t N, int deconvolve, std::uint64_t n,
+                  const double* x, const double* y, const double* z,
+                  const double* masses, double uniform_mass, double* density_out,
+                  double* phi_out) {
+    return guarded([&] {
+        mesh::MeshGeometry geom(L, N);
+        mesh::CICMassAssignment cic(geom, config::MemoryPolicyParams{});
+        mesh::RealField field(geom.padded_real_size());
+        cic.deposit(std::span<const double>(x, n), std::span<const double>(y, n),
+                    std::span<const double>(z, n), mass_span(masses, n),
+                    uniform_or_none(masses, uniform_mass), field);
+        double total = 0.0;
+        if (masses) {
+            for (std::uint64_t i = 0; i < n; ++i) total += masses[i];
+        } else {
+            total = uniform_mass * static_cast<double>(n);
+        }
+        const std::size_t cells = N * N * N;
+        const math::DensityNormalization norm(total, cells, geom.cell_size(),
+                                              "ref_potential");
+        if (norm.direct_available()) {
+            const double mean = norm.mean_mass_per_cell();
+            const double inv_vol = norm.inverse_cell_volume();
+            for (std::size_t i = 0; i < cells; ++i) field[i] = (field[i] - mean) * inv_vol;
+        } else {
+            for (std::size_t i = 0; i < cells; ++i) {
+                field[i] = norm.normalize(field[i], "ref_potential");
+            }
+        }
+        if (density_out) std::memcpy(density_out, field.data(), sizeof(double) * cells);
+        mesh::FFTBackend fft(geom);
+        mesh::ComplexField modes(geom.complex_size());
+        fft.forward(field, modes);
+        mesh::GreenFunction green(geom, mesh::PMForceMethod::pure_pm(deconvolve != 0));
+        green.apply(modes);
+        fft.inverse(modes, field);
+        std::memcpy(phi_out, field.data(), sizeof(double) * cells);
+    });
+}
+
+// PMSolver::compute_forces (src/gravity/pm_solver.cpp:494-567): ADDS the PM
+// acceleration to ax/ay/az. method 0 = pure PM, 1 = TreePM long range (r_s).
+int ref_pm_forces(double L, std::uint64_t N, int method, int deconvolve, double r_s,
+                  std::uint64_t n, const double* x, const double* y, const double* z,
+                  const double* masses, double uniform_mass, double* ax, double* ay,
+                  double* az) {
+    return guarded([&] {
+        mesh::MeshGeometry geom(L, N);
+        const auto pm_method = method == 0
+            ? mesh::PMForceMethod::pure_pm(deconvolve != 0)
+            : mesh::PMForceMethod::treepm_long_range(r_s);
+        gravity::PMSolver solver(geom, pm_method, false, config::MemoryPolicyParams{});
+        (void)solver.compute_forces(
+            std::span<const double>(x, n), std::span<const double>(y, n),
+            std::span<const double>(z, n), mass_span(masses, n),
+            uniform_or_none(masses, uniform_mass), std::span<double>(ax, n),
+            std::span<double>(ay, n), std::span<double>(az, n), false);
+    });
+}
+
+// TimeStepper boundaries plus DriftKickIntegrator factors per step
+// (src/time/time_stepper.cpp:194-276, src/cosmology/drift_kick_factors.cpp:91-141).
+// out6 receives, per step, {a_begin, a_half, a_end, D, K1, K2}.
+int ref_schedule(double omega_m, double omega_l, double a_start, double a_final,
+                 double delta_ln_a, std::uint64_t max_steps, double* out6,
+                 std::uint64_t* n_steps) {
+    return guarded([&] {
+        cosmology::CosmologyModel model(flat_lcdm(omega_m, omega_l));
+        cosmology::DriftKickIntegrator factors(model);
+        time::TimeStepper stepper(a_start, a_final, delta_ln_a);
+        std::uint64_t k = 0;
+        while (auto step = stepper.next_step()) {
+            if (k >= max_steps) throw std::length_error("ref_schedule: max_steps too small");
+            out6[6 * k + 0] = step->a_begin();
+            out6[6 * k + 1] = step->a_half();
+            out6[6 * k + 2] = step->a_end();
+            out6[6 * k + 3] = factors.drift_factor(step->a_begin(), step->a_end());
+            out6[6 * k + 4] = factors.kick_factor(step->a_begin(), step->a_half());
+            out6[6 * k + 5] = factors.kick_factor(step->a_half(), step->a_end());
+            ++k;
+        }
+        *n_steps = k;
+    });
+}
+
+// H(a) in km/s/(Mpc/h) (src/cosmology/cosmology_model.cpp:167-179).
+int ref_hubble(double omega_m, double omega_l, std::uint64_t n, const double* a,
+               double* H) {
+    return guarded([&] {
+        cosmology::CosmologyModel model(flat_lcdm(omega_m, omega_l));
+        for (std::uint64_t i = 0; i < n; ++i) H[i] = model.H(a[i]);
+    });
+}
+
+// Linear growth D1(a) and f1(a) (cosmology_model.hpp:47-48).
+int ref_growth(double omega_m, double omega_l, std::uint64_t n, const double* a,
+               double* D1, double* f1) {
+    return guarded([&] {
+        cosmology::CosmologyModel model(flat_lcdm(omega_m, omega_l));
+        for (std::uint64_t i = 0; i < n; ++i) {
+            D1[i] = model.D1(a[i]);
+            f1[i] = model.f1(a[i]);
+        }
+    });
+}
+
+// The production KDK loop: TimeStepper + LeapfrogIntegrator with a PMSolver
+// force callback (src/runtime/simulation_runner.cpp:1009-1143,1348-1351).
+// Runs the first `steps_to_run` steps of the schedule on the state in
+// x..pz (in/out), returns the accelerations of the last force solve, the
+// per-step maximum drift telemetry and the wall time of the step loop
+// (steady clock, excluding setup and the initial force).
+int ref_kdk_run(double L, std::uint64_t N, int deconvolve, double omega_m,
+                double omega_l, double a_start, double a_final, double delta_ln_a,
+                std::uint64_t steps_to_run, std::uint64_t n, double* x, double* y,
+                double* z, double* px, double* py, double* pz, double uniform_mass,
+                double* ax, double* ay, double* az, double* max_drift,
+                double* seconds) {
+    return guarded([&] {
+        core::ParticleStore store;
+        store.set_uniform_mass(uniform_mass);
+        store.resize(n);
+        std::memcpy(store.get_positions_x().data(), x, sizeof(double) * n);
+        std::memcpy(store.get_positions_y().data(), y, sizeof(double) * n);
+        std::memcpy(store.get_positions_z().data(), z, sizeof(double) * n);
+        std::memcpy(store.get_momenta_x().data(), px, sizeof(double) * n);
+        std::memcpy(store.get_momenta_y().data(), py, sizeof(double) * n);
+        std::memcpy(store.get_momenta_z().data(), pz, sizeof(double) * n);
+
+        cosmology::CosmologyModel model(flat_lcdm(omega_m, omega_l));
+        cosmology::DriftKickIntegrator factors(model);
+        mesh::MeshGeometry geom(L, N);
+        gravity::PMSolver solver(geom, mesh::PMForceMethod::pure_pm(deconvolve != 0),
+                                 false, config::MemoryPolicyParams{});
+        auto force = [&](std::span<const double> fx, std::span<const double> fy,
+                         std::span<const double> fz, std::span<const double> m,
+                         std::span<double> gx, std::span<double> gy,
+                         std::span<double> gz, double) {
+            (void)solver.compute_forces(fx, fy, fz, m, store.get_uniform_mass(), gx,
+                                        gy, gz, false);
+        };
+        time::LeapfrogIntegrator integrator(store, factors, force, L, 1);
+        time::TimeStepper stepper(a_start, a_final, delta_ln_a);
+        integrator.ensure_force_at(a_start);
+        const auto t0 = std::chrono::steady_clock::now();
+        std::uint64_t k = 0;
+        while (k < steps_to_run) {
+            auto step = stepper.next_step();
+            if (!step) break;
+            integrator.step(*step);
+            if (max_drift) max_drift[k] = integrator.last_step_max_drift_displacement().value_or(-1.0);
+            ++k;
+        }
+        const auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+        std::memcpy(x, store.get_positions_x().data(), sizeof(double) * n);
+        std::memcpy(y, store.get_positions_y().data(), sizeof(double) * n);
+        std::memcpy(z, store.get_positions_z().data(), sizeof(double) * n);
+        std::memcpy(px, store.get_momenta_x().data(), sizeof(double) * n);
+        std::memcpy(py, store.get_momenta_y().data(), sizeof(double) * n);
+        std::memcpy(pz, store.get_momenta_z().data(), sizeof(double) * n);
+        std::memcpy(ax, store.get_accelerations_x().data(), sizeof(double) * n);
+        std::memcpy(ay, store.get_accelerations_y().data(), sizeof(double) * n);
+        std::memcpy(az, store.get_accelerations_z().data(), sizeof(double) * n);
+    });
+}
+
+}  // extern "C"
