@@ -73,6 +73,7 @@ _SIGS = {
     "hyowon_pm_download_mass_mesh": (c_int, [c_void_p, P_double]),
     "hyowon_pm_cell_coords": (c_int, [c_void_p, P_i64, P_double]),
     "hyowon_pm_set_timing": (c_int, [c_void_p, c_int]),
+    "hyowon_pm_set_sort_interval": (c_int, [c_void_p, c_int]),
     "hyowon_pm_last_timing": (c_int, [c_void_p, P_double]),
     "hyowon_hubble": (c_int, [c_double, c_double, c_u64, P_double, P_double]),
     "hyowon_drift_factor": (c_int, [c_double, c_double, c_double, c_double, P_double]),

@@ -74,7 +74,9 @@ __device__ __forceinline__ bool cic_coord_f64(double pos, const Axis& a, int& ba
     const double fl = floor(s);
     const int b = static_cast<int>(fl);
     if (b < 0 || b >= a.N) return false;
-    const double f = s - fl;
+    // frac = scaled - (double)base, as the reference forms it: for scaled = -0.0
+    // this keeps the sign (-0.0 - +0.0), which `s - floor(s)` would not.
+    const double f = s - static_cast<double>(b);
     if (!(f >= 0.0 && f < 1.0)) return false;
     base = b;
     frac = f;

@@ -1,43 +1,942 @@
 // pm_fp32.cu -- precision form of the PM step (see pm_fp32.h).
+//
+// Per particle: u32 fixed-point position per axis (x = u L / 2^32), FP32
+// momentum and acceleration. The cell of u on an N mesh is (u*N) >> 32 and the
+// CIC fraction is the low word of u*N, so cell assignment needs no division and
+// the periodic wrap of the drift is the natural wrap of 32-bit integers.
+//
+// Deposit: each particle adds the exact integer weights
+// w = wx*wy*wz, wx in {2^B - f, f} with f the top B bits of the fraction, to
+// int64 cells that start at -mean (the deposit is an offset from the mean cell
+// mass). Integer addition is associative, so the mesh is bit-identical run to
+// run whatever order the atomics land in, and the mesh sum equals
+// n 2^(3B) - mean*N^3 exactly (checked every step). B <= 16 is chosen per step
+// on the device from the densest sort bucket so that no cell can overflow.
+//
+// The int64 offsets are converted to FP32 for cuFFT R2C, the Green's function
+// (with the density normalisation and the 1/N^3 folded into one constant) is
+// applied in FP32, C2R gives the FP32 potential, and the centred-gradient gather
+// + K2 kick run in FP32. Only the drift p*D and its rounding into the
+// fixed-point position are FP64.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "hyowon_pm.h"
 #include "pm_fp32.h"
+#include "pm_kernels.h"
 
 namespace hyowon::fp32 {
 
-struct State {
-    std::string err = "the FP32 fixed-point form is not available in this build";
+namespace {
+
+constexpr int kThreads = 256;
+constexpr double kTwo32 = 4294967296.0;
+
+inline unsigned blocks_for(uint64_t n, int t = kThreads) {
+    return static_cast<unsigned>((n + t - 1) / t);
+}
+
+struct FixedPlan {
+    int B;                 // fraction bits per axis of the deposit weights
+    int pad;
+    long long mean_q;      // floor(n 2^(3B) / N^3)
+    unsigned long long residual;  // n 2^(3B) - mean_q N^3 (the exact mesh sum)
+    float c_green;         // 4 pi G m / dx^3 / N^3 * 2^(-3B)
+    float pad2;
 };
 
-int create(State** out, double, int, int, int, double, const double*, const double*, double,
-           cudaStream_t) {
-    *out = new State();
-    return HYOWON_EINVAL;
+__device__ __forceinline__ uint32_t cell_of(uint32_t u, int N, uint32_t& frac) {
+    const unsigned long long p = static_cast<unsigned long long>(u) * static_cast<unsigned>(N);
+    frac = static_cast<uint32_t>(p);
+    return static_cast<uint32_t>(p >> 32);
 }
-void destroy(State* st) { delete st; }
+
+__device__ __forceinline__ uint32_t cell_index(uint32_t ix, uint32_t iy, uint32_t iz, int N) {
+    return (ix * static_cast<uint32_t>(N) + iy) * static_cast<uint32_t>(N) + iz;
+}
+
+__device__ __forceinline__ uint32_t to_fixed(double x, double L, bool& ok) {
+    const double w = wrap_f64(x, L);
+    ok = isfinite(w) && w >= 0.0 && w < L;
+    if (!ok) return 0u;
+    double t = floor(w / L * kTwo32);
+    if (t >= kTwo32) t = kTwo32 - 1.0;
+    if (t < 0.0) t = 0.0;
+    return static_cast<uint32_t>(t);
+}
+
+__global__ void k_to_fixed(uint32_t n, const double* __restrict__ x, const double* __restrict__ y,
+                           const double* __restrict__ z, const double* __restrict__ px,
+                           const double* __restrict__ py, const double* __restrict__ pz,
+                           double L, uint32_t* __restrict__ ux, uint32_t* __restrict__ uy,
+                           uint32_t* __restrict__ uz, float* __restrict__ fx,
+                           float* __restrict__ fy, float* __restrict__ fz,
+                           unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool a, b, c;
+    ux[i] = to_fixed(x[i], L, a);
+    uy[i] = to_fixed(y[i], L, b);
+    uz[i] = to_fixed(z[i], L, c);
+    const double qx = px ? px[i] : 0.0, qy = py ? py[i] : 0.0, qz = pz ? pz[i] : 0.0;
+    if (!(a && b && c) || !isfinite(qx) || !isfinite(qy) || !isfinite(qz))
+        raise_status(status, ST_NONFINITE_INPUT);
+    fx[i] = static_cast<float>(qx);
+    fy[i] = static_cast<float>(qy);
+    fz[i] = static_cast<float>(qz);
+}
+
+__global__ void k_key(uint32_t n, const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy,
+                      const uint32_t* __restrict__ uz, int N, int shift,
+                      uint32_t* __restrict__ key, uint32_t* __restrict__ rank,
+                      uint32_t* __restrict__ count, uint32_t* max_count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t f;
+    const uint32_t b = cell_index(cell_of(ux[i], N, f), cell_of(uy[i], N, f), cell_of(uz[i], N, f), N)
+        >> shift;
+    key[i] = b;
+    rank[i] = atomicAdd(&count[b], 1u);
+}
+
+// K1 kick (FP32) + drift (FP64 increment rounded once into the fixed point).
+__global__ void k_kick_drift_key(uint32_t n, const uint32_t* __restrict__ ux,
+                                 const uint32_t* __restrict__ uy, const uint32_t* __restrict__ uz,
+                                 const float* __restrict__ px, const float* __restrict__ py,
+                                 const float* __restrict__ pz, const float* __restrict__ ax,
+                                 const float* __restrict__ ay, const float* __restrict__ az,
+                                 float K1, double D, double to_units, int N,
+                                 uint32_t* __restrict__ uxo, uint32_t* __restrict__ uyo,
+                                 uint32_t* __restrict__ uzo, float* __restrict__ pxo,
+                                 float* __restrict__ pyo, float* __restrict__ pzo, int shift,
+                                 int with_rank, uint32_t* __restrict__ key,
+                                 uint32_t* __restrict__ rank, uint32_t* __restrict__ count,
+                                 uint32_t* max_count, unsigned long long* max_drift_bits,
+                                 unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double drift_norm = 0.0;
+    if (i < n) {
+        const float qx = fmaf(ax[i], K1, px[i]);
+        const float qy = fmaf(ay[i], K1, py[i]);
+        const float qz = fmaf(az[i], K1, pz[i]);
+        const double dx = static_cast<double>(qx) * D;
+        const double dy = static_cast<double>(qy) * D;
+        const double dz = static_cast<double>(qz) * D;
+        const double sx = dx * to_units, sy = dy * to_units, sz = dz * to_units;
+        const double lim = 4.0e18;
+        const bool ok = isfinite(qx) && isfinite(qy) && isfinite(qz) && fabs(sx) < lim
+            && fabs(sy) < lim && fabs(sz) < lim;
+        uint32_t nx = ux[i], ny = uy[i], nz = uz[i];
+        if (ok) {
+            nx += static_cast<uint32_t>(static_cast<unsigned long long>(__double2ll_rn(sx)));
+            ny += static_cast<uint32_t>(static_cast<unsigned long long>(__double2ll_rn(sy)));
+            nz += static_cast<uint32_t>(static_cast<unsigned long long>(__double2ll_rn(sz)));
+            drift_norm = hypot(hypot(dx, dy), dz);
+        } else {
+            raise_status(status, ST_KICK_DRIFT);
+        }
+        uxo[i] = nx;
+        uyo[i] = ny;
+        uzo[i] = nz;
+        pxo[i] = qx;
+        pyo[i] = qy;
+        pzo[i] = qz;
+        uint32_t f;
+        const uint32_t b = cell_index(cell_of(nx, N, f), cell_of(ny, N, f), cell_of(nz, N, f), N)
+            >> shift;
+        if (with_rank) {
+            key[i] = b;
+            const uint32_t r = atomicAdd(&count[b], 1u);
+            rank[i] = r;
+        } else {
+            atomicAdd(&count[b], 1u);  // occupancy only: bounds the deposit weights
+        }
+    }
+    unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(drift_norm));
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+        bits = other > bits ? other : bits;
+    }
+    if ((threadIdx.x & 31) == 0 && bits != 0ull) atomicMax(max_drift_bits, bits);
+}
+
+__global__ void k_max_count(uint32_t nb, const uint32_t* __restrict__ count, uint32_t* max_count) {
+    uint32_t m = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+        m = max(m, count[i]);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(max_count, m);
+}
+
+// Chooses the deposit fraction bits B for this step: the largest B <= 16 with
+// 8 * max_bucket * 2^(3B) <= 2^63 - 1, so no cell (fed by at most 8 buckets'
+// particles) can overflow; then the mean offset and the Green constant.
+__global__ void k_plan(uint32_t n, uint64_t cells, const uint32_t* max_count, double c0,
+                       int centre, FixedPlan* plan) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const unsigned long long mc = *max_count > 0 ? *max_count : 1u;
+    int B = 16;
+    while (B > 4) {
+        const unsigned __int128 worst =
+            static_cast<unsigned __int128>(8ull * mc) << (3 * B);
+        if (worst <= static_cast<unsigned __int128>(0x7fffffffffffffffull)) break;
+        --B;
+    }
+    const unsigned __int128 total = static_cast<unsigned __int128>(n) << (3 * B);
+    const unsigned long long mean = centre ? static_cast<unsigned long long>(total / cells) : 0ull;
+    plan->B = B;
+    plan->mean_q = static_cast<long long>(mean);
+    plan->residual = static_cast<unsigned long long>(total - static_cast<unsigned __int128>(mean) * cells);
+    plan->c_green = static_cast<float>(ldexp(c0, -3 * B));
+}
+
+__global__ void k_fill(uint64_t cells, long long* __restrict__ q, const FixedPlan* plan) {
+    const long long v = -plan->mean_q;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cells;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        q[i] = v;
+}
+
+__global__ void k_deposit(uint32_t n, const uint32_t* __restrict__ ux,
+                          const uint32_t* __restrict__ uy, const uint32_t* __restrict__ uz, int N,
+                          unsigned long long* __restrict__ q, const FixedPlan* plan,
+                          const unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+    const int B = plan->B;
+    const unsigned one = 1u << B;
+    uint32_t fx, fy, fz;
+    const uint32_t ix = cell_of(ux[i], N, fx);
+    const uint32_t iy = cell_of(uy[i], N, fy);
+    const uint32_t iz = cell_of(uz[i], N, fz);
+    fx >>= (32 - B);
+    fy >>= (32 - B);
+    fz >>= (32 - B);
+    const unsigned long long wx[2] = {one - fx, fx};
+    const unsigned long long wy[2] = {one - fy, fy};
+    const unsigned long long wz[2] = {one - fz, fz};
+    const uint32_t gx[2] = {ix, ix + 1 == static_cast<uint32_t>(N) ? 0u : ix + 1};
+    const uint32_t gy[2] = {iy, iy + 1 == static_cast<uint32_t>(N) ? 0u : iy + 1};
+    const uint32_t gz[2] = {iz, iz + 1 == static_cast<uint32_t>(N) ? 0u : iz + 1};
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const unsigned long long wab = wx[a] * wy[b];
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const unsigned long long w = wab * wz[c];
+                if (w) atomicAdd(&q[cell_index(gx[a], gy[b], gz[c], N)], w);
+            }
+        }
+    }
+}
+
+// int64 offsets -> FP32 real mesh, with the exact (modular) mesh-sum check.
+__global__ void k_convert(uint64_t cells, const long long* __restrict__ q, float* __restrict__ r,
+                          unsigned long long* qsum) {
+    unsigned long long local = 0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cells;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const long long v = q[i];
+        r[i] = __ll2float_rn(v);
+        local += static_cast<unsigned long long>(v);
+    }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(qsum, local);
+}
+
+__global__ void k_check_mass(const unsigned long long* qsum, const FixedPlan* plan,
+                             unsigned int* status) {
+    if (threadIdx.x == 0 && *qsum != plan->residual) raise_status(status, ST_MASS);
+}
+
+__global__ void k_green(int N, float2* __restrict__ modes, const float* __restrict__ lap,
+                        const float* __restrict__ win, int deconvolve, const FixedPlan* plan) {
+    const int Hz = N / 2 + 1;
+    const uint64_t total = static_cast<uint64_t>(N) * N * Hz;
+    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    if (idx == 0) {
+        modes[0] = make_float2(0.f, 0.f);
+        return;
+    }
+    const int iz = static_cast<int>(idx % Hz);
+    const uint64_t t = idx / Hz;
+    const int iy = static_cast<int>(t % N);
+    const int ix = static_cast<int>(t / N);
+    float f = plan->c_green / (lap[ix] + lap[iy] + lap[iz]);
+    if (deconvolve) {
+        const float wt = win[ix] * win[iy] * win[iz];
+        f /= wt * wt;
+    }
+    float2 v = modes[idx];
+    v.x *= f;
+    v.y *= f;
+    modes[idx] = v;
+}
+
+__global__ void k_green_spectral(int N, double L, float2* __restrict__ modes,
+                                 const float* __restrict__ win, float r_s, const FixedPlan* plan) {
+    const int Hz = N / 2 + 1;
+    const uint64_t total = static_cast<uint64_t>(N) * N * Hz;
+    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    if (idx == 0) {
+        modes[0] = make_float2(0.f, 0.f);
+        return;
+    }
+    const int iz = static_cast<int>(idx % Hz);
+    const uint64_t t = idx / Hz;
+    const int iy = static_cast<int>(t % N);
+    const int ix = static_cast<int>(t / N);
+    const float kf = static_cast<float>(2.0 * 3.141592653589793 / L);
+    const float kx = kf * static_cast<float>(ix <= N / 2 ? ix : ix - N);
+    const float ky = kf * static_cast<float>(iy <= N / 2 ? iy : iy - N);
+    const float kz = kf * static_cast<float>(iz);
+    const float k2 = kx * kx + ky * ky + kz * kz;
+    const float wt = win[ix] * win[iy] * win[iz];
+    const float f = -plan->c_green / k2 * expf(-k2 * r_s * r_s) / (wt * wt);
+    float2 v = modes[idx];
+    v.x *= f;
+    v.y *= f;
+    modes[idx] = v;
+}
+
+__global__ void k_spectral_axis(int N, double L, int axis, const float2* __restrict__ phi,
+                                float2* __restrict__ out) {
+    const int Hz = N / 2 + 1;
+    const uint64_t total = static_cast<uint64_t>(N) * N * Hz;
+    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int iz = static_cast<int>(idx % Hz);
+    const uint64_t t = idx / Hz;
+    const int iy = static_cast<int>(t % N);
+    const int ix = static_cast<int>(t / N);
+    const int i = axis == 0 ? ix : (axis == 1 ? iy : iz);
+    float k = 0.f;
+    if (!(N % 2 == 0 && i == N / 2))
+        k = static_cast<float>(2.0 * 3.141592653589793 / L) * static_cast<float>(i <= N / 2 ? i : i - N);
+    const float2 p = phi[idx];
+    out[idx] = make_float2(p.y * k, -p.x * k);
+}
+
+__global__ void k_interp_add(uint32_t n, const float* __restrict__ field,
+                             const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy,
+                             const uint32_t* __restrict__ uz, int N, float* __restrict__ out,
+                             const unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+    uint32_t fx, fy, fz;
+    const uint32_t ix = cell_of(ux[i], N, fx), iy = cell_of(uy[i], N, fy), iz = cell_of(uz[i], N, fz);
+    const float tx = __uint2float_rn(fx) * 2.3283064365386963e-10f;
+    const float ty = __uint2float_rn(fy) * 2.3283064365386963e-10f;
+    const float tz = __uint2float_rn(fz) * 2.3283064365386963e-10f;
+    const float wx[2] = {1.f - tx, tx}, wy[2] = {1.f - ty, ty}, wz[2] = {1.f - tz, tz};
+    const uint32_t gx[2] = {ix, ix + 1 == static_cast<uint32_t>(N) ? 0u : ix + 1};
+    const uint32_t gy[2] = {iy, iy + 1 == static_cast<uint32_t>(N) ? 0u : iy + 1};
+    const uint32_t gz[2] = {iz, iz + 1 == static_cast<uint32_t>(N) ? 0u : iz + 1};
+    float s = 0.f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                s += __ldg(&field[cell_index(gx[a], gy[b], gz[c], N)]) * (wx[a] * wy[b] * wz[c]);
+    out[i] += s;
+}
+
+// Centred-gradient CIC gather (FP32) fused with the K2 kick.
+__global__ void __launch_bounds__(kThreads)
+k_gather_kick(uint32_t n, const float* __restrict__ phi, const uint32_t* __restrict__ ux,
+              const uint32_t* __restrict__ uy, const uint32_t* __restrict__ uz,
+              const float* __restrict__ px, const float* __restrict__ py,
+              const float* __restrict__ pz, float* __restrict__ ax, float* __restrict__ ay,
+              float* __restrict__ az, int do_kick, float K2, float* __restrict__ pxo,
+              float* __restrict__ pyo, float* __restrict__ pzo, int N, float inv_two_dx,
+              unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+    uint32_t fx, fy, fz;
+    const int ix = static_cast<int>(cell_of(ux[i], N, fx));
+    const int iy = static_cast<int>(cell_of(uy[i], N, fy));
+    const int iz = static_cast<int>(cell_of(uz[i], N, fz));
+    const int xs[4] = {ix == 0 ? N - 1 : ix - 1, ix, ix + 1 == N ? 0 : ix + 1,
+                       ix + 2 >= N ? ix + 2 - N : ix + 2};
+    const int ys[4] = {iy == 0 ? N - 1 : iy - 1, iy, iy + 1 == N ? 0 : iy + 1,
+                       iy + 2 >= N ? iy + 2 - N : iy + 2};
+    const int zs[4] = {iz == 0 ? N - 1 : iz - 1, iz, iz + 1 == N ? 0 : iz + 1,
+                       iz + 2 >= N ? iz + 2 - N : iz + 2};
+#define PHI(a_, b_, c_) __ldg(&phi[cell_index(xs[a_], ys[b_], zs[c_], N)])
+    float c[2][2][2], xm[2][2], xp[2][2], ym[2][2], yp[2][2], zm[2][2], zp[2][2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            xm[u][v] = PHI(0, u + 1, v + 1);
+            xp[u][v] = PHI(3, u + 1, v + 1);
+            ym[u][v] = PHI(u + 1, 0, v + 1);
+            yp[u][v] = PHI(u + 1, 3, v + 1);
+            zm[u][v] = PHI(u + 1, v + 1, 0);
+            zp[u][v] = PHI(u + 1, v + 1, 3);
+#pragma unroll
+            for (int w = 0; w < 2; ++w) c[u][v][w] = PHI(u + 1, v + 1, w + 1);
+        }
+    }
+#undef PHI
+    const float tx = __uint2float_rn(fx) * 2.3283064365386963e-10f;
+    const float ty = __uint2float_rn(fy) * 2.3283064365386963e-10f;
+    const float tz = __uint2float_rn(fz) * 2.3283064365386963e-10f;
+    const float wx[2] = {1.f - tx, tx}, wy[2] = {1.f - ty, ty}, wz[2] = {1.f - tz, tz};
+    float gxs = 0.f, gys = 0.f, gzs = 0.f;
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox) {
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy) {
+#pragma unroll
+            for (int oz = 0; oz < 2; ++oz) {
+                const float w = wx[ox] * wy[oy] * wz[oz];
+                const float dxv = (ox == 0 ? c[1][oy][oz] : xp[oy][oz])
+                    - (ox == 0 ? xm[oy][oz] : c[0][oy][oz]);
+                const float dyv = (oy == 0 ? c[ox][1][oz] : yp[ox][oz])
+                    - (oy == 0 ? ym[ox][oz] : c[ox][0][oz]);
+                const float dzv = (oz == 0 ? c[ox][oy][1] : zp[ox][oy])
+                    - (oz == 0 ? zm[ox][oy] : c[ox][oy][0]);
+                gxs -= w * dxv;
+                gys -= w * dyv;
+                gzs -= w * dzv;
+            }
+        }
+    }
+    const float gx = gxs * inv_two_dx, gy = gys * inv_two_dx, gz = gzs * inv_two_dx;
+    if (!(isfinite(gx) && isfinite(gy) && isfinite(gz))) raise_status(status, ST_FORCE);
+    ax[i] = gx;
+    ay[i] = gy;
+    az[i] = gz;
+    if (do_kick) {
+        const float qx = fmaf(gx, K2, px[i]);
+        const float qy = fmaf(gy, K2, py[i]);
+        const float qz = fmaf(gz, K2, pz[i]);
+        if (!(isfinite(qx) && isfinite(qy) && isfinite(qz))) raise_status(status, ST_KICK2);
+        pxo[i] = qx;
+        pyo[i] = qy;
+        pzo[i] = qz;
+    }
+}
+
+__global__ void k_kick_only(uint32_t n, const float* __restrict__ px, const float* __restrict__ py,
+                            const float* __restrict__ pz, const float* __restrict__ ax,
+                            const float* __restrict__ ay, const float* __restrict__ az, float K2,
+                            float* __restrict__ pxo, float* __restrict__ pyo,
+                            float* __restrict__ pzo, unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+    const float qx = fmaf(ax[i], K2, px[i]);
+    const float qy = fmaf(ay[i], K2, py[i]);
+    const float qz = fmaf(az[i], K2, pz[i]);
+    if (!(isfinite(qx) && isfinite(qy) && isfinite(qz))) raise_status(status, ST_KICK2);
+    pxo[i] = qx;
+    pyo[i] = qy;
+    pzo[i] = qz;
+}
+
+template <typename T>
+__global__ void k_unpermute_widen(uint32_t n, const uint32_t* __restrict__ id,
+                                  const T* __restrict__ src, double scale,
+                                  double* __restrict__ dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[id[i]] = static_cast<double>(src[i]) * scale;
+}
+
+__global__ void k_widen_mesh(uint64_t cells, const float* __restrict__ r, double* __restrict__ d) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cells;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        d[i] = static_cast<double>(r[i]);
+}
+
+__global__ void k_mass_mesh(uint64_t cells, const long long* __restrict__ q, const FixedPlan* plan,
+                            double m, double* __restrict__ d) {
+    const double s = ldexp(m, -3 * plan->B);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cells;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        d[i] = static_cast<double>(q[i]) * s;
+}
+
+}  // namespace
+
+struct State {
+    double L = 0.0;
+    int N = 0;
+    int method = 0;
+    int deconvolve = 0;
+    double r_s = 0.0;
+    double four_pi_G = 0.0;
+    uint32_t n = 0, cap = 0;
+    uint32_t* pos[2][3] = {};
+    float* mom[2][3] = {};
+    uint32_t* id[2] = {};
+    float* acc[3] = {};
+    int pc = 0, mc = 0, ic = 0;
+    int ic_before = 0;
+    double uniform_mass = 0.0;
+    double input_mass = 0.0;
+    SortWork sort{};
+    uint32_t sort_cap = 0;
+    uint32_t* d_max_count = nullptr;
+    FixedPlan* d_plan = nullptr;
+    unsigned long long* d_qsum = nullptr;
+    long long* qmesh = nullptr;
+    float* rmesh = nullptr;
+    float2* modes = nullptr;
+    float2* phi_k = nullptr;
+    float* lap = nullptr;
+    float* win = nullptr;
+    cufftHandle r2c = 0, c2r = 0;
+    bool plans = false;
+    void* fft_work = nullptr;
+    unsigned fill_blocks = 0;
+    int sort_interval = 4;
+    int since_sort = 0;
+    int step_P = 0, step_M = 0;  // position / momentum sets of the step in flight
+    bool step_sorted = false;
+    std::string err;
+};
+
+namespace {
+
+int fail(State* st, int code, const std::string& m) {
+    st->err = m;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(st, e_ == cudaErrorMemoryAllocation ? HYOWON_ENOMEM : HYOWON_ECUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));              \
+    } while (0)
+
+#define CKFFT(call)                                                                     \
+    do {                                                                                \
+        if ((call) != CUFFT_SUCCESS) return fail(st, HYOWON_ECUDA, std::string(#call)); \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    *p = nullptr;
+    return cudaMalloc(reinterpret_cast<void**>(p), (count ? count : 1) * sizeof(T));
+}
+
+void free_particles(State* st) {
+    for (int s = 0; s < 2; ++s) {
+        for (int a = 0; a < 3; ++a) {
+            cudaFree(st->pos[s][a]);
+            cudaFree(st->mom[s][a]);
+            st->pos[s][a] = nullptr;
+            st->mom[s][a] = nullptr;
+        }
+        cudaFree(st->id[s]);
+        st->id[s] = nullptr;
+    }
+    for (int a = 0; a < 3; ++a) {
+        cudaFree(st->acc[a]);
+        st->acc[a] = nullptr;
+    }
+    cudaFree(st->sort.key);
+    cudaFree(st->sort.rank);
+    st->sort.key = st->sort.rank = nullptr;
+    st->cap = 0;
+}
+
+int ensure(State* st, uint32_t n) {
+    if (n > st->cap) {
+        free_particles(st);
+        for (int s = 0; s < 2; ++s) {
+            for (int a = 0; a < 3; ++a) {
+                CK(dalloc(&st->pos[s][a], n));
+                CK(dalloc(&st->mom[s][a], n));
+            }
+            CK(dalloc(&st->id[s], n));
+        }
+        for (int a = 0; a < 3; ++a) CK(dalloc(&st->acc[a], n));
+        CK(dalloc(&st->sort.key, n));
+        CK(dalloc(&st->sort.rank, n));
+        st->cap = n;
+    }
+    const uint64_t cells = static_cast<uint64_t>(st->N) * st->N * st->N;
+    int shift = 0;
+    while (shift < 30 && (cells >> (shift + 1)) * 8 >= n && (cells >> (shift + 1)) > 0) ++shift;
+    const uint32_t nb = static_cast<uint32_t>((cells + (1ull << shift) - 1) >> shift);
+    st->sort.shift = shift;
+    st->sort.n_buckets = nb;
+    if (nb > st->sort_cap) {
+        cudaFree(st->sort.count);
+        cudaFree(st->sort.offset);
+        cudaFree(st->sort.scan_tmp);
+        CK(dalloc(&st->sort.count, nb + 1));
+        CK(dalloc(&st->sort.offset, nb + 1));
+        CK(dalloc(&st->sort.scan_tmp, scan_tmp_elements(nb + 1)));
+        st->sort_cap = nb;
+    }
+    return HYOWON_OK;
+}
+
+void rec(cudaEvent_t* ev, int i, cudaStream_t s) {
+    if (ev) cudaEventRecord(ev[i], s);
+}
+
+double green_c0(const State* st) {
+    const double dx = st->L / st->N;
+    const double n3 = static_cast<double>(st->N) * st->N * st->N;
+    return st->four_pi_G * st->uniform_mass / (dx * dx * dx) / n3;
+}
+
+}  // namespace
+
+int create(State** out, double L, int N, int method, int deconvolve, double r_s,
+           const double* lap, const double* win, double four_pi_G, cudaStream_t s) {
+    State* st = new State();
+    *out = st;
+    st->L = L;
+    st->N = N;
+    st->method = method;
+    st->deconvolve = deconvolve;
+    st->r_s = r_s;
+    st->four_pi_G = four_pi_G;
+    const size_t cells = static_cast<size_t>(N) * N * N;
+    const size_t half = static_cast<size_t>(N) * N * (N / 2 + 1);
+    CK(dalloc(&st->qmesh, cells));
+    CK(dalloc(&st->rmesh, cells));
+    CK(dalloc(&st->modes, half));
+    if (method == HYOWON_TREEPM_LONG_RANGE) CK(dalloc(&st->phi_k, half));
+    CK(dalloc(&st->lap, N));
+    CK(dalloc(&st->win, N));
+    CK(dalloc(&st->d_max_count, 1));
+    CK(dalloc(&st->d_plan, 1));
+    CK(dalloc(&st->d_qsum, 1));
+    std::vector<float> lf(N), wf(N);
+    for (int i = 0; i < N; ++i) {
+        lf[i] = static_cast<float>(lap[i]);
+        wf[i] = static_cast<float>(win[i]);
+    }
+    CK(cudaMemcpy(st->lap, lf.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(st->win, wf.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+    CKFFT(cufftCreate(&st->r2c));
+    CKFFT(cufftCreate(&st->c2r));
+    st->plans = true;
+    cufftSetAutoAllocation(st->r2c, 0);
+    cufftSetAutoAllocation(st->c2r, 0);
+    size_t w1 = 0, w2 = 0;
+    CKFFT(cufftMakePlan3d(st->r2c, N, N, N, CUFFT_R2C, &w1));
+    CKFFT(cufftMakePlan3d(st->c2r, N, N, N, CUFFT_C2R, &w2));
+    CK(cudaMalloc(&st->fft_work, std::max<size_t>(1, std::max(w1, w2))));
+    cufftSetWorkArea(st->r2c, st->fft_work);
+    cufftSetWorkArea(st->c2r, st->fft_work);
+    cufftSetStream(st->r2c, s);
+    cufftSetStream(st->c2r, s);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    st->fill_blocks = static_cast<unsigned>(sms) * 8;
+    return HYOWON_OK;
+}
+
+void destroy(State* st) {
+    if (!st) return;
+    if (st->plans) {
+        cufftDestroy(st->r2c);
+        cufftDestroy(st->c2r);
+    }
+    cudaFree(st->fft_work);
+    cudaFree(st->qmesh);
+    cudaFree(st->rmesh);
+    cudaFree(st->modes);
+    cudaFree(st->phi_k);
+    cudaFree(st->lap);
+    cudaFree(st->win);
+    cudaFree(st->d_max_count);
+    cudaFree(st->d_plan);
+    cudaFree(st->d_qsum);
+    free_particles(st);
+    cudaFree(st->sort.count);
+    cudaFree(st->sort.offset);
+    cudaFree(st->sort.scan_tmp);
+    delete st;
+}
+
 const std::string& last_error(State* st) { return st->err; }
-int upload(State*, uint32_t, const double*, const double*, const double*, const double*,
-           const double*, const double*, const double*, double, double, double, cudaStream_t) {
-    return HYOWON_EINVAL;
+
+int upload_device(State* st, uint32_t n, double* const pos[3], double* const mom[3],
+                  double uniform_mass, double total_mass, double, cudaStream_t s) {
+    int rc = ensure(st, n);
+    if (rc) return rc;
+    st->n = n;
+    st->uniform_mass = uniform_mass;
+    st->input_mass = total_mass;
+    st->pc = st->mc = st->ic = 0;
+    unsigned int* d_status = nullptr;
+    CK(dalloc(&d_status, 1));
+    cudaMemsetAsync(d_status, 0, sizeof(unsigned int), s);
+    k_to_fixed<<<blocks_for(n), kThreads, 0, s>>>(n, pos[0], pos[1], pos[2], mom[0], mom[1], mom[2],
+                                                  st->L, st->pos[0][0], st->pos[0][1], st->pos[0][2],
+                                                  st->mom[0][0], st->mom[0][1], st->mom[0][2], d_status);
+    launch_iota_u32(n, st->id[0], s);
+    unsigned int h = 0;
+    cudaMemcpyAsync(&h, d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    cudaFree(d_status);
+    if (e != cudaSuccess) return fail(st, HYOWON_ECUDA, cudaGetErrorString(e));
+    if (h) return fail(st, HYOWON_EINVAL, "particle positions and momenta must be finite");
+    return HYOWON_OK;
 }
-int upload_device(State*, uint32_t, double* const*, double* const*, double, double, double,
-                  cudaStream_t) {
-    return HYOWON_EINVAL;
+
+int upload(State* st, uint32_t n, const double* x, const double* y, const double* z,
+           const double* px, const double* py, const double* pz, const double* masses,
+           double uniform_mass, double total_mass, double mass_tol, cudaStream_t s) {
+    if (masses) return fail(st, HYOWON_EINVAL, "the FP32 fixed-point form requires a uniform particle mass");
+    double* tmp[6] = {};
+    const double* src[6] = {x, y, z, px, py, pz};
+    int rc = HYOWON_OK;
+    for (int a = 0; a < 6 && rc == HYOWON_OK; ++a) {
+        if (!src[a]) continue;
+        if (dalloc(&tmp[a], n) != cudaSuccess
+            || cudaMemcpyAsync(tmp[a], src[a], sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            rc = fail(st, HYOWON_ENOMEM, "staging allocation failed");
+    }
+    if (rc == HYOWON_OK) {
+        double* const p3[3] = {tmp[0], tmp[1], tmp[2]};
+        double* const m3[3] = {tmp[3], tmp[4], tmp[5]};
+        rc = upload_device(st, n, p3, m3, uniform_mass, total_mass, mass_tol, s);
+    }
+    for (auto* t : tmp) cudaFree(t);
+    return rc;
 }
+
 void validate(State*, cudaStream_t, unsigned int*) {}
-int sort_current(State*, cudaStream_t, unsigned int*) { return HYOWON_EINVAL; }
-int enqueue_force(State*, cudaStream_t, unsigned int*, bool, double, cudaEvent_t*) {
-    return HYOWON_EINVAL;
+
+int sort_current(State* st, cudaStream_t s, unsigned int* d_status) {
+    const uint32_t n = st->n;
+    CK(cudaMemsetAsync(st->sort.count, 0, sizeof(uint32_t) * (st->sort.n_buckets + 1), s));
+    CK(cudaMemsetAsync(st->d_max_count, 0, sizeof(uint32_t), s));
+    k_key<<<blocks_for(n), kThreads, 0, s>>>(n, st->pos[st->pc][0], st->pos[st->pc][1],
+                                             st->pos[st->pc][2], st->N, st->sort.shift, st->sort.key,
+                                             st->sort.rank, st->sort.count, st->d_max_count);
+    k_max_count<<<st->fill_blocks, kThreads, 0, s>>>(st->sort.n_buckets, st->sort.count,
+                                                     st->d_max_count);
+    launch_exclusive_scan(st->sort.count, st->sort.offset, st->sort.n_buckets + 1,
+                          st->sort.scan_tmp, s);
+    const uint32_t* src[7];
+    uint32_t* dst[7];
+    for (int a = 0; a < 3; ++a) {
+        src[a] = st->pos[st->pc][a];
+        dst[a] = st->pos[1 - st->pc][a];
+        src[3 + a] = reinterpret_cast<const uint32_t*>(st->mom[st->mc][a]);
+        dst[3 + a] = reinterpret_cast<uint32_t*>(st->mom[1 - st->mc][a]);
+    }
+    src[6] = st->id[st->ic];
+    dst[6] = st->id[1 - st->ic];
+    launch_scatter4_multi(n, st->sort.key, st->sort.rank, st->sort.offset, 7, src, dst, nullptr, s);
+    CK(cudaStreamSynchronize(s));
+    (void)d_status;
+    st->pc = 1 - st->pc;
+    st->mc = 1 - st->mc;
+    st->ic = 1 - st->ic;
+    return HYOWON_OK;
 }
-int kdk_step(State*, cudaStream_t, unsigned int*, unsigned long long*, double, double, double,
-             cudaEvent_t*) {
-    return HYOWON_EINVAL;
+
+namespace {
+int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool kick, double K2,
+                       cudaEvent_t* ev, int P, int M);
 }
-void commit_step(State*, bool, bool) {}
-int download(State*, cudaStream_t, double*, double*, double*, double*, double*, double*, double*,
-             double*, double*) {
-    return HYOWON_EINVAL;
+
+int enqueue_force(State* st, cudaStream_t s, unsigned int* d_status, bool kick, double K2,
+                  cudaEvent_t* ev) {
+    return enqueue_force_sets(st, s, d_status, kick, K2, ev, st->pc, st->mc);
 }
-int download_potential(State*, cudaStream_t, double*) { return HYOWON_EINVAL; }
-int download_mass_mesh(State*, cudaStream_t, unsigned int*, double*) { return HYOWON_EINVAL; }
+
+namespace {
+int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool kick, double K2,
+                       cudaEvent_t* ev, int P, int M) {
+    const uint32_t n = st->n;
+    const int N = st->N;
+    const uint64_t cells = static_cast<uint64_t>(N) * N * N;
+    const uint64_t half = static_cast<uint64_t>(N) * N * (N / 2 + 1);
+    rec(ev, 1, s);
+    k_plan<<<1, 32, 0, s>>>(n, cells, st->d_max_count, green_c0(st), 1, st->d_plan);
+    k_fill<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->d_plan);
+    k_deposit<<<blocks_for(n), kThreads, 0, s>>>(
+        n, st->pos[P][0], st->pos[P][1], st->pos[P][2], N,
+        reinterpret_cast<unsigned long long*>(st->qmesh), st->d_plan, d_status);
+    CK(cudaMemsetAsync(st->d_qsum, 0, sizeof(unsigned long long), s));
+    k_convert<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->rmesh, st->d_qsum);
+    k_check_mass<<<1, 32, 0, s>>>(st->d_qsum, st->d_plan, d_status);
+    rec(ev, 2, s);
+    CKFFT(cufftExecR2C(st->r2c, st->rmesh, reinterpret_cast<cufftComplex*>(st->modes)));
+    rec(ev, 3, s);
+    float* const pxo = st->mom[1 - M][0];
+    float* const pyo = st->mom[1 - M][1];
+    float* const pzo = st->mom[1 - M][2];
+    const float K2f = static_cast<float>(K2);
+    if (st->method == HYOWON_PURE_PM) {
+        k_green<<<blocks_for(half), kThreads, 0, s>>>(N, st->modes, st->lap, st->win, st->deconvolve,
+                                                      st->d_plan);
+        rec(ev, 4, s);
+        CKFFT(cufftExecC2R(st->c2r, reinterpret_cast<cufftComplex*>(st->modes), st->rmesh));
+        rec(ev, 5, s);
+        const float inv_two_dx = static_cast<float>(1.0 / (2.0 * st->L / N));
+        k_gather_kick<<<blocks_for(n), kThreads, 0, s>>>(
+            n, st->rmesh, st->pos[P][0], st->pos[P][1], st->pos[P][2],
+            st->mom[M][0], st->mom[M][1], st->mom[M][2], st->acc[0], st->acc[1],
+            st->acc[2], kick ? 1 : 0, K2f, pxo, pyo, pzo, N, inv_two_dx, d_status);
+        rec(ev, 6, s);
+        return HYOWON_OK;
+    }
+    k_green_spectral<<<blocks_for(half), kThreads, 0, s>>>(N, st->L, st->modes, st->win,
+                                                           static_cast<float>(st->r_s), st->d_plan);
+    CK(cudaMemcpyAsync(st->phi_k, st->modes, sizeof(float2) * half, cudaMemcpyDeviceToDevice, s));
+    rec(ev, 4, s);
+    for (int a = 0; a < 3; ++a) {
+        CK(cudaMemsetAsync(st->acc[a], 0, sizeof(float) * n, s));
+        k_spectral_axis<<<blocks_for(half), kThreads, 0, s>>>(N, st->L, a, st->phi_k, st->modes);
+        CKFFT(cufftExecC2R(st->c2r, reinterpret_cast<cufftComplex*>(st->modes), st->rmesh));
+        k_interp_add<<<blocks_for(n), kThreads, 0, s>>>(n, st->rmesh, st->pos[P][0],
+                                                        st->pos[P][1], st->pos[P][2], N,
+                                                        st->acc[a], d_status);
+    }
+    rec(ev, 5, s);
+    if (kick) {
+        k_kick_only<<<blocks_for(n), kThreads, 0, s>>>(n, st->mom[M][0], st->mom[M][1],
+                                                       st->mom[M][2], st->acc[0], st->acc[1],
+                                                       st->acc[2], K2f, pxo, pyo, pzo, d_status);
+    }
+    rec(ev, 6, s);
+    return HYOWON_OK;
+}
+}  // namespace
+
+int kdk_step(State* st, cudaStream_t s, unsigned int* d_status, unsigned long long* d_maxdrift,
+             double K1, double D, double K2, cudaEvent_t* ev) {
+    const uint32_t n = st->n;
+    const bool sort_now = st->sort_interval <= 1 || st->since_sort + 1 >= st->sort_interval;
+    CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned int), s));
+    CK(cudaMemsetAsync(d_maxdrift, 0, sizeof(unsigned long long), s));
+    CK(cudaMemsetAsync(st->sort.count, 0, sizeof(uint32_t) * (st->sort.n_buckets + 1), s));
+    CK(cudaMemsetAsync(st->d_max_count, 0, sizeof(uint32_t), s));
+    rec(ev, 0, s);
+    const int pc = st->pc, mc = st->mc;
+    k_kick_drift_key<<<blocks_for(n), kThreads, 0, s>>>(
+        n, st->pos[pc][0], st->pos[pc][1], st->pos[pc][2], st->mom[mc][0], st->mom[mc][1],
+        st->mom[mc][2], st->acc[0], st->acc[1], st->acc[2], static_cast<float>(K1), D,
+        kTwo32 / st->L, st->N, st->pos[1 - pc][0], st->pos[1 - pc][1], st->pos[1 - pc][2],
+        st->mom[1 - mc][0], st->mom[1 - mc][1], st->mom[1 - mc][2], st->sort.shift,
+        sort_now ? 1 : 0, st->sort.key, st->sort.rank, st->sort.count, st->d_max_count,
+        d_maxdrift, d_status);
+    st->step_sorted = sort_now;
+    st->ic_before = st->ic;
+    int P = 1 - pc, M = 1 - mc;
+    if (sort_now) {
+        launch_exclusive_scan(st->sort.count, st->sort.offset, st->sort.n_buckets + 1,
+                              st->sort.scan_tmp, s);
+        const uint32_t* src[7];
+        uint32_t* dst[7];
+        for (int a = 0; a < 3; ++a) {
+            src[a] = st->pos[1 - pc][a];
+            dst[a] = st->pos[pc][a];
+            src[3 + a] = reinterpret_cast<const uint32_t*>(st->mom[1 - mc][a]);
+            dst[3 + a] = reinterpret_cast<uint32_t*>(st->mom[mc][a]);
+        }
+        src[6] = st->id[st->ic];
+        dst[6] = st->id[1 - st->ic];
+        launch_scatter4_multi(n, st->sort.key, st->sort.rank, st->sort.offset, 7, src, dst,
+                              d_status, s);
+        st->ic = 1 - st->ic;
+        P = pc;
+        M = mc;
+    }
+    k_max_count<<<st->fill_blocks, kThreads, 0, s>>>(st->sort.n_buckets, st->sort.count,
+                                                     st->d_max_count);
+    st->step_P = P;
+    st->step_M = M;
+    return enqueue_force_sets(st, s, d_status, true, K2, ev, P, M);
+}
+
+void set_sort_interval(State* st, int steps) { st->sort_interval = steps < 1 ? 1 : steps; }
+
+void commit_step(State* st, bool published, bool ok) {
+    if (!published) {
+        st->ic = st->ic_before;
+        return;
+    }
+    st->pc = st->step_P;
+    st->mc = ok ? 1 - st->step_M : st->step_M;
+    st->since_sort = st->step_sorted ? 0 : st->since_sort + 1;
+}
+
+int download(State* st, cudaStream_t s, double* x, double* y, double* z, double* px, double* py,
+             double* pz, double* ax, double* ay, double* az) {
+    const uint32_t n = st->n;
+    double* stage = nullptr;
+    CK(dalloc(&stage, n));
+    double* outs[9] = {x, y, z, px, py, pz, ax, ay, az};
+    const double pos_scale = st->L / kTwo32;
+    int rc = HYOWON_OK;
+    for (int a = 0; a < 9 && rc == HYOWON_OK; ++a) {
+        if (!outs[a]) continue;
+        if (a < 3)
+            k_unpermute_widen<uint32_t><<<blocks_for(n), kThreads, 0, s>>>(n, st->id[st->ic],
+                                                                         st->pos[st->pc][a], pos_scale, stage);
+        else if (a < 6)
+            k_unpermute_widen<float><<<blocks_for(n), kThreads, 0, s>>>(n, st->id[st->ic],
+                                                                      st->mom[st->mc][a - 3], 1.0, stage);
+        else
+            k_unpermute_widen<float><<<blocks_for(n), kThreads, 0, s>>>(n, st->id[st->ic],
+                                                                      st->acc[a - 6], 1.0, stage);
+        if (cudaMemcpyAsync(outs[a], stage, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess
+            || cudaStreamSynchronize(s) != cudaSuccess)
+            rc = fail(st, HYOWON_ECUDA, "download copy failed");
+    }
+    cudaFree(stage);
+    return rc;
+}
+
+int download_potential(State* st, cudaStream_t s, double* phi) {
+    const uint64_t cells = static_cast<uint64_t>(st->N) * st->N * st->N;
+    double* d = nullptr;
+    CK(dalloc(&d, cells));
+    k_widen_mesh<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->rmesh, d);
+    const cudaError_t e = cudaMemcpyAsync(phi, d, sizeof(double) * cells, cudaMemcpyDeviceToHost, s);
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (e != cudaSuccess || e2 != cudaSuccess) return fail(st, HYOWON_ECUDA, "potential copy failed");
+    return HYOWON_OK;
+}
+
+int download_mass_mesh(State* st, cudaStream_t s, unsigned int* d_status, double* mesh) {
+    const uint32_t n = st->n;
+    const uint64_t cells = static_cast<uint64_t>(st->N) * st->N * st->N;
+    k_plan<<<1, 32, 0, s>>>(n, cells, st->d_max_count, green_c0(st), 0, st->d_plan);
+    k_fill<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->d_plan);
+    cudaMemsetAsync(d_status, 0, sizeof(unsigned int), s);
+    k_deposit<<<blocks_for(n), kThreads, 0, s>>>(n, st->pos[st->pc][0], st->pos[st->pc][1],
+                                                 st->pos[st->pc][2], st->N,
+                                                 reinterpret_cast<unsigned long long*>(st->qmesh),
+                                                 st->d_plan, d_status);
+    double* d = nullptr;
+    CK(dalloc(&d, cells));
+    k_mass_mesh<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->d_plan, st->uniform_mass, d);
+    const cudaError_t e = cudaMemcpyAsync(mesh, d, sizeof(double) * cells, cudaMemcpyDeviceToHost, s);
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (e != cudaSuccess || e2 != cudaSuccess) return fail(st, HYOWON_ECUDA, "mass mesh copy failed");
+    return HYOWON_OK;
+}
 
 }  // namespace hyowon::fp32

@@ -42,6 +42,7 @@ int enqueue_force(State* st, cudaStream_t s, unsigned int* d_status, bool kick, 
 int kdk_step(State* st, cudaStream_t s, unsigned int* d_status,
              unsigned long long* d_maxdrift, double K1, double D, double K2,
              cudaEvent_t* ev);
+void set_sort_interval(State* st, int steps);
 // Host bookkeeping after a kdk_step: `published` when the drift was published,
 // `ok` when the whole step succeeded.
 void commit_step(State* st, bool published, bool ok);

@@ -72,7 +72,7 @@ __global__ void k_kick_drift_key(uint32_t n, const double* __restrict__ x,
                                  double* __restrict__ pxo, double* __restrict__ pyo,
                                  double* __restrict__ pzo, uint32_t* __restrict__ key,
                                  uint32_t* __restrict__ rank, uint32_t* __restrict__ count,
-                                 int shift, unsigned long long* max_drift_bits,
+                                 int shift, int with_key, unsigned long long* max_drift_bits,
                                  unsigned int* status) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double drift_norm = 0.0;
@@ -107,9 +107,11 @@ __global__ void k_kick_drift_key(uint32_t n, const double* __restrict__ x,
         pxo[i] = qx;
         pyo[i] = qy;
         pzo[i] = qz;
-        const uint32_t b = cell_index(bx, by, bz, a.N) >> shift;
-        key[i] = b;
-        rank[i] = atomicAdd(&count[b], 1u);
+        if (with_key) {
+            const uint32_t b = cell_index(bx, by, bz, a.N) >> shift;
+            key[i] = b;
+            rank[i] = atomicAdd(&count[b], 1u);
+        }
     }
     // Non-negative doubles order like their bit patterns.
     unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(drift_norm));
@@ -449,13 +451,13 @@ void launch_key_f64(uint32_t n, const ParticlesF64& p, Axis a, const SortWork& w
 void launch_kick_drift_key_f64(uint32_t n, const ParticlesF64& cur, const double* ax,
                                const double* ay, const double* az, double K1, double D,
                                Axis a, const ParticlesF64& cand, const SortWork& w,
-                               unsigned long long* max_drift_bits, unsigned int* status,
-                               cudaStream_t s) {
+                               bool with_key, unsigned long long* max_drift_bits,
+                               unsigned int* status, cudaStream_t s) {
     if (n == 0) return;
     k_kick_drift_key<<<blocks_for(n), kThreads, 0, s>>>(
         n, cur.x, cur.y, cur.z, cur.px, cur.py, cur.pz, ax, ay, az, K1, D, a, cand.x, cand.y,
-        cand.z, cand.px, cand.py, cand.pz, w.key, w.rank, w.count, w.shift, max_drift_bits,
-        status);
+        cand.z, cand.px, cand.py, cand.pz, w.key, w.rank, w.count, w.shift, with_key ? 1 : 0,
+        max_drift_bits, status);
 }
 
 void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,

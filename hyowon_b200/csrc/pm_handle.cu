@@ -27,14 +27,6 @@
 #include "pm_kernels.h"
 #include "pm_lpt.h"
 
-namespace hyowon {
-void launch_scatter_multi(uint32_t n, const uint32_t* key, const uint32_t* rank,
-                          const uint32_t* offset, int n_f64, const double* const* src,
-                          double* const* dst, int n_u32, const uint32_t* const* src_u,
-                          uint32_t* const* dst_u, const unsigned int* status,
-                          cudaStream_t s);
-}
-
 using namespace hyowon;
 
 namespace {
@@ -112,6 +104,8 @@ struct hyowon_pm_s {
     cudaEvent_t call_ev[2] = {};
     double last_times[8] = {};
     uint64_t launches = 0;  // kernels launched by this library (cuFFT excluded)
+    int sort_interval = 4;  // re-sort the particles every this many steps
+    int since_sort = 0;
 
     std::string err;
 };
@@ -301,14 +295,14 @@ void record(hyowon_pm_t h, int i) {
 
 // Deposit -> FFT -> Green -> inverse FFT -> gather (+ K2 into the spare momenta).
 // Leaves the status check to the caller.
-int enqueue_force(hyowon_pm_t h, bool kick, double K2) {
+int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2) {
     const uint32_t n = h->n;
     const int N = h->N;
     const size_t cells = static_cast<size_t>(N) * N * N;
     if (h->precision == HYOWON_FP32_FIXED) {
         return fp32::enqueue_force(h->f32, h->stream, h->d_status, kick, K2, h->timing ? h->ev : nullptr);
     }
-    const ParticlesF64 p = set_view(h, h->pc, h->mc);
+    const ParticlesF64 p = set_view(h, pset, mset);
     record(h, 1);
     CK(cudaMemsetAsync(h->mesh, 0, sizeof(double) * cells, h->stream));
     ++h->launches;
@@ -317,9 +311,9 @@ int enqueue_force(hyowon_pm_t h, bool kick, double K2) {
     record(h, 2);
     CKFFT(cufftExecD2Z(h->plan_r2c, h->mesh, reinterpret_cast<cufftDoubleComplex*>(h->modes)));
     record(h, 3);
-    double* const pxo = h->mom[1 - h->mc][0];
-    double* const pyo = h->mom[1 - h->mc][1];
-    double* const pzo = h->mom[1 - h->mc][2];
+    double* const pxo = h->mom[1 - mset][0];
+    double* const pyo = h->mom[1 - mset][1];
+    double* const pzo = h->mom[1 - mset][2];
     if (h->method == HYOWON_PURE_PM) {
         ++h->launches;
         launch_green_f64(N, h->modes, h->lap, h->win, h->four_pi_G, h->field_scale, h->deconvolve,
@@ -397,7 +391,7 @@ int solve_force(hyowon_pm_t h) {
     }
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
     record(h, 0);
-    int rc = enqueue_force(h, false, 0.0);
+    int rc = enqueue_force(h, h->pc, h->mc, false, 0.0);
     if (rc) return rc;
     unsigned int st = 0;
     rc = read_status(h, &st);
@@ -455,20 +449,25 @@ int kdk_step_impl(hyowon_pm_t h, double K1, double D, double K2, double* max_dri
         return HYOWON_OK;
     }
     const uint32_t n = h->n;
+    const bool sort_now = h->sort_interval <= 1 || h->since_sort + 1 >= h->sort_interval;
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
     CK(cudaMemsetAsync(h->d_maxdrift, 0, sizeof(unsigned long long), h->stream));
-    CK(cudaMemsetAsync(h->sort.count, 0, sizeof(uint32_t) * (h->sort.n_buckets + 1), h->stream));
+    if (sort_now)
+        CK(cudaMemsetAsync(h->sort.count, 0, sizeof(uint32_t) * (h->sort.n_buckets + 1), h->stream));
     record(h, 0);
     // 1. candidate = K1 kick + drift of the current state, into the spare set.
     const ParticlesF64 cur = set_view(h, h->pc, h->mc);
     const ParticlesF64 cand = set_view(h, 1 - h->pc, 1 - h->mc);
     ++h->launches;
     launch_kick_drift_key_f64(n, cur, h->acc[0], h->acc[1], h->acc[2], K1, D, h->axis, cand,
-                              h->sort, h->d_maxdrift, h->d_status, h->stream);
-    // 2-3. sort the candidate back into the current set (publication).
-    h->launches += launch_exclusive_scan(h->sort.count, h->sort.offset, h->sort.n_buckets + 1, h->sort.scan_tmp,
-                          h->stream);
-    {
+                              h->sort, sort_now, h->d_maxdrift, h->d_status, h->stream);
+    // Positions / momenta of the force solve: the candidate set itself, or, on
+    // sort steps, the current set the candidate is scattered into in cell order.
+    int P = 1 - h->pc, M = 1 - h->mc;
+    const int ic_before = h->ic;
+    if (sort_now) {
+        h->launches += launch_exclusive_scan(h->sort.count, h->sort.offset, h->sort.n_buckets + 1,
+                                             h->sort.scan_tmp, h->stream);
         const double* src[8];
         double* dst[8];
         int k = 0;
@@ -487,12 +486,12 @@ int kdk_step_impl(hyowon_pm_t h, double K1, double D, double K2, double* max_dri
         ++h->launches;
         launch_scatter_multi(n, h->sort.key, h->sort.rank, h->sort.offset, k, src, dst, 1, su, du,
                              h->d_status, h->stream);
+        P = h->pc;
+        M = h->mc;
+        h->ic = 1 - h->ic;
     }
-    // The scatter is the publication point; later kernels skip on error too.
-    const int ic_after = 1 - h->ic;
-    const int ic_before = h->ic;
-    h->ic = ic_after;
-    int rc = enqueue_force(h, true, K2);
+    // Kernels after the candidate skip all writes when it failed (status gate).
+    int rc = enqueue_force(h, P, M, true, K2);
     if (rc) return rc;
     unsigned int st = 0;
     rc = read_status(h, &st);
@@ -503,13 +502,16 @@ int kdk_step_impl(hyowon_pm_t h, double K1, double D, double K2, double* max_dri
         h->ic = ic_before;
         return status_to_code(h, st);
     }
+    h->pc = P;
+    h->since_sort = sort_now ? 0 : h->since_sort + 1;
     if (st) {
         // Positions drifted and momenta K1-kicked are published; the force or
         // the K2 kick failed, so momenta stay at p' and acceleration is invalid.
+        h->mc = M;
         h->acc_valid = false;
         return status_to_code(h, st);
     }
-    h->mc = 1 - h->mc;  // publish p''
+    h->mc = 1 - M;  // publish p''
     h->acc_valid = true;
     if (max_drift) {
         CK(cudaMemcpy(h->h_maxdrift, h->d_maxdrift, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
@@ -992,6 +994,13 @@ int hyowon_pm_cell_coords(hyowon_pm_t h, int64_t* base, double* frac) {
     cudaFree(df);
     cudaFree(stage);
     return rc;
+}
+
+int hyowon_pm_set_sort_interval(hyowon_pm_t h, int steps) {
+    if (!h || steps < 1) return HYOWON_EINVAL;
+    h->sort_interval = steps;
+    if (h->f32) fp32::set_sort_interval(h->f32, steps);
+    return HYOWON_OK;
 }
 
 int hyowon_pm_set_timing(hyowon_pm_t h, int enabled) {

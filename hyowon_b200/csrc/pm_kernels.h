@@ -41,6 +41,14 @@ void launch_scatter_f64(uint32_t n, const uint32_t* key, const uint32_t* rank,
                         const unsigned int* status, cudaStream_t s);
 void launch_unpermute_f64(uint32_t n, const uint32_t* id, const double* src, double* dst,
                           cudaStream_t s);
+void launch_scatter_multi(uint32_t n, const uint32_t* key, const uint32_t* rank,
+                          const uint32_t* offset, int n_f64, const double* const* src,
+                          double* const* dst, int n_u32, const uint32_t* const* src_u,
+                          uint32_t* const* dst_u, const unsigned int* status,
+                          cudaStream_t s);
+void launch_scatter4_multi(uint32_t n, const uint32_t* key, const uint32_t* rank,
+                           const uint32_t* offset, int count, const uint32_t* const* src,
+                           uint32_t* const* dst, const unsigned int* status, cudaStream_t s);
 void launch_iota_u32(uint32_t n, uint32_t* out, cudaStream_t s);
 
 // ---- FP64 form (pm_fp64.cu) -----------------------------------------------
@@ -52,8 +60,8 @@ void launch_key_f64(uint32_t n, const ParticlesF64& p, Axis a, const SortWork& w
 void launch_kick_drift_key_f64(uint32_t n, const ParticlesF64& cur, const double* ax,
                                const double* ay, const double* az, double K1, double D,
                                Axis a, const ParticlesF64& cand, const SortWork& w,
-                               unsigned long long* max_drift_bits, unsigned int* status,
-                               cudaStream_t s);
+                               bool with_key, unsigned long long* max_drift_bits,
+                               unsigned int* status, cudaStream_t s);
 void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,
                         double uniform_mass, Axis a, double* mesh, unsigned int* status,
                         cudaStream_t s);

@@ -99,6 +99,27 @@ __global__ void k_scatter(uint32_t n, const uint32_t* __restrict__ key,
     }
 }
 
+// Permute up to 8 arrays of 4-byte elements (u32 or float bit patterns).
+struct Scatter4 {
+    const uint32_t* src[8];
+    uint32_t* dst[8];
+    int count;
+};
+
+__global__ void k_scatter4(uint32_t n, const uint32_t* __restrict__ key,
+                           const uint32_t* __restrict__ rank,
+                           const uint32_t* __restrict__ offset, Scatter4 arr,
+                           const unsigned int* status) {
+    if (status && (*status & ST_BLOCKS_PUBLISH)) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t d = offset[key[i]] + rank[i];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        if (a < arr.count) arr.dst[a][d] = arr.src[a][i];
+    }
+}
+
 __global__ void k_unpermute(uint32_t n, const uint32_t* __restrict__ id,
                             const double* __restrict__ src, double* __restrict__ dst) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -184,6 +205,19 @@ void launch_scatter_multi(uint32_t n, const uint32_t* key, const uint32_t* rank,
     a.n_f64 = n_f64;
     a.n_u32 = n_u32;
     k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, key, rank, offset, a, status);
+}
+
+void launch_scatter4_multi(uint32_t n, const uint32_t* key, const uint32_t* rank,
+                           const uint32_t* offset, int count, const uint32_t* const* src,
+                           uint32_t* const* dst, const unsigned int* status, cudaStream_t s) {
+    if (n == 0) return;
+    Scatter4 a{};
+    for (int i = 0; i < count; ++i) {
+        a.src[i] = src[i];
+        a.dst[i] = dst[i];
+    }
+    a.count = count;
+    k_scatter4<<<blocks_for(n, 256), 256, 0, s>>>(n, key, rank, offset, a, status);
 }
 
 void launch_unpermute_f64(uint32_t n, const uint32_t* id, const double* src, double* dst,

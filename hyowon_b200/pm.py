@@ -207,6 +207,9 @@ class PMSolver:
             self._h, base.ctypes.data_as(nat.P_i64), nat.dptr(frac)), "cell_coords")
         return base.reshape(3, n), frac.reshape(3, n)
 
+    def set_sort_interval(self, steps: int):
+        self._check(nat.lib().hyowon_pm_set_sort_interval(self._h, int(steps)), "set_sort_interval")
+
     def set_timing(self, on: bool):
         self._check(nat.lib().hyowon_pm_set_timing(self._h, int(on)), "set_timing")
 

@@ -149,6 +149,12 @@ int hyowon_pm_download_mass_mesh(hyowon_pm_t h, double* mesh);
  * the same device function the sort key uses (src/mesh/cic_coordinate.hpp:95-121). */
 int hyowon_pm_cell_coords(hyowon_pm_t h, int64_t* base, double* frac);
 
+/* Particles are permuted into cell order every `steps` KDK steps (default 4);
+ * between re-sorts the drift is published by swapping candidate buffers. The
+ * sort only serves memory locality: results do not depend on the interval
+ * beyond floating-point summation order. */
+int hyowon_pm_set_sort_interval(hyowon_pm_t h, int steps);
+
 /* Device timing, measured with CUDA events on the handle's stream. When
  * enabled, times[0] is the device time of the whole last hyowon_pm_run /
  * kdk_step / compute_forces call, and times[1..6] the phases of its last step:
