@@ -75,6 +75,9 @@ _SIGS = {
     "hyowon_pm_set_timing": (c_int, [c_void_p, c_int]),
     "hyowon_pm_set_sort_interval": (c_int, [c_void_p, c_int]),
     "hyowon_pm_last_timing": (c_int, [c_void_p, P_double]),
+    "hyowon_vjp_1lpt_pm": (c_int, [c_void_p, P_double, P_double, P_double, P_double,
+                                   P_double, P_double]),
+    "hyowon_vjp_last_error": (ctypes.c_char_p, []),
     "hyowon_hubble": (c_int, [c_double, c_double, c_u64, P_double, P_double]),
     "hyowon_drift_factor": (c_int, [c_double, c_double, c_double, c_double, P_double]),
     "hyowon_kick_factor": (c_int, [c_double, c_double, c_double, c_double, P_double]),

@@ -31,6 +31,7 @@ UNITS = [
     ("pm_fp64.cu", ["--fmad=false"]),
     ("pm_sort.cu", []),
     ("pm_lpt.cu", []),
+    ("pm_adjoint.cu", []),
     ("pm_handle.cu", ["--fmad=false"]),
     ("pm_fp32.cu", []),
     ("cosmology.cpp", []),
@@ -47,7 +48,7 @@ def _needs(obj: str, deps: list[str]) -> bool:
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    headers.append(os.path.join(ROOT, "include", "hyowon_pm.h"))
+    headers += [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
     objs = []
     for src, extra in UNITS:
         s = os.path.join(CSRC, src)

@@ -88,6 +88,19 @@ __device__ __forceinline__ int wrap_index(int i, int N) {
     return i < 0 ? i + N : i;
 }
 
+// Rank of this particle inside its bucket with one atomic per group of lanes
+// that share the bucket (sorted particles share buckets ~8-way).
+__device__ __forceinline__ uint32_t bucket_rank(uint32_t* count, uint32_t b) {
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, b);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&count[b], static_cast<uint32_t>(__popc(peers)));
+    base = __shfl_sync(peers, base, leader);
+    return base + static_cast<uint32_t>(__popc(peers & ((1u << lane) - 1u)));
+}
+
 __device__ __forceinline__ void raise_status(unsigned int* status, unsigned int bits) {
     atomicOr(status, bits);
 }

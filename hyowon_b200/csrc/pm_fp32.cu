@@ -101,7 +101,7 @@ __global__ void k_key(uint32_t n, const uint32_t* __restrict__ ux, const uint32_
     const uint32_t b = cell_index(cell_of(ux[i], N, f), cell_of(uy[i], N, f), cell_of(uz[i], N, f), N)
         >> shift;
     key[i] = b;
-    rank[i] = atomicAdd(&count[b], 1u);
+    rank[i] = bucket_rank(count, b);
 }
 
 // K1 kick (FP32) + drift (FP64 increment rounded once into the fixed point).
@@ -151,8 +151,7 @@ __global__ void k_kick_drift_key(uint32_t n, const uint32_t* __restrict__ ux,
             >> shift;
         if (with_rank) {
             key[i] = b;
-            const uint32_t r = atomicAdd(&count[b], 1u);
-            rank[i] = r;
+            rank[i] = bucket_rank(count, b);
         } else {
             atomicAdd(&count[b], 1u);  // occupancy only: bounds the deposit weights
         }
@@ -506,6 +505,7 @@ struct State {
     int since_sort = 0;
     int step_P = 0, step_M = 0;  // position / momentum sets of the step in flight
     bool step_sorted = false;
+    uint64_t launches = 0;  // kernels launched (cuFFT's excluded)
     std::string err;
 };
 
@@ -685,9 +685,11 @@ int upload_device(State* st, uint32_t n, double* const pos[3], double* const mom
     unsigned int* d_status = nullptr;
     CK(dalloc(&d_status, 1));
     cudaMemsetAsync(d_status, 0, sizeof(unsigned int), s);
+    ++st->launches;
     k_to_fixed<<<blocks_for(n), kThreads, 0, s>>>(n, pos[0], pos[1], pos[2], mom[0], mom[1], mom[2],
                                                   st->L, st->pos[0][0], st->pos[0][1], st->pos[0][2],
                                                   st->mom[0][0], st->mom[0][1], st->mom[0][2], d_status);
+    ++st->launches;
     launch_iota_u32(n, st->id[0], s);
     unsigned int h = 0;
     cudaMemcpyAsync(&h, d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
@@ -726,12 +728,14 @@ int sort_current(State* st, cudaStream_t s, unsigned int* d_status) {
     const uint32_t n = st->n;
     CK(cudaMemsetAsync(st->sort.count, 0, sizeof(uint32_t) * (st->sort.n_buckets + 1), s));
     CK(cudaMemsetAsync(st->d_max_count, 0, sizeof(uint32_t), s));
+    ++st->launches;
     k_key<<<blocks_for(n), kThreads, 0, s>>>(n, st->pos[st->pc][0], st->pos[st->pc][1],
                                              st->pos[st->pc][2], st->N, st->sort.shift, st->sort.key,
                                              st->sort.rank, st->sort.count, st->d_max_count);
+    ++st->launches;
     k_max_count<<<st->fill_blocks, kThreads, 0, s>>>(st->sort.n_buckets, st->sort.count,
                                                      st->d_max_count);
-    launch_exclusive_scan(st->sort.count, st->sort.offset, st->sort.n_buckets + 1,
+    st->launches += launch_exclusive_scan(st->sort.count, st->sort.offset, st->sort.n_buckets + 1,
                           st->sort.scan_tmp, s);
     const uint32_t* src[7];
     uint32_t* dst[7];
@@ -743,6 +747,7 @@ int sort_current(State* st, cudaStream_t s, unsigned int* d_status) {
     }
     src[6] = st->id[st->ic];
     dst[6] = st->id[1 - st->ic];
+    ++st->launches;
     launch_scatter4_multi(n, st->sort.key, st->sort.rank, st->sort.offset, 7, src, dst, nullptr, s);
     CK(cudaStreamSynchronize(s));
     (void)d_status;
@@ -770,13 +775,18 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
     const uint64_t cells = static_cast<uint64_t>(N) * N * N;
     const uint64_t half = static_cast<uint64_t>(N) * N * (N / 2 + 1);
     rec(ev, 1, s);
+    ++st->launches;
     k_plan<<<1, 32, 0, s>>>(n, cells, st->d_max_count, green_c0(st), 1, st->d_plan);
+    ++st->launches;
     k_fill<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->d_plan);
+    ++st->launches;
     k_deposit<<<blocks_for(n), kThreads, 0, s>>>(
         n, st->pos[P][0], st->pos[P][1], st->pos[P][2], N,
         reinterpret_cast<unsigned long long*>(st->qmesh), st->d_plan, d_status);
     CK(cudaMemsetAsync(st->d_qsum, 0, sizeof(unsigned long long), s));
+    ++st->launches;
     k_convert<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->rmesh, st->d_qsum);
+    ++st->launches;
     k_check_mass<<<1, 32, 0, s>>>(st->d_qsum, st->d_plan, d_status);
     rec(ev, 2, s);
     CKFFT(cufftExecR2C(st->r2c, st->rmesh, reinterpret_cast<cufftComplex*>(st->modes)));
@@ -786,12 +796,14 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
     float* const pzo = st->mom[1 - M][2];
     const float K2f = static_cast<float>(K2);
     if (st->method == HYOWON_PURE_PM) {
+        ++st->launches;
         k_green<<<blocks_for(half), kThreads, 0, s>>>(N, st->modes, st->lap, st->win, st->deconvolve,
                                                       st->d_plan);
         rec(ev, 4, s);
         CKFFT(cufftExecC2R(st->c2r, reinterpret_cast<cufftComplex*>(st->modes), st->rmesh));
         rec(ev, 5, s);
         const float inv_two_dx = static_cast<float>(1.0 / (2.0 * st->L / N));
+        ++st->launches;
         k_gather_kick<<<blocks_for(n), kThreads, 0, s>>>(
             n, st->rmesh, st->pos[P][0], st->pos[P][1], st->pos[P][2],
             st->mom[M][0], st->mom[M][1], st->mom[M][2], st->acc[0], st->acc[1],
@@ -799,20 +811,24 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
         rec(ev, 6, s);
         return HYOWON_OK;
     }
+    ++st->launches;
     k_green_spectral<<<blocks_for(half), kThreads, 0, s>>>(N, st->L, st->modes, st->win,
                                                            static_cast<float>(st->r_s), st->d_plan);
     CK(cudaMemcpyAsync(st->phi_k, st->modes, sizeof(float2) * half, cudaMemcpyDeviceToDevice, s));
     rec(ev, 4, s);
     for (int a = 0; a < 3; ++a) {
         CK(cudaMemsetAsync(st->acc[a], 0, sizeof(float) * n, s));
+        ++st->launches;
         k_spectral_axis<<<blocks_for(half), kThreads, 0, s>>>(N, st->L, a, st->phi_k, st->modes);
         CKFFT(cufftExecC2R(st->c2r, reinterpret_cast<cufftComplex*>(st->modes), st->rmesh));
+        ++st->launches;
         k_interp_add<<<blocks_for(n), kThreads, 0, s>>>(n, st->rmesh, st->pos[P][0],
                                                         st->pos[P][1], st->pos[P][2], N,
                                                         st->acc[a], d_status);
     }
     rec(ev, 5, s);
     if (kick) {
+        ++st->launches;
         k_kick_only<<<blocks_for(n), kThreads, 0, s>>>(n, st->mom[M][0], st->mom[M][1],
                                                        st->mom[M][2], st->acc[0], st->acc[1],
                                                        st->acc[2], K2f, pxo, pyo, pzo, d_status);
@@ -832,6 +848,7 @@ int kdk_step(State* st, cudaStream_t s, unsigned int* d_status, unsigned long lo
     CK(cudaMemsetAsync(st->d_max_count, 0, sizeof(uint32_t), s));
     rec(ev, 0, s);
     const int pc = st->pc, mc = st->mc;
+    ++st->launches;
     k_kick_drift_key<<<blocks_for(n), kThreads, 0, s>>>(
         n, st->pos[pc][0], st->pos[pc][1], st->pos[pc][2], st->mom[mc][0], st->mom[mc][1],
         st->mom[mc][2], st->acc[0], st->acc[1], st->acc[2], static_cast<float>(K1), D,
@@ -843,7 +860,7 @@ int kdk_step(State* st, cudaStream_t s, unsigned int* d_status, unsigned long lo
     st->ic_before = st->ic;
     int P = 1 - pc, M = 1 - mc;
     if (sort_now) {
-        launch_exclusive_scan(st->sort.count, st->sort.offset, st->sort.n_buckets + 1,
+        st->launches += launch_exclusive_scan(st->sort.count, st->sort.offset, st->sort.n_buckets + 1,
                               st->sort.scan_tmp, s);
         const uint32_t* src[7];
         uint32_t* dst[7];
@@ -855,18 +872,22 @@ int kdk_step(State* st, cudaStream_t s, unsigned int* d_status, unsigned long lo
         }
         src[6] = st->id[st->ic];
         dst[6] = st->id[1 - st->ic];
+        ++st->launches;
         launch_scatter4_multi(n, st->sort.key, st->sort.rank, st->sort.offset, 7, src, dst,
                               d_status, s);
         st->ic = 1 - st->ic;
         P = pc;
         M = mc;
     }
+    ++st->launches;
     k_max_count<<<st->fill_blocks, kThreads, 0, s>>>(st->sort.n_buckets, st->sort.count,
                                                      st->d_max_count);
     st->step_P = P;
     st->step_M = M;
     return enqueue_force_sets(st, s, d_status, true, K2, ev, P, M);
 }
+
+uint64_t launches(const State* st) { return st->launches; }
 
 void set_sort_interval(State* st, int steps) { st->sort_interval = steps < 1 ? 1 : steps; }
 
@@ -890,6 +911,7 @@ int download(State* st, cudaStream_t s, double* x, double* y, double* z, double*
     int rc = HYOWON_OK;
     for (int a = 0; a < 9 && rc == HYOWON_OK; ++a) {
         if (!outs[a]) continue;
+        ++st->launches;
         if (a < 3)
             k_unpermute_widen<uint32_t><<<blocks_for(n), kThreads, 0, s>>>(n, st->id[st->ic],
                                                                          st->pos[st->pc][a], pos_scale, stage);
@@ -911,6 +933,7 @@ int download_potential(State* st, cudaStream_t s, double* phi) {
     const uint64_t cells = static_cast<uint64_t>(st->N) * st->N * st->N;
     double* d = nullptr;
     CK(dalloc(&d, cells));
+    ++st->launches;
     k_widen_mesh<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->rmesh, d);
     const cudaError_t e = cudaMemcpyAsync(phi, d, sizeof(double) * cells, cudaMemcpyDeviceToHost, s);
     const cudaError_t e2 = cudaStreamSynchronize(s);
@@ -922,15 +945,19 @@ int download_potential(State* st, cudaStream_t s, double* phi) {
 int download_mass_mesh(State* st, cudaStream_t s, unsigned int* d_status, double* mesh) {
     const uint32_t n = st->n;
     const uint64_t cells = static_cast<uint64_t>(st->N) * st->N * st->N;
+    ++st->launches;
     k_plan<<<1, 32, 0, s>>>(n, cells, st->d_max_count, green_c0(st), 0, st->d_plan);
+    ++st->launches;
     k_fill<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->d_plan);
     cudaMemsetAsync(d_status, 0, sizeof(unsigned int), s);
+    ++st->launches;
     k_deposit<<<blocks_for(n), kThreads, 0, s>>>(n, st->pos[st->pc][0], st->pos[st->pc][1],
                                                  st->pos[st->pc][2], st->N,
                                                  reinterpret_cast<unsigned long long*>(st->qmesh),
                                                  st->d_plan, d_status);
     double* d = nullptr;
     CK(dalloc(&d, cells));
+    ++st->launches;
     k_mass_mesh<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->d_plan, st->uniform_mass, d);
     const cudaError_t e = cudaMemcpyAsync(mesh, d, sizeof(double) * cells, cudaMemcpyDeviceToHost, s);
     const cudaError_t e2 = cudaStreamSynchronize(s);

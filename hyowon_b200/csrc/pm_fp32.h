@@ -43,6 +43,7 @@ int kdk_step(State* st, cudaStream_t s, unsigned int* d_status,
              unsigned long long* d_maxdrift, double K1, double D, double K2,
              cudaEvent_t* ev);
 void set_sort_interval(State* st, int steps);
+uint64_t launches(const State* st);
 // Host bookkeeping after a kdk_step: `published` when the drift was published,
 // `ok` when the whole step succeeded.
 void commit_step(State* st, bool published, bool ok);

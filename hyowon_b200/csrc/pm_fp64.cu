@@ -57,7 +57,7 @@ __global__ void k_key(uint32_t n, const double* __restrict__ x, const double* __
     }
     const uint32_t b = cell_index(bx, by, bz, a.N) >> shift;
     key[i] = b;
-    rank[i] = atomicAdd(&count[b], 1u);
+    rank[i] = bucket_rank(count, b);
 }
 
 // K1 kick + drift (particle_update.hpp:20-116, leapfrog_integrator.cpp:170-225)
@@ -110,7 +110,7 @@ __global__ void k_kick_drift_key(uint32_t n, const double* __restrict__ x,
         if (with_key) {
             const uint32_t b = cell_index(bx, by, bz, a.N) >> shift;
             key[i] = b;
-            rank[i] = atomicAdd(&count[b], 1u);
+            rank[i] = bucket_rank(count, b);
         }
     }
     // Non-negative doubles order like their bit patterns.

@@ -102,7 +102,9 @@ struct hyowon_pm_s {
     bool timing = false;
     cudaEvent_t ev[8] = {};
     cudaEvent_t call_ev[2] = {};
-    double last_times[8] = {};
+    double last_times[9] = {};
+    double phase_sum[6] = {};  // per-phase device ms summed over the steps of a call
+    int phase_steps = 0;
     uint64_t launches = 0;  // kernels launched by this library (cuFFT excluded)
     int sort_interval = 4;  // re-sort the particles every this many steps
     int since_sort = 0;
@@ -359,15 +361,21 @@ void collect_timing(hyowon_pm_t h) {
     float t = 0.f;
     for (int i = 0; i < 6; ++i) {
         cudaEventElapsedTime(&t, h->ev[i], h->ev[i + 1]);
-        h->last_times[i + 1] = t;
+        h->phase_sum[i] += t;
     }
+    ++h->phase_steps;
 }
 
 // Whole-call device time and launch count (hyowon_pm_last_timing).
 struct CallTimer {
     hyowon_pm_t h;
     uint64_t launches0;
-    explicit CallTimer(hyowon_pm_t hh) : h(hh), launches0(hh->launches) {
+    static uint64_t total(hyowon_pm_t hh) {
+        return hh->launches + (hh->f32 ? fp32::launches(hh->f32) : 0);
+    }
+    explicit CallTimer(hyowon_pm_t hh) : h(hh), launches0(total(hh)) {
+        for (double& v : h->phase_sum) v = 0.0;
+        h->phase_steps = 0;
         if (h->timing) cudaEventRecord(h->call_ev[0], h->stream);
     }
     ~CallTimer() {
@@ -377,7 +385,9 @@ struct CallTimer {
         float t = 0.f;
         cudaEventElapsedTime(&t, h->call_ev[0], h->call_ev[1]);
         h->last_times[0] = t;
-        h->last_times[7] = static_cast<double>(h->launches - launches0);
+        for (int i = 0; i < 6; ++i) h->last_times[i + 1] = h->phase_sum[i];
+        h->last_times[7] = static_cast<double>(total(h) - launches0);
+        h->last_times[8] = h->phase_steps;
     }
 };
 
@@ -1011,7 +1021,7 @@ int hyowon_pm_set_timing(hyowon_pm_t h, int enabled) {
 
 int hyowon_pm_last_timing(hyowon_pm_t h, double* times) {
     if (!h || !times) return HYOWON_EINVAL;
-    for (int i = 0; i < 8; ++i) times[i] = h->last_times[i];
+    for (int i = 0; i < 9; ++i) times[i] = h->last_times[i];
     return HYOWON_OK;
 }
 

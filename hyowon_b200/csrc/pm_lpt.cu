@@ -117,7 +117,121 @@ __global__ void k_lpt_apply(int N, double L, int axis, const double* __restrict_
     mom[p] = pf * s;
 }
 
+// Transpose of the displacement operator, accumulated over axes:
+// acc_k (+)= i k_d T(k) / k^2 * g_k, the same symbol as k_lpt_psi.
+__global__ void k_lpt_adjoint_accumulate(int N, double L, int axis, const double2* __restrict__ gk,
+                                         const double* __restrict__ xs,
+                                         const double* __restrict__ ys,
+                                         const double* __restrict__ y2, int n_nodes, double norm,
+                                         int first, double2* __restrict__ acc) {
+    const uint64_t total = static_cast<uint64_t>(N) * N * (N / 2 + 1);
+    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    int ix, iy, iz;
+    mode_of(idx, N, ix, iy, iz);
+    const double kf = 2.0 * 3.141592653589793 / L;
+    const int mx = ix <= N / 2 ? ix : ix - N;
+    const int my = iy <= N / 2 ? iy : iy - N;
+    const double kx = kf * mx, ky = kf * my, kz = kf * iz;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    double2 r = first ? make_double2(0.0, 0.0) : acc[idx];
+    if (k2 > 0.0) {
+        const double lk = 0.5 * log(k2);
+        const int i = axis == 0 ? ix : (axis == 1 ? iy : iz);
+        double kd = axis == 0 ? kx : (axis == 1 ? ky : kz);
+        if (N % 2 == 0 && i == N / 2) kd = 0.0;
+        if (lk >= xs[0] && lk <= xs[n_nodes - 1]) {
+            const double amp = sqrt(exp(spline_eval(lk, xs, ys, y2, n_nodes)) * norm);
+            const double f = kd / k2 * amp;
+            const double2 g = gk[idx];
+            r.x += -g.y * f;
+            r.y += g.x * f;
+        }
+    }
+    acc[idx] = r;
+}
+
+__global__ void k_scale(uint64_t n, const double* __restrict__ in, double s, double* __restrict__ out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i] * s;
+}
+
 }  // namespace
+
+int lpt_adjoint_device(int N, double L, double* const d_g[3], const double* d_xs,
+                       const double* d_ys, const double* d_y2, int n_nodes, double* d_grad,
+                       cudaStream_t s, const char** err) {
+    const size_t cells = static_cast<size_t>(N) * N * N;
+    const size_t half = static_cast<size_t>(N) * N * (N / 2 + 1);
+    double2* gk = nullptr;
+    double2* acc = nullptr;
+    double* real = nullptr;
+    void* ws = nullptr;
+    cufftHandle r2c = 0, c2r = 0;
+    bool hr = false, hc = false;
+    size_t w1 = 0, w2 = 0;
+    int rc = 0;
+    *err = nullptr;
+    const unsigned bh = static_cast<unsigned>((half + 255) / 256);
+    const unsigned bc = static_cast<unsigned>((cells + 255) / 256);
+    const double norm = static_cast<double>(cells) / (L * L * L);
+    if (cudaMalloc(&gk, sizeof(double2) * half) != cudaSuccess
+        || cudaMalloc(&acc, sizeof(double2) * half) != cudaSuccess
+        || cudaMalloc(&real, sizeof(double) * cells) != cudaSuccess) {
+        *err = "LPT adjoint work arrays could not be allocated";
+        rc = 7;
+        goto done;
+    }
+    if (cufftCreate(&r2c) != CUFFT_SUCCESS || cufftCreate(&c2r) != CUFFT_SUCCESS) {
+        *err = "cufftCreate failed";
+        rc = 6;
+        goto done;
+    }
+    hr = hc = true;
+    cufftSetAutoAllocation(r2c, 0);
+    cufftSetAutoAllocation(c2r, 0);
+    if (cufftMakePlan3d(r2c, N, N, N, CUFFT_D2Z, &w1) != CUFFT_SUCCESS
+        || cufftMakePlan3d(c2r, N, N, N, CUFFT_Z2D, &w2) != CUFFT_SUCCESS
+        || cudaMalloc(&ws, w1 > w2 ? w1 : w2) != cudaSuccess) {
+        *err = "cuFFT plan for the LPT adjoint failed";
+        rc = 6;
+        goto done;
+    }
+    cufftSetWorkArea(r2c, ws);
+    cufftSetWorkArea(c2r, ws);
+    cufftSetStream(r2c, s);
+    cufftSetStream(c2r, s);
+    for (int a = 0; a < 3; ++a) {
+        // the D2Z input is copied so the caller's cotangent survives
+        cudaMemcpyAsync(real, d_g[a], sizeof(double) * cells, cudaMemcpyDeviceToDevice, s);
+        if (cufftExecD2Z(r2c, real, reinterpret_cast<cufftDoubleComplex*>(gk)) != CUFFT_SUCCESS) {
+            *err = "LPT adjoint r2c failed";
+            rc = 6;
+            goto done;
+        }
+        k_lpt_adjoint_accumulate<<<bh, 256, 0, s>>>(N, L, a, gk, d_xs, d_ys, d_y2, n_nodes, norm,
+                                                    a == 0, acc);
+    }
+    if (cufftExecZ2D(c2r, reinterpret_cast<cufftDoubleComplex*>(acc), real) != CUFFT_SUCCESS) {
+        *err = "LPT adjoint c2r failed";
+        rc = 6;
+        goto done;
+    }
+    // grad = -(1/N^3) c2r(acc): the displacement operator is antisymmetric.
+    k_scale<<<bc, 256, 0, s>>>(cells, real, -1.0 / static_cast<double>(cells), d_grad);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        *err = "LPT adjoint kernels failed";
+        rc = 6;
+    }
+done:
+    if (hr) cufftDestroy(r2c);
+    if (hc) cufftDestroy(c2r);
+    cudaFree(ws);
+    cudaFree(gk);
+    cudaFree(acc);
+    cudaFree(real);
+    return rc;
+}
 
 int lpt_ics_device(int N, double L, const double* d_noise, const double* d_xs,
                    const double* d_ys, const double* d_y2, int n_nodes, double pf,

@@ -214,10 +214,10 @@ class PMSolver:
         self._check(nat.lib().hyowon_pm_set_timing(self._h, int(on)), "set_timing")
 
     def last_timing(self):
-        t = np.zeros(8)
+        t = np.zeros(9)
         self._check(nat.lib().hyowon_pm_last_timing(self._h, nat.dptr(t)), "last_timing")
         return dict(zip(("total", "sort", "deposit", "fft_forward", "green", "fft_inverse",
-                         "gather", "launches"), t.tolist()))
+                         "gather", "launches", "solves"), t.tolist()))
 
 
 # --------------------------------------------------------------------------

@@ -157,10 +157,11 @@ int hyowon_pm_set_sort_interval(hyowon_pm_t h, int steps);
 
 /* Device timing, measured with CUDA events on the handle's stream. When
  * enabled, times[0] is the device time of the whole last hyowon_pm_run /
- * kdk_step / compute_forces call, and times[1..6] the phases of its last step:
- * sort (kick/drift, scan, scatter), deposit, forward FFT, Green, inverse FFT,
- * gather (+K2), in milliseconds. times[7] = kernels this library launched
- * during that call (cuFFT's own kernels excluded). times has 8 entries. */
+ * kdk_step / compute_forces call; times[1..6] the phases summed over the force
+ * solves of that call: kick/drift + sort, deposit (with fill / conversion),
+ * forward FFT, Green, inverse FFT, gather (+K2), in milliseconds; times[7] the
+ * kernels this library launched during the call (cuFFT's own excluded);
+ * times[8] the number of force solves timed. times has 9 entries. */
 int hyowon_pm_set_timing(hyowon_pm_t h, int enabled);
 int hyowon_pm_last_timing(hyowon_pm_t h, double* times);
 
