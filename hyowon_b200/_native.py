@@ -78,6 +78,10 @@ _SIGS = {
     "hyowon_vjp_1lpt_pm": (c_int, [c_void_p, P_double, P_double, P_double, P_double,
                                    P_double, P_double]),
     "hyowon_vjp_last_error": (ctypes.c_char_p, []),
+    "hyowon_treepm_short_forces": (c_int, [c_void_p, c_u64, P_double, P_double, P_double, c_u64,
+                                           ctypes.POINTER(ctypes.c_uint32), P_double, P_double,
+                                           P_double, P_double]),
+    "hyowon_treepm_last_error": (ctypes.c_char_p, []),
     "hyowon_hubble": (c_int, [c_double, c_double, c_u64, P_double, P_double]),
     "hyowon_drift_factor": (c_int, [c_double, c_double, c_double, c_double, P_double]),
     "hyowon_kick_factor": (c_int, [c_double, c_double, c_double, c_double, P_double]),

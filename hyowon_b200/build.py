@@ -32,6 +32,7 @@ UNITS = [
     ("pm_sort.cu", []),
     ("pm_lpt.cu", []),
     ("pm_adjoint.cu", []),
+    ("pm_tree.cu", []),
     ("pm_handle.cu", ["--fmad=false"]),
     ("pm_fp32.cu", []),
     ("cosmology.cpp", []),

@@ -126,6 +126,24 @@ class Oracle:
         self._check(rc, "orc_pm_forces")
         return ax, ay, az
 
+    def short_range_pair(self, r_s, eps, mass, dx, dy, dz):
+        dx, dy, dz = (np.ascontiguousarray(a, dtype=np.float64) for a in (dx, dy, dz))
+        out = [np.zeros(dx.size) for _ in range(3)]
+        self.lib.orc_short_range_pair(_c_double(r_s), _c_double(eps), _c_double(mass),
+                                      _c_u64(dx.size), _dp(dx), _dp(dy), _dp(dz),
+                                      *(_dp(o) for o in out))
+        return out
+
+    def short_range_direct(self, L, x, y, z, mass, targets, r_s, r_cut, eps):
+        targets = np.ascontiguousarray(targets, dtype=np.uint32)
+        out = [np.zeros(targets.size) for _ in range(3)]
+        rc = self.lib.orc_short_range_direct(
+            _c_double(L), _c_u64(x.size), _dp(x), _dp(y), _dp(z), _c_double(mass),
+            _c_u64(targets.size), _ip(targets, ctypes.c_uint32), _c_double(r_s),
+            _c_double(r_cut), _c_double(eps), *(_dp(o) for o in out))
+        self._check(rc, "orc_short_range_direct")
+        return out
+
     def kdk_step(self, L, N, state, K1, D, K2, masses=None, uniform_mass=1.0,
                  deconvolve=False):
         """state: dict of float64 arrays x,y,z,px,py,pz,ax,ay,az (updated in place)."""
@@ -190,6 +208,27 @@ class Reference:
                                     _dp(ax), _dp(ay), _dp(az))
         self._check(rc, "ref_pm_forces")
         return ax, ay, az
+
+    def short_range_pair(self, r_s, cutoff_multiplier, eps, mass, dx, dy, dz):
+        dx, dy, dz = (np.ascontiguousarray(a, dtype=np.float64) for a in (dx, dy, dz))
+        out = [np.zeros(dx.size) for _ in range(3)]
+        rc = self.lib.ref_short_range_pair(_c_double(r_s), _c_double(cutoff_multiplier),
+                                           _c_double(eps), _c_double(mass), _c_u64(dx.size),
+                                           _dp(dx), _dp(dy), _dp(dz), *(_dp(o) for o in out))
+        self._check(rc, "ref_short_range_pair")
+        return out
+
+    def tree_short_forces(self, L, n_side, n_mesh, split_scale_cells, cutoff_multiplier, eps,
+                          theta, mass, x, y, z, targets):
+        targets = np.ascontiguousarray(targets, dtype=np.uint32)
+        out = [np.zeros(targets.size) for _ in range(3)]
+        rc = self.lib.ref_tree_short_forces(
+            _c_double(L), _c_u64(n_side), _c_u64(n_mesh), _c_double(split_scale_cells),
+            _c_double(cutoff_multiplier), _c_double(eps), _c_double(theta), _c_double(mass),
+            _c_u64(x.size), _dp(x), _dp(y), _dp(z), _c_u64(targets.size),
+            _ip(targets, ctypes.c_uint32), *(_dp(o) for o in out))
+        self._check(rc, "ref_tree_short_forces")
+        return out
 
     def schedule(self, a_start, a_final, delta_ln_a, omega_m=0.3, omega_l=0.7, max_steps=100000):
         out = np.zeros(6 * max_steps)

@@ -458,3 +458,110 @@ int orc_kdk_step(double L, uint64_t N, int deconvolve, uint64_t n, double* x,
     }
     return ORC_OK;
 }
+
+/* G m [(r^2+eps^2)^(-3/2) - (1 - M_S(q))/r^3] in long double; the small-q
+ * branch uses the series of (1 - M_S(q))/q^3 = (1/6 - q^2/40 + q^4/448 -
+ * q^6/6912 + q^8/110592)/sqrt(pi). */
+static long double short_factor_ld(long double r2, long double eps2, long double r_s,
+                                   long double Gm) {
+    const long double r = sqrtl(r2);
+    const long double q = r / r_s;
+    const long double isp = 0.564189583547756286948079451560772586L;
+    long double longf;
+    if (q < 0.02L) {
+        const long double q2 = q * q;
+        longf = isp * (1.0L / 6.0L + q2 * (-1.0L / 40.0L + q2 * (1.0L / 448.0L
+                + q2 * (-1.0L / 6912.0L + q2 / 110592.0L)))) / (r_s * r_s * r_s);
+    } else {
+        const long double one_minus_ms = erfl(0.5L * q) - q * isp * expl(-0.25L * q * q);
+        longf = one_minus_ms / (r2 * r);
+    }
+    const long double s = r2 + eps2;
+    return Gm * (1.0L / (s * sqrtl(s)) - longf);
+}
+
+void orc_short_range_pair(double r_s, double eps, double mass, uint64_t n, const double* dx,
+                          const double* dy, const double* dz, double* ax, double* ay, double* az) {
+    const long double Gm = (long double)orc_gravitational_constant() * mass;
+    for (uint64_t i = 0; i < n; ++i) {
+        const long double r2 = (long double)dx[i] * dx[i] + (long double)dy[i] * dy[i]
+            + (long double)dz[i] * dz[i];
+        const long double f = short_factor_ld(r2, (long double)eps * eps, r_s, Gm);
+        ax[i] = (double)(f * dx[i]);
+        ay[i] = (double)(f * dy[i]);
+        az[i] = (double)(f * dz[i]);
+    }
+}
+
+int orc_short_range_direct(double L, uint64_t n, const double* x, const double* y,
+                           const double* z, double mass, uint64_t n_targets,
+                           const uint32_t* targets, double r_s, double r_cut, double eps,
+                           double* ax, double* ay, double* az) {
+    if (!(L > 0.0) || !(r_cut > 0.0) || !(r_cut < 0.5 * L)) return ORC_EINVAL;
+    int nc = (int)floor(L / r_cut);
+    if (nc < 3) nc = 1;
+    const double cs = L / nc;
+    const uint64_t ncells = (uint64_t)nc * nc * nc;
+    uint64_t* start = (uint64_t*)calloc(ncells + 1, sizeof(uint64_t));
+    uint32_t* order = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    int* cell = (int*)malloc(sizeof(int) * (n ? n : 1));
+    double* wx = (double*)malloc(sizeof(double) * (n ? n : 1));
+    double* wy = (double*)malloc(sizeof(double) * (n ? n : 1));
+    double* wz = (double*)malloc(sizeof(double) * (n ? n : 1));
+    for (uint64_t i = 0; i < n; ++i) {
+        wx[i] = orc_wrap(x[i], L);
+        wy[i] = orc_wrap(y[i], L);
+        wz[i] = orc_wrap(z[i], L);
+        int cx = (int)(wx[i] / cs), cy = (int)(wy[i] / cs), cz = (int)(wz[i] / cs);
+        if (cx >= nc) cx = nc - 1;
+        if (cy >= nc) cy = nc - 1;
+        if (cz >= nc) cz = nc - 1;
+        cell[i] = (cx * nc + cy) * nc + cz;
+        start[cell[i] + 1]++;
+    }
+    for (uint64_t c = 0; c < ncells; ++c) start[c + 1] += start[c];
+    uint64_t* cur = (uint64_t*)malloc(sizeof(uint64_t) * ncells);
+    memcpy(cur, start, sizeof(uint64_t) * ncells);
+    for (uint64_t i = 0; i < n; ++i) order[cur[cell[i]]++] = (uint32_t)i;
+    free(cur);
+    const long double Gm = (long double)orc_gravitational_constant() * mass;
+    const long double eps2 = (long double)eps * eps;
+    const double rc2 = r_cut * r_cut;
+    const int reach = nc >= 3 ? 1 : 0;
+#pragma omp parallel for schedule(dynamic, 8)
+    for (long long ti = 0; ti < (long long)n_targets; ++ti) {
+        const uint32_t t = targets[ti];
+        const double tx = wx[t], ty = wy[t], tz = wz[t];
+        const int cx = cell[t] / (nc * nc), cy = (cell[t] / nc) % nc, cz = cell[t] % nc;
+        long double sx = 0, sy = 0, sz = 0;
+        for (int ox = -reach; ox <= reach; ++ox)
+            for (int oy = -reach; oy <= reach; ++oy)
+                for (int oz = -reach; oz <= reach; ++oz) {
+                    const int qx = (cx + ox + nc) % nc, qy = (cy + oy + nc) % nc, qz = (cz + oz + nc) % nc;
+                    const uint64_t c = ((uint64_t)qx * nc + qy) * nc + qz;
+                    for (uint64_t k = start[c]; k < start[c + 1]; ++k) {
+                        const uint32_t j = order[k];
+                        if (j == t) continue;
+                        const double dx = orc_minimum_image(wx[j] - tx, L);
+                        const double dy = orc_minimum_image(wy[j] - ty, L);
+                        const double dz = orc_minimum_image(wz[j] - tz, L);
+                        const double r2 = dx * dx + dy * dy + dz * dz;
+                        if (!(r2 < rc2) || r2 == 0.0) continue;
+                        const long double f = short_factor_ld(r2, eps2, r_s, Gm);
+                        sx += f * dx;
+                        sy += f * dy;
+                        sz += f * dz;
+                    }
+                }
+        ax[ti] = (double)sx;
+        ay[ti] = (double)sy;
+        az[ti] = (double)sz;
+    }
+    free(start);
+    free(order);
+    free(cell);
+    free(wx);
+    free(wy);
+    free(wz);
+    return ORC_OK;
+}

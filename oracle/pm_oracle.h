@@ -77,6 +77,21 @@ int orc_kdk_step(double L, uint64_t N, int deconvolve, uint64_t n, double* x,
                  double uniform_mass, double K1, double D, double K2,
                  double* max_drift);
 
+/* TreePM short-range force by direct summation (the checker of the tree walk):
+ * for each target index t, the sum over all sources j != t with r < r_cut of
+ * G m dx [(r^2+eps^2)^(-3/2) - (1 - M_S(r/r_s))/r^3], dx the minimum-image
+ * displacement, M_S(q) = erfc(q/2) + q/sqrt(pi) exp(-q^2/4)
+ * (include/cosmo_nbody/gravity/force_split.hpp:1-6), evaluated in long double
+ * with a cell list of side >= r_cut. Writes ax/ay/az[n_targets]. */
+int orc_short_range_direct(double L, uint64_t n, const double* x, const double* y,
+                           const double* z, double mass, uint64_t n_targets,
+                           const uint32_t* targets, double r_s, double r_cut, double eps,
+                           double* ax, double* ay, double* az);
+
+/* The pair law alone: acceleration from a source of mass m at displacement d. */
+void orc_short_range_pair(double r_s, double eps, double mass, uint64_t n, const double* dx,
+                          const double* dy, const double* dz, double* ax, double* ay, double* az);
+
 #ifdef __cplusplus
 }
 #endif

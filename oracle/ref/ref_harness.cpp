@@ -13,6 +13,10 @@
 #include "cosmo_nbody/core/particle_store.hpp"
 #include "cosmo_nbody/cosmology/cosmology_model.hpp"
 #include "cosmo_nbody/cosmology/drift_kick_factors.hpp"
+#include "cosmo_nbody/domain/domain_decomposition.hpp"
+#include "cosmo_nbody/gravity/force_split.hpp"
+#include "cosmo_nbody/gravity/octree.hpp"
+#include "cosmo_nbody/gravity/tree_walk.hpp"
 #include "cosmo_nbody/gravity/pm_solver.hpp"
 #include "cosmo_nbody/math/density_normalization.hpp"
 #include "cosmo_nbody/mesh/fft_backend.hpp"
@@ -290,6 +294,75 @@ int ref_kdk_run(double L, std::uint64_t N, int deconvolve, double omega_m,
         std::memcpy(ax, store.get_accelerations_x().data(), sizeof(double) * n);
         std::memcpy(ay, store.get_accelerations_y().data(), sizeof(double) * n);
         std::memcpy(az, store.get_accelerations_z().data(), sizeof(double) * n);
+    });
+}
+
+// ForceSplitKernel::scale_safe_short_range_acceleration
+// (src/gravity/force_split.cpp:439): acceleration of a target from a source of
+// mass m at displacement (dx, dy, dz), for n displacements.
+int ref_short_range_pair(double split_scale, double cutoff_multiplier, double eps, double mass,
+                         std::uint64_t n, const double* dx, const double* dy, const double* dz,
+                         double* ax, double* ay, double* az) {
+    return guarded([&] {
+        gravity::ForceSplitKernel k(split_scale, cutoff_multiplier);
+        for (std::uint64_t i = 0; i < n; ++i) {
+            const core::Vec3 a = k.scale_safe_short_range_acceleration({dx[i], dy[i], dz[i]},
+                                                                        mass, eps);
+            ax[i] = a.x;
+            ay[i] = a.y;
+            az[i] = a.z;
+        }
+    });
+}
+
+// The reference's TreePM short-range walk: Octree::build over [0,L)^3 and
+// TreeWalk::compute_force per target (src/gravity/octree.cpp:169-440,
+// src/gravity/tree_walk.cpp:203-464) with uniform particle mass m,
+// r_s = split_scale_cells * L / n_mesh, r_cut = cutoff_multiplier * r_s.
+int ref_tree_short_forces(double L, std::uint64_t n_side, std::uint64_t n_mesh,
+                          double split_scale_cells, double cutoff_multiplier, double eps,
+                          double theta, double mass, std::uint64_t n, const double* x,
+                          const double* y, const double* z, std::uint64_t n_targets,
+                          const std::uint32_t* targets, double* ax, double* ay, double* az) {
+    return guarded([&] {
+        config::GravityParams g;
+        g.solver = "TreePM";
+        g.eps = eps;
+        g.theta = theta;
+        g.split_scale_cells = split_scale_cells;
+        g.cutoff_multiplier = cutoff_multiplier;
+        g.deconvolve_cic = core::ExplicitBoolean(true);
+        config::BoxParams b;
+        b.L = L;
+        b.N = n_side;
+        b.N_mesh = n_mesh;
+        config::TimeParams t;
+        t.z_start = 49.0;
+        t.z_final = 0.0;
+        t.delta_ln_a = 0.1;
+        config::ICParams ic;
+        ic.mode = "snapshot";
+        ic.snapshot_file = "unused.hdf5";
+        config::OutputParams o;
+        config::SimulationParameters cfg(flat_lcdm(0.3, 0.7), b, g, t, ic, o);
+        core::ParticleStore store;
+        store.set_uniform_mass(mass);
+        store.resize(n);
+        for (std::uint64_t i = 0; i < n; ++i) {
+            store.get_positions_x()[i] = x[i];
+            store.get_positions_y()[i] = y[i];
+            store.get_positions_z()[i] = z[i];
+        }
+        gravity::Octree tree;
+        domain::DomainBounds bounds{0.0, L, 0.0, L, 0.0, L};
+        tree.build(store, bounds);
+        gravity::TreeWalk walk(tree, store, cfg);
+        for (std::uint64_t k = 0; k < n_targets; ++k) {
+            const core::Vec3 a = walk.compute_force(targets[k], theta);
+            ax[k] = a.x;
+            ay[k] = a.y;
+            az[k] = a.z;
+        }
     });
 }
 

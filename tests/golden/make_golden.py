@@ -75,11 +75,36 @@ def main():
     _, phi_dec = ref.potential(L, N, x, y, z, uniform_mass=0.75, deconvolve=True)
     ax, ay, az = ref.pm_forces(L, N, x, y, z, uniform_mass=0.75)
     bx, by, bz = ref.pm_forces(L, N, x, y, z, masses=masses)
+    # TreePM long range: continuum Green's function, Gaussian split, W^-2, -ik
+    tx, ty, tz = ref.pm_forces(L, N, x, y, z, uniform_mass=0.75, method=1, r_s=1.25 * L / N)
     np.savez_compressed(
         os.path.join(HERE, "small_pm.npz"), L=L, N=N, x=x, y=y, z=z, masses=masses,
         base_x=base_x, frac_x=frac_x, deposit_uniform=dep_u, deposit_masses=dep_m,
         density=dens, phi=phi, phi_deconvolved=phi_dec, ax=ax, ay=ay, az=az,
-        ax_m=bx, ay_m=by, az_m=bz, uniform_mass=0.75)
+        ax_m=bx, ay_m=by, az_m=bz, uniform_mass=0.75, tl_x=tx, tl_y=ty, tl_z=tz,
+        tl_r_s=1.25 * L / N)
+
+    # -- TreePM short-range pair law (ForceSplitKernel) --------------------------
+    prng = np.random.default_rng(55)
+    r_s, mult, eps = 1.25, 4.5, 1.0 / 30.0
+    r = np.concatenate([np.exp(prng.uniform(np.log(1e-4), np.log(5.6), 400)),
+                        [1e-6, 0.001, 0.05, 0.0625, 0.06249, 1.25, 5.624]])
+    u = prng.normal(size=(r.size, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    d = u * r[:, None]
+    pax, pay, paz = ref.short_range_pair(r_s, mult, eps, 2.5, d[:, 0], d[:, 1], d[:, 2])
+    np.savez_compressed(os.path.join(HERE, "treepm_pair.npz"), r_s=r_s, cutoff_multiplier=mult,
+                        eps=eps, mass=2.5, dx=d[:, 0], dy=d[:, 1], dz=d[:, 2], ax=pax, ay=pay,
+                        az=paz)
+
+    # -- TreePM short-range walk of the reference (Octree + TreeWalk) ------------
+    trng = np.random.default_rng(3)
+    Lt, nst = 32.0, 32
+    ux, uy, uz = (trng.uniform(0, Lt, nst ** 3) for _ in range(3))
+    ut = np.sort(np.random.default_rng(4).choice(nst ** 3, 256, replace=False)).astype(np.uint32)
+    uf = ref.tree_short_forces(Lt, nst, 32, 1.25, 4.5, 1.0 / 30.0, 0.5, 1.0, ux, uy, uz, ut)
+    tree_out = dict(u_L=Lt, u_x=ux, u_y=uy, u_z=uz, u_targets=ut, u_ax=uf[0], u_ay=uf[1],
+                    u_az=uf[2], u_r_s=1.25, u_r_cut=5.625, u_eps=1.0 / 30.0, u_mass=1.0)
 
     # -- c1 evolution -------------------------------------------------------
     c = ic.CONFIGS["c1"]
@@ -104,6 +129,16 @@ def main():
     out.update({"s32_" + k: v for k, v in full.items()})
     out.update(max_drift_1=md1, max_drift_32=mdf)
     np.savez_compressed(os.path.join(HERE, "c1_kdk.npz"), **out)
+
+    # clustered input for the tree: the c1 state at z = 0
+    dxc = c["box"] / c["mesh"]
+    ct = np.sort(np.random.default_rng(6).choice(c["n_side"] ** 3, 256, replace=False)).astype(np.uint32)
+    cf = ref.tree_short_forces(c["box"], c["n_side"], c["mesh"], 1.25, 4.5,
+                               c["box"] / c["n_side"] / 30.0, 0.5, m_p, full["x"], full["y"],
+                               full["z"], ct)
+    tree_out.update(c_targets=ct, c_ax=cf[0], c_ay=cf[1], c_az=cf[2], c_r_s=1.25 * dxc,
+                    c_r_cut=4.5 * 1.25 * dxc, c_eps=c["box"] / c["n_side"] / 30.0)
+    np.savez_compressed(os.path.join(HERE, "treepm_tree.npz"), **tree_out)
     print(f"c1 reference evolution: {c['steps']} steps in {secs:.2f} s")
 
 

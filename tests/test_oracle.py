@@ -131,3 +131,30 @@ def test_nonfinite_position_rejected(oracle, small_pm):
     with pytest.raises(OracleError) as e:
         oracle.deposit(float(g["L"]), int(g["N"]), x, g["y"], g["z"], uniform_mass=1.0)
     assert e.value.code == 1
+
+
+def test_short_range_pair_law_matches_reference(oracle):
+    from conftest import load_golden
+    g = load_golden("treepm_pair.npz")
+    got = np.stack(oracle.short_range_pair(float(g["r_s"]), float(g["eps"]), float(g["mass"]),
+                                           g["dx"], g["dy"], g["dz"]))
+    ref = np.stack([g["ax"], g["ay"], g["az"]])
+    scale = np.abs(ref).max(axis=0)
+    assert np.max(np.abs(got - ref) / scale) <= 1e-14
+
+
+def test_short_range_direct_is_pairwise_sum(oracle):
+    rng = np.random.default_rng(3)
+    L, n = 20.0, 300
+    x, y, z = (rng.uniform(0, L, n) for _ in range(3))
+    targets = np.arange(0, n, 7, dtype=np.uint32)
+    r_s, r_cut, eps = 1.0, 4.5, 0.05
+    ax, ay, az = oracle.short_range_direct(L, x, y, z, 2.0, targets, r_s, r_cut, eps)
+    for k, t in enumerate(targets[:10]):
+        d = np.stack([x - x[t], y - y[t], z - z[t]], axis=1)
+        d = (d + L / 2) % L - L / 2
+        r = np.linalg.norm(d, axis=1)
+        sel = (r < r_cut) & (r > 0)
+        px, py, pz = oracle.short_range_pair(r_s, eps, 2.0, d[sel, 0], d[sel, 1], d[sel, 2])
+        np.testing.assert_allclose([ax[k], ay[k], az[k]], [px.sum(), py.sum(), pz.sum()],
+                                   rtol=1e-12, atol=1e-12 * np.abs(px).sum())
