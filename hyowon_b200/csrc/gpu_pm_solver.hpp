@@ -1,0 +1,164 @@
+// gpu_pm_solver.hpp -- header-only C++20 face of the C ABI in hyowon_pm.h,
+// shaped like HYOWON's gravity::PMSolver and time::LeapfrogIntegrator so that a
+// host written against those classes can switch to the device path.
+//
+// Status codes become the exception types the reference throws for the same
+// condition (src/gravity/pm_solver.cpp:509-525 and :281-326,
+// src/time/leapfrog_integrator.cpp:183-261):
+//   HYOWON_EINVAL     -> std::invalid_argument
+//   HYOWON_ELOGIC     -> std::logic_error
+//   HYOWON_EOVERFLOW  -> std::overflow_error
+//   HYOWON_EUNDERFLOW -> std::underflow_error
+//   HYOWON_ERUNTIME   -> std::runtime_error
+//   HYOWON_ECUDA      -> std::runtime_error ("CUDA: ...")
+//   HYOWON_ENOMEM     -> std::bad_alloc
+// Link with libhyowon_pm.so.
+#pragma once
+
+#include "hyowon_pm.h"
+
+#include <cstdint>
+#include <new>
+#include <optional>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace hyowon::b200 {
+
+enum class Method { PurePM = HYOWON_PURE_PM, TreePMLongRange = HYOWON_TREEPM_LONG_RANGE };
+enum class Precision { FP64 = HYOWON_FP64, FP32Fixed = HYOWON_FP32_FIXED };
+
+inline void throw_on_status(int code, const char* what) {
+    if (code == HYOWON_OK) return;
+    const std::string msg = std::string("hyowon: ") + (what ? what : "");
+    switch (code) {
+    case HYOWON_EINVAL: throw std::invalid_argument(msg);
+    case HYOWON_ELOGIC: throw std::logic_error(msg);
+    case HYOWON_EOVERFLOW: throw std::overflow_error(msg);
+    case HYOWON_EUNDERFLOW: throw std::underflow_error(msg);
+    case HYOWON_ENOMEM: throw std::bad_alloc();
+    case HYOWON_ECUDA: throw std::runtime_error("CUDA: " + msg);
+    default: throw std::runtime_error(msg);
+    }
+}
+
+// PMSolver(MeshGeometry{L, N}, PMForceMethod, ...) on one device. Owns the
+// handle; movable, not copyable.
+class GpuPMSolver {
+public:
+    GpuPMSolver(double box_size, std::uint64_t mesh_size, Method method = Method::PurePM,
+                bool deconvolve_cic = false, double split_scale = 0.0,
+                Precision precision = Precision::FP64) {
+        const int rc = hyowon_pm_create(box_size, mesh_size, static_cast<int>(method),
+                                        deconvolve_cic ? 1 : 0, split_scale,
+                                        static_cast<int>(precision), &h_);
+        throw_on_status(rc, rc == HYOWON_EINVAL ? "invalid PM solver configuration"
+                                                : "PM solver creation failed");
+    }
+    GpuPMSolver(const GpuPMSolver&) = delete;
+    GpuPMSolver& operator=(const GpuPMSolver&) = delete;
+    GpuPMSolver(GpuPMSolver&& o) noexcept : h_(o.h_) { o.h_ = nullptr; }
+    GpuPMSolver& operator=(GpuPMSolver&& o) noexcept {
+        if (this != &o) {
+            reset();
+            h_ = o.h_;
+            o.h_ = nullptr;
+        }
+        return *this;
+    }
+    ~GpuPMSolver() { reset(); }
+
+    hyowon_pm_t handle() const noexcept { return h_; }
+
+    // PMSolver::compute_forces (src/gravity/pm_solver.cpp:494-567) on host
+    // spans: ADDS the PM acceleration to acc_*; masses empty means uniform_mass.
+    // The device particle state is replaced by these positions.
+    void compute_forces(std::span<const double> pos_x, std::span<const double> pos_y,
+                        std::span<const double> pos_z, std::span<const double> masses,
+                        std::optional<double> uniform_mass, std::span<double> acc_x,
+                        std::span<double> acc_y, std::span<double> acc_z) {
+        const std::size_t n = pos_x.size();
+        if (pos_y.size() != n || pos_z.size() != n || acc_x.size() != n || acc_y.size() != n
+            || acc_z.size() != n)
+            throw std::invalid_argument("PMSolver: position/acceleration span sizes differ");
+        if (masses.empty() == !uniform_mass.has_value() && n != 0)
+            throw std::invalid_argument("PMSolver: give either masses or a uniform mass");
+        if (!masses.empty() && masses.size() != n)
+            throw std::invalid_argument("PMSolver: mass span size differs");
+        check(hyowon_pm_forces_host(h_, n, pos_x.data(), pos_y.data(), pos_z.data(),
+                                    masses.empty() ? nullptr : masses.data(),
+                                    uniform_mass.value_or(0.0), acc_x.data(), acc_y.data(),
+                                    acc_z.data()));
+    }
+
+    // ParticleStore -> device. Momenta may be empty (zero).
+    void upload(std::span<const double> x, std::span<const double> y, std::span<const double> z,
+                std::span<const double> px, std::span<const double> py,
+                std::span<const double> pz, std::span<const double> masses,
+                std::optional<double> uniform_mass) {
+        const std::size_t n = x.size();
+        if (y.size() != n || z.size() != n || (!px.empty() && (px.size() != n || py.size() != n
+                                                                || pz.size() != n)))
+            throw std::invalid_argument("upload: span sizes differ");
+        if (!masses.empty() && masses.size() != n)
+            throw std::invalid_argument("upload: mass span size differs");
+        check(hyowon_pm_upload(h_, n, x.data(), y.data(), z.data(),
+                               px.empty() ? nullptr : px.data(),
+                               py.empty() ? nullptr : py.data(),
+                               pz.empty() ? nullptr : pz.data(),
+                               masses.empty() ? nullptr : masses.data(),
+                               uniform_mass.value_or(0.0)));
+    }
+
+    // Device -> host in the original particle order; empty spans are skipped.
+    void download(std::span<double> x, std::span<double> y, std::span<double> z,
+                  std::span<double> px = {}, std::span<double> py = {}, std::span<double> pz = {},
+                  std::span<double> ax = {}, std::span<double> ay = {},
+                  std::span<double> az = {}) {
+        const std::uint64_t n = particle_count();
+        for (auto s : {x, y, z, px, py, pz, ax, ay, az})
+            if (!s.empty() && s.size() != n)
+                throw std::invalid_argument("download: span size differs from particle count");
+        auto p = [](std::span<double> s) { return s.empty() ? nullptr : s.data(); };
+        check(hyowon_pm_download(h_, p(x), p(y), p(z), p(px), p(py), p(pz), p(ax), p(ay), p(az)));
+    }
+
+    // LeapfrogIntegrator::step (src/time/leapfrog_integrator.cpp:143-279) with
+    // host-computed factors; returns max ||D p_half|| (the integrator's
+    // last_step_max_drift_displacement).
+    double kdk_step(double K1, double D, double K2) {
+        double max_drift = 0.0;
+        check(hyowon_pm_kdk_step(h_, K1, D, K2, &max_drift));
+        return max_drift;
+    }
+
+    // Several steps without host work in between; returns per-step max drift.
+    std::vector<double> run(std::span<const double> K1, std::span<const double> D,
+                            std::span<const double> K2) {
+        if (D.size() != K1.size() || K2.size() != K1.size())
+            throw std::invalid_argument("run: factor span sizes differ");
+        std::vector<double> drift(K1.size());
+        check(hyowon_pm_run(h_, K1.size(), K1.data(), D.data(), K2.data(), drift.data()));
+        return drift;
+    }
+
+    std::uint64_t particle_count() const {
+        std::uint64_t n = 0, mesh = 0;
+        int prec = 0, meth = 0;
+        check(hyowon_pm_info(h_, &n, &mesh, &prec, &meth));
+        return n;
+    }
+
+private:
+    hyowon_pm_t h_ = nullptr;
+
+    void reset() noexcept {
+        if (h_) hyowon_pm_destroy(h_);
+        h_ = nullptr;
+    }
+    void check(int code) const { throw_on_status(code, hyowon_pm_last_error(h_)); }
+};
+
+}  // namespace hyowon::b200

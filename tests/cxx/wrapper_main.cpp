@@ -1,0 +1,59 @@
+// Drives hyowon::b200::GpuPMSolver the way a C++ host of the reference would.
+//   wrapper_main invalid             -> prints the exception type of a bad config
+//   wrapper_main forces IN OUT       -> IN: u64 n, u64 N, f64 L, f64 m, x[n], y[n], z[n]
+//                                       OUT: ax[n], ay[n], az[n] (added to zero)
+#include "gpu_pm_solver.hpp"
+
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <typeinfo>
+#include <vector>
+
+using hyowon::b200::GpuPMSolver;
+
+int main(int argc, char** argv) {
+    if (argc >= 2 && std::string(argv[1]) == "invalid") {
+        try {
+            GpuPMSolver s(-1.0, 64);
+        } catch (const std::invalid_argument&) {
+            std::cout << "invalid_argument\n";
+            return 0;
+        } catch (const std::exception& e) {
+            std::cout << "other: " << e.what() << "\n";
+            return 1;
+        }
+        std::cout << "no exception\n";
+        return 1;
+    }
+    if (argc == 4 && std::string(argv[1]) == "forces") {
+        std::ifstream in(argv[2], std::ios::binary);
+        std::uint64_t n = 0, N = 0;
+        double L = 0.0, m = 0.0;
+        in.read(reinterpret_cast<char*>(&n), 8);
+        in.read(reinterpret_cast<char*>(&N), 8);
+        in.read(reinterpret_cast<char*>(&L), 8);
+        in.read(reinterpret_cast<char*>(&m), 8);
+        std::vector<double> x(n), y(n), z(n), ax(n, 0.0), ay(n, 0.0), az(n, 0.0);
+        in.read(reinterpret_cast<char*>(x.data()), 8 * n);
+        in.read(reinterpret_cast<char*>(y.data()), 8 * n);
+        in.read(reinterpret_cast<char*>(z.data()), 8 * n);
+        if (!in) return 2;
+        try {
+            GpuPMSolver s(L, N);
+            s.compute_forces(x, y, z, {}, m, ax, ay, az);
+            // a second solve adds the same force again (PMSolver add semantics)
+            s.compute_forces(x, y, z, {}, m, ax, ay, az);
+        } catch (const std::exception& e) {
+            std::cerr << typeid(e).name() << ": " << e.what() << "\n";
+            return 3;
+        }
+        std::ofstream out(argv[3], std::ios::binary);
+        out.write(reinterpret_cast<const char*>(ax.data()), 8 * n);
+        out.write(reinterpret_cast<const char*>(ay.data()), 8 * n);
+        out.write(reinterpret_cast<const char*>(az.data()), 8 * n);
+        return out ? 0 : 4;
+    }
+    std::cerr << "usage: wrapper_main invalid | forces IN OUT\n";
+    return 64;
+}

@@ -1,0 +1,56 @@
+"""The header-only C++ face (hyowon_b200/csrc/gpu_pm_solver.hpp) as a C++ host
+of the reference would use it: status codes become the reference's exception
+types, and GpuPMSolver::compute_forces keeps PMSolver's add semantics
+(src/gravity/pm_solver.cpp:494-567)."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "hyowon_b200")
+
+
+@pytest.fixture(scope="module")
+def wrapper_exe(tmp_path_factory):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    if not os.path.exists(os.path.join(LIBDIR, "libhyowon_pm.so")):
+        pytest.fail("libhyowon_pm.so is not built")
+    exe = str(tmp_path_factory.mktemp("cxx") / "wrapper_main")
+    subprocess.run(["g++", "-std=c++20", "-O1", "-I" + os.path.join(ROOT, "include"),
+                    "-I" + os.path.join(ROOT, "hyowon_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "cxx", "wrapper_main.cpp"), "-L" + LIBDIR,
+                    "-lhyowon_pm", "-Wl,-rpath," + LIBDIR, "-o", exe], check=True)
+    return exe
+
+
+def test_invalid_configuration_throws_invalid_argument(wrapper_exe):
+    out = subprocess.run([wrapper_exe, "invalid"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.strip() == "invalid_argument"
+
+
+@pytest.mark.gpu
+def test_compute_forces_through_cxx_matches_oracle(wrapper_exe, oracle, tmp_path):
+    rng = np.random.default_rng(11)
+    n, N, L, m = 20000, 32, 50.0, 0.7
+    x, y, z = (rng.uniform(0, L, n) for _ in range(3))
+    src = tmp_path / "in.bin"
+    dst = tmp_path / "out.bin"
+    with open(src, "wb") as f:
+        f.write(np.array([n, N], dtype=np.uint64).tobytes())
+        f.write(np.array([L, m], dtype=np.float64).tobytes())
+        for a in (x, y, z):
+            f.write(a.tobytes())
+    out = subprocess.run([wrapper_exe, "forces", str(src), str(dst)], capture_output=True,
+                         text=True)
+    assert out.returncode == 0, out.stderr
+    got = np.fromfile(dst, dtype=np.float64).reshape(3, n)
+    ref = oracle.pm_forces(L, N, x, y, z, uniform_mass=m)
+    scale = max(np.max(np.abs(r)) for r in ref)
+    for g, r in zip(got, ref):
+        # two solves were added to zeroed arrays
+        assert np.max(np.abs(g - 2.0 * r)) <= 1e-12 * scale
