@@ -82,6 +82,9 @@ _SIGS = {
                                            ctypes.POINTER(ctypes.c_uint32), P_double, P_double,
                                            P_double, P_double]),
     "hyowon_treepm_last_error": (ctypes.c_char_p, []),
+    "hyowon_cic_deposit_noalloc": (c_int, [c_double, c_u64, c_u64, c_void_p, c_void_p,
+                                           c_void_p, c_void_p, c_double, c_void_p, c_void_p]),
+    "hyowon_noalloc_last_error": (ctypes.c_char_p, []),
     "hyowon_hubble": (c_int, [c_double, c_double, c_u64, P_double, P_double]),
     "hyowon_drift_factor": (c_int, [c_double, c_double, c_double, c_double, P_double]),
     "hyowon_kick_factor": (c_int, [c_double, c_double, c_double, c_double, P_double]),
