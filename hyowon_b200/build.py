@@ -35,6 +35,7 @@ UNITS = [
     ("pm_tree.cu", []),
     ("pm_handle.cu", ["--fmad=false"]),
     ("pm_fp32.cu", []),
+    ("pm_poisson.cu", []),
     ("pm_noalloc.cu", ["--fmad=false"]),
     ("cosmology.cpp", []),
 ]

@@ -24,6 +24,7 @@ enum StatusBits : unsigned int {
     ST_MASS = 1u << 5,             // CIC mass conservation violated  -> ERUNTIME
     ST_CAPACITY = 1u << 6,         // fixed-point cell capacity       -> ERUNTIME
     ST_UNDERFLOW = 1u << 7,        // lost non-zero product           -> EUNDERFLOW
+    ST_PIPELINE = 1u << 8,         // a bounded device wait timed out -> ERUNTIME
 };
 
 // Kernels that publish state check this mask first and skip all writes when a

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -28,6 +29,7 @@
 
 #include "hyowon_pm.h"
 #include "pm_fp32.h"
+#include "pm_poisson.h"
 #include "pm_kernels.h"
 
 namespace hyowon::fp32 {
@@ -153,7 +155,12 @@ __global__ void k_kick_drift_key(uint32_t n, const uint32_t* __restrict__ ux,
             key[i] = b;
             rank[i] = bucket_rank(count, b);
         } else {
-            atomicAdd(&count[b], 1u);  // occupancy only: bounds the deposit weights
+            // occupancy only (bounds the deposit weights): one atomic per group
+            // of lanes that share the bucket, as sorted neighbours mostly do
+            const unsigned active = __activemask();
+            const unsigned peers = __match_any_sync(active, b);
+            if ((threadIdx.x & 31) == __ffs(peers) - 1)
+                atomicAdd(&count[b], static_cast<uint32_t>(__popc(peers)));
         }
     }
     unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(drift_norm));
@@ -497,6 +504,9 @@ struct State {
     float2* phi_k = nullptr;
     float* lap = nullptr;
     float* win = nullptr;
+    float2* tw = nullptr;     // exp(-2 pi i m/N) (N): five-pass potential solve
+    poisson::Plan* fft_plan = nullptr;  // its tensor maps of `modes`
+    bool five_pass = false;   // pure PM on a power-of-two mesh: pm_poisson.cu
     cufftHandle r2c = 0, c2r = 0;
     bool plans = false;
     void* fft_work = nullptr;
@@ -615,7 +625,9 @@ int create(State** out, double L, int N, int method, int deconvolve, double r_s,
     const size_t half = static_cast<size_t>(N) * N * (N / 2 + 1);
     CK(dalloc(&st->qmesh, cells));
     CK(dalloc(&st->rmesh, cells));
-    CK(dalloc(&st->modes, half));
+    const size_t modes_n = method == HYOWON_PURE_PM && poisson::supported(N)
+        ? std::max(half, poisson::modes_elements_f32(N)) : half;
+    CK(dalloc(&st->modes, modes_n));
     if (method == HYOWON_TREEPM_LONG_RANGE) CK(dalloc(&st->phi_k, half));
     CK(dalloc(&st->lap, N));
     CK(dalloc(&st->win, N));
@@ -629,6 +641,22 @@ int create(State** out, double L, int N, int method, int deconvolve, double r_s,
     }
     CK(cudaMemcpy(st->lap, lf.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(st->win, wf.data(), sizeof(float) * N, cudaMemcpyHostToDevice));
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    st->fill_blocks = static_cast<unsigned>(sms) * 8;
+    if (method == HYOWON_PURE_PM && poisson::supported(N)) {
+        std::vector<double> t(2 * static_cast<size_t>(N));
+        poisson::twiddles(N, t.data());
+        std::vector<float> tf(t.begin(), t.end());
+        CK(dalloc(&st->tw, N));
+        CK(cudaMemcpy(st->tw, tf.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
+        const char* perr = "";
+        st->fft_plan = poisson::create_plan(N, true, st->modes, &perr);
+        if (!st->fft_plan) return fail(st, HYOWON_ECUDA, perr);
+        st->five_pass = true;
+        return HYOWON_OK;
+    }
     CKFFT(cufftCreate(&st->r2c));
     CKFFT(cufftCreate(&st->c2r));
     st->plans = true;
@@ -642,10 +670,6 @@ int create(State** out, double L, int N, int method, int deconvolve, double r_s,
     cufftSetWorkArea(st->c2r, st->fft_work);
     cufftSetStream(st->r2c, s);
     cufftSetStream(st->c2r, s);
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    st->fill_blocks = static_cast<unsigned>(sms) * 8;
     return HYOWON_OK;
 }
 
@@ -656,6 +680,8 @@ void destroy(State* st) {
         cufftDestroy(st->c2r);
     }
     cudaFree(st->fft_work);
+    cudaFree(st->tw);
+    poisson::destroy_plan(st->fft_plan);
     cudaFree(st->qmesh);
     cudaFree(st->rmesh);
     cudaFree(st->modes);
@@ -784,6 +810,39 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
         n, st->pos[P][0], st->pos[P][1], st->pos[P][2], N,
         reinterpret_cast<unsigned long long*>(st->qmesh), st->d_plan, d_status);
     CK(cudaMemsetAsync(st->d_qsum, 0, sizeof(unsigned long long), s));
+    float* const pxo = st->mom[1 - M][0];
+    float* const pyo = st->mom[1 - M][1];
+    float* const pzo = st->mom[1 - M][2];
+    const float K2f = static_cast<float>(K2);
+    if (st->five_pass) {
+        rec(ev, 2, s);
+        int k = poisson::forward_f32_fixed(st->fft_plan, N, st->qmesh, st->modes, st->tw, st->d_qsum,
+                                           d_status, s);
+        if (k < 0) return fail(st, HYOWON_ECUDA, "potential solve: forward pass launch failed");
+        st->launches += k;
+        ++st->launches;
+        k_check_mass<<<1, 32, 0, s>>>(st->d_qsum, st->d_plan, d_status);
+        rec(ev, 3, s);
+        const float* c_green = reinterpret_cast<const float*>(
+            reinterpret_cast<const char*>(st->d_plan) + offsetof(FixedPlan, c_green));
+        const poisson::GreenF32 g{st->lap, st->win, st->deconvolve, c_green};
+        k = poisson::green_f32(st->fft_plan, N, st->modes, st->tw, g, d_status, s);
+        if (k < 0) return fail(st, HYOWON_ECUDA, "potential solve: Green pass launch failed");
+        st->launches += k;
+        rec(ev, 4, s);
+        k = poisson::inverse_f32(st->fft_plan, N, st->modes, st->rmesh, st->tw, d_status, s);
+        if (k < 0) return fail(st, HYOWON_ECUDA, "potential solve: inverse pass launch failed");
+        st->launches += k;
+        rec(ev, 5, s);
+        const float inv_two_dx = static_cast<float>(1.0 / (2.0 * st->L / N));
+        ++st->launches;
+        k_gather_kick<<<blocks_for(n), kThreads, 0, s>>>(
+            n, st->rmesh, st->pos[P][0], st->pos[P][1], st->pos[P][2],
+            st->mom[M][0], st->mom[M][1], st->mom[M][2], st->acc[0], st->acc[1],
+            st->acc[2], kick ? 1 : 0, K2f, pxo, pyo, pzo, N, inv_two_dx, d_status);
+        rec(ev, 6, s);
+        return HYOWON_OK;
+    }
     ++st->launches;
     k_convert<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->rmesh, st->d_qsum);
     ++st->launches;
@@ -791,10 +850,6 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
     rec(ev, 2, s);
     CKFFT(cufftExecR2C(st->r2c, st->rmesh, reinterpret_cast<cufftComplex*>(st->modes)));
     rec(ev, 3, s);
-    float* const pxo = st->mom[1 - M][0];
-    float* const pyo = st->mom[1 - M][1];
-    float* const pzo = st->mom[1 - M][2];
-    const float K2f = static_cast<float>(K2);
     if (st->method == HYOWON_PURE_PM) {
         ++st->launches;
         k_green<<<blocks_for(half), kThreads, 0, s>>>(N, st->modes, st->lap, st->win, st->deconvolve,

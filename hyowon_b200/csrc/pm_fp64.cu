@@ -294,18 +294,68 @@ __global__ void k_interp_add(uint32_t n, const double* __restrict__ field,
     out[i] = r;
 }
 
+// -d / (2 dx) with the divisor fixed per launch: the product with the
+// precomputed reciprocal y = RN(1/(2dx)), corrected by one exact-remainder FMA
+// step (Markstein, IBM J. Res. Dev. 34(1), 1990): q = RN(d y), r = d - q (2dx)
+// exactly, q' = RN(q + r y). q' is the correctly rounded quotient except in
+// rare double-rounding cases, where it is within one ulp of it.
+__device__ __forceinline__ double neg_quot(double d, double two_dx, double inv_two_dx) {
+    const double q = d * inv_two_dx;
+    const double r = fma(-q, two_dx, d);
+    return -fma(r, inv_two_dx, q);
+}
+
+// One axis of the centred-gradient gather: adds w * (-(phi+ - phi-)/(2dx)) over
+// the 8 CIC corners, in the reference's corner order, to *sum and accumulates
+// the underflow flags. lo/hi are the stencil values one cell below / above
+// the 2x2x2 block along the axis, in the block's other two indices.
+template <int AXIS>
+__device__ __forceinline__ void gather_axis(const double (&c)[2][2][2], const double (&lo)[2][2],
+                                            const double (&hi)[2][2], const double (&wx)[2],
+                                            const double (&wy)[2], const double (&wz)[2],
+                                            double two_dx, double inv_two_dx, double& sum,
+                                            bool& lost) {
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox) {
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy) {
+#pragma unroll
+            for (int oz = 0; oz < 2; ++oz) {
+                const double w = wx[ox] * wy[oy] * wz[oz];
+                const bool w_lost = wx[ox] != 0.0 && wy[oy] != 0.0 && wz[oz] != 0.0 && w == 0.0;
+                double dv;
+                if (AXIS == 0)
+                    dv = (ox == 0 ? c[1][oy][oz] : hi[oy][oz]) - (ox == 0 ? lo[oy][oz] : c[0][oy][oz]);
+                else if (AXIS == 1)
+                    dv = (oy == 0 ? c[ox][1][oz] : hi[ox][oz]) - (oy == 0 ? lo[ox][oz] : c[ox][0][oz]);
+                else
+                    dv = (oz == 0 ? c[ox][oy][1] : hi[ox][oy]) - (oz == 0 ? lo[ox][oy] : c[ox][oy][0]);
+                const double g = neg_quot(dv, two_dx, inv_two_dx);
+                const bool w_nonzero = w != 0.0 || w_lost;
+                lost |= w_nonzero && dv != 0.0 && g == 0.0;
+                lost |= w_lost && g != 0.0;
+                const double cg = w * g;
+                lost |= w != 0.0 && g != 0.0 && cg == 0.0;
+                sum += cg;
+            }
+        }
+    }
+}
+
 // interpolate_centered_gradient3_add_full_mesh
 // (src/mesh/mass_assignment_gradient.cpp:117-206) into zeroed accelerations,
-// fused with the K2 kick (leapfrog_integrator.cpp:240-278). Loads the 32
-// distinct potential values of the 4x4x4 stencil footprint once.
-__global__ void __launch_bounds__(kThreads)
+// fused with the K2 kick (leapfrog_integrator.cpp:240-278). The 32 distinct
+// potential values of the 4x4x4 stencil footprint are loaded once: the 2x2x2
+// block first, then the two outer faces of one axis at a time, so each axis
+// sum is formed in the reference's corner order with few values live.
+__global__ void __launch_bounds__(kThreads, 3)
 k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restrict__ x,
               const double* __restrict__ y, const double* __restrict__ z,
               const double* __restrict__ px, const double* __restrict__ py,
               const double* __restrict__ pz, double* __restrict__ ax,
               double* __restrict__ ay, double* __restrict__ az, int do_kick, double K2,
               double* __restrict__ pxo, double* __restrict__ pyo,
-              double* __restrict__ pzo, Axis a, unsigned int* status) {
+              double* __restrict__ pzo, Axis a, double inv_two_dx, unsigned int* status) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
     int ix, iy, iz;
@@ -323,62 +373,45 @@ k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restri
     const int zs[4] = {iz == 0 ? N - 1 : iz - 1, iz, iz + 1 == N ? 0 : iz + 1,
                        iz + 2 >= N ? iz + 2 - N : iz + 2};
 #define PHI(a_, b_, c_) __ldg(&phi[cell_index(xs[a_], ys[b_], zs[c_], N)])
-    double c[2][2][2], xm[2][2], xp[2][2], ym[2][2], yp[2][2], zm[2][2], zp[2][2];
+    double c[2][2][2];
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < 2; ++u)
 #pragma unroll
-        for (int v = 0; v < 2; ++v) {
-            xm[u][v] = PHI(0, u + 1, v + 1);
-            xp[u][v] = PHI(3, u + 1, v + 1);
-            ym[u][v] = PHI(u + 1, 0, v + 1);
-            yp[u][v] = PHI(u + 1, 3, v + 1);
-            zm[u][v] = PHI(u + 1, v + 1, 0);
-            zp[u][v] = PHI(u + 1, v + 1, 3);
+        for (int v = 0; v < 2; ++v)
 #pragma unroll
             for (int w = 0; w < 2; ++w) c[u][v][w] = PHI(u + 1, v + 1, w + 1);
-        }
-    }
-#undef PHI
     const double wx[2] = {1.0 - tx, tx};
     const double wy[2] = {1.0 - ty, ty};
     const double wz[2] = {1.0 - tz, tz};
     const double two_dx = 2.0 * a.dx;
     double gx_sum = 0.0, gy_sum = 0.0, gz_sum = 0.0;
     bool lost = false;
+    double lo[2][2], hi[2][2];
 #pragma unroll
-    for (int ox = 0; ox < 2; ++ox) {
+    for (int u = 0; u < 2; ++u)
 #pragma unroll
-        for (int oy = 0; oy < 2; ++oy) {
-#pragma unroll
-            for (int oz = 0; oz < 2; ++oz) {
-                const double w = wx[ox] * wy[oy] * wz[oz];
-                const bool w_lost = wx[ox] != 0.0 && wy[oy] != 0.0 && wz[oz] != 0.0 && w == 0.0;
-                const double dxv = (ox == 0 ? c[1][oy][oz] : xp[oy][oz])
-                    - (ox == 0 ? xm[oy][oz] : c[0][oy][oz]);
-                const double dyv = (oy == 0 ? c[ox][1][oz] : yp[ox][oz])
-                    - (oy == 0 ? ym[ox][oz] : c[ox][0][oz]);
-                const double dzv = (oz == 0 ? c[ox][oy][1] : zp[ox][oy])
-                    - (oz == 0 ? zm[ox][oy] : c[ox][oy][0]);
-                const double gx = -dxv / two_dx;
-                const double gy = -dyv / two_dx;
-                const double gz = -dzv / two_dx;
-                const bool w_nonzero = w != 0.0 || w_lost;
-                lost |= w_nonzero
-                    && ((dxv != 0.0 && gx == 0.0) || (dyv != 0.0 && gy == 0.0)
-                        || (dzv != 0.0 && gz == 0.0));
-                lost |= w_lost && (gx != 0.0 || gy != 0.0 || gz != 0.0);
-                const double cx = w * gx;
-                const double cy = w * gy;
-                const double cz = w * gz;
-                lost |= w != 0.0
-                    && ((gx != 0.0 && cx == 0.0) || (gy != 0.0 && cy == 0.0)
-                        || (gz != 0.0 && cz == 0.0));
-                gx_sum += cx;
-                gy_sum += cy;
-                gz_sum += cz;
-            }
+        for (int v = 0; v < 2; ++v) {
+            lo[u][v] = PHI(0, u + 1, v + 1);
+            hi[u][v] = PHI(3, u + 1, v + 1);
         }
-    }
+    gather_axis<0>(c, lo, hi, wx, wy, wz, two_dx, inv_two_dx, gx_sum, lost);
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            lo[u][v] = PHI(u + 1, 0, v + 1);
+            hi[u][v] = PHI(u + 1, 3, v + 1);
+        }
+    gather_axis<1>(c, lo, hi, wx, wy, wz, two_dx, inv_two_dx, gy_sum, lost);
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            lo[u][v] = PHI(u + 1, v + 1, 0);
+            hi[u][v] = PHI(u + 1, v + 1, 3);
+        }
+    gather_axis<2>(c, lo, hi, wx, wy, wz, two_dx, inv_two_dx, gz_sum, lost);
+#undef PHI
     if (lost) raise_status(status, ST_UNDERFLOW);
     // The evolution path adds into zeroed accelerations (leapfrog_integrator.cpp:75-83).
     const double gax = 0.0 + gx_sum;
@@ -505,7 +538,7 @@ void launch_gather_kick_f64(uint32_t n, const double* phi, const ParticlesF64& p
     if (n == 0) return;
     k_gather_kick<<<blocks_for(n), kThreads, 0, s>>>(n, phi, p.x, p.y, p.z, p.px, p.py, p.pz,
                                                      ax, ay, az, do_kick, K2, pxo, pyo, pzo,
-                                                     a, status);
+                                                     a, 1.0 / (2.0 * a.dx), status);
 }
 
 void launch_kick_only_f64(uint32_t n, const ParticlesF64& p, const double* ax,

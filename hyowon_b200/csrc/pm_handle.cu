@@ -24,6 +24,7 @@
 
 #include "hyowon_pm.h"
 #include "pm_fp32.h"
+#include "pm_poisson.h"
 #include "pm_kernels.h"
 #include "pm_lpt.h"
 
@@ -72,6 +73,9 @@ struct hyowon_pm_s {
     double2* phi_k = nullptr;    // spectral method: kept copy of phi_k
     double* lap = nullptr;       // 1-D discrete Laplacian symbol (N)
     double* win = nullptr;       // 1-D CIC window W(k) (N)
+    double2* tw = nullptr;       // exp(-2 pi i m/N) (N): five-pass potential solve
+    poisson::Plan* fft_plan = nullptr;  // its tensor maps of `modes`
+    bool five_pass = false;      // pure PM on a power-of-two mesh: pm_poisson.cu
 
     uint32_t n = 0;
     uint32_t cap = 0;
@@ -164,6 +168,8 @@ int status_to_code(hyowon_pm_t h, unsigned int st) {
         return fail(h, HYOWON_EOVERFLOW, "Leapfrog K2 update is not finite and representable");
     if (st & ST_UNDERFLOW)
         return fail(h, HYOWON_EUNDERFLOW, "CIC centered-gradient gather lost a non-zero product");
+    if (st & ST_PIPELINE)
+        return fail(h, HYOWON_ERUNTIME, "potential solve: a device pipeline wait timed out");
     return fail(h, HYOWON_ERUNTIME, "unknown device status");
 }
 
@@ -311,11 +317,32 @@ int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2) {
     launch_deposit_f64(n, p, h->has_masses ? h->mass[h->ic] : nullptr, h->uniform_mass, h->axis,
                        h->mesh, h->d_status, h->stream);
     record(h, 2);
-    CKFFT(cufftExecD2Z(h->plan_r2c, h->mesh, reinterpret_cast<cufftDoubleComplex*>(h->modes)));
-    record(h, 3);
     double* const pxo = h->mom[1 - mset][0];
     double* const pyo = h->mom[1 - mset][1];
     double* const pzo = h->mom[1 - mset][2];
+    if (h->five_pass) {
+        int k = poisson::forward_f64(h->fft_plan, N, h->mesh, h->modes, h->tw, h->d_status, h->stream);
+        if (k < 0) return fail(h, HYOWON_ECUDA, "potential solve: forward pass launch failed");
+        h->launches += k;
+        record(h, 3);
+        const poisson::GreenF64 g{h->lap, h->win, h->four_pi_G, h->field_scale, h->deconvolve,
+                                  h->input_mass, h->mass_tol, h->d_status};
+        k = poisson::green_f64(h->fft_plan, N, h->modes, h->tw, g, h->stream);
+        if (k < 0) return fail(h, HYOWON_ECUDA, "potential solve: Green pass launch failed");
+        h->launches += k;
+        record(h, 4);
+        k = poisson::inverse_f64(h->fft_plan, N, h->modes, h->mesh, h->tw, h->d_status, h->stream);
+        if (k < 0) return fail(h, HYOWON_ECUDA, "potential solve: inverse pass launch failed");
+        h->launches += k;
+        record(h, 5);
+        ++h->launches;
+        launch_gather_kick_f64(n, h->mesh, p, h->acc[0], h->acc[1], h->acc[2], kick ? 1 : 0, K2,
+                               pxo, pyo, pzo, h->axis, h->d_status, h->stream);
+        record(h, 6);
+        return HYOWON_OK;
+    }
+    CKFFT(cufftExecD2Z(h->plan_r2c, h->mesh, reinterpret_cast<cufftDoubleComplex*>(h->modes)));
+    record(h, 3);
     if (h->method == HYOWON_PURE_PM) {
         ++h->launches;
         launch_green_f64(N, h->modes, h->lap, h->win, h->four_pi_G, h->field_scale, h->deconvolve,
@@ -622,10 +649,28 @@ int hyowon_pm_create(double box_size, uint64_t mesh_size, int method, int deconv
 
     const size_t cells = static_cast<size_t>(N) * N * N;
     const size_t half = static_cast<size_t>(N) * N * (N / 2 + 1);
-    if (dalloc(&h->mesh, cells) != cudaSuccess || dalloc(&h->modes, half) != cudaSuccess)
+    const size_t modes_n = method == HYOWON_PURE_PM && poisson::supported(N)
+        ? std::max(half, poisson::modes_elements_f64(N)) : half;
+    if (dalloc(&h->mesh, cells) != cudaSuccess || dalloc(&h->modes, modes_n) != cudaSuccess)
         return bail(HYOWON_ENOMEM);
     if (method == HYOWON_TREEPM_LONG_RANGE && dalloc(&h->phi_k, half) != cudaSuccess)
         return bail(HYOWON_ENOMEM);
+    if (method == HYOWON_PURE_PM && poisson::supported(N)) {
+        std::vector<double> t(2 * static_cast<size_t>(N));
+        poisson::twiddles(N, t.data());
+        if (dalloc(&h->tw, N) != cudaSuccess) return bail(HYOWON_ENOMEM);
+        if (cudaMemcpy(h->tw, t.data(), sizeof(double2) * N, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(HYOWON_ECUDA);
+        const char* perr = "";
+        h->fft_plan = poisson::create_plan(N, false, h->modes, &perr);
+        if (!h->fft_plan) {
+            h->err = perr;
+            return bail(HYOWON_ECUDA);
+        }
+        h->five_pass = true;
+        *out = h;
+        return HYOWON_OK;
+    }
     size_t ws1 = 0, ws2 = 0;
     if (cufftCreate(&h->plan_r2c) != CUFFT_SUCCESS || cufftCreate(&h->plan_c2r) != CUFFT_SUCCESS)
         return bail(HYOWON_ECUDA);
@@ -654,6 +699,8 @@ int hyowon_pm_destroy(hyowon_pm_t h) {
         cufftDestroy(h->plan_c2r);
     }
     cudaFree(h->fft_work);
+    cudaFree(h->tw);
+    poisson::destroy_plan(h->fft_plan);
     cudaFree(h->mesh);
     cudaFree(h->modes);
     cudaFree(h->phi_k);

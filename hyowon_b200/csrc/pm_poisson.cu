@@ -1,0 +1,609 @@
+// pm_poisson.cu -- pure-PM potential solve on power-of-two meshes in five
+// passes over HBM (see pm_poisson.h for the pass structure).
+//
+// The half spectrum is held kz-chunk-major: H[kc][kx][ky][kzc] with
+// kz = kc * CC + kzc, CC = 16 FP32 / 8 FP64 complex values (128 bytes), so
+//  * a y-pass tile (kc, kx) is one contiguous N * 128-byte block,
+//  * an x-pass tile (kc, ky) reads 128-byte runs inside one N^2 * 128-byte
+//    chunk (a small page footprint instead of the whole 4-8 GB mesh),
+//  * a z-pass block of CZ consecutive rows writes CZ * 128 contiguous bytes
+//    per chunk.
+// The last chunk holds the Nyquist plane kz = N/2 and CC-1 unused columns
+// (memory and transform work +1/(N/(2 CC)+1)).
+//
+// Bytes moved per solve on an N^3 mesh with b-byte reals: z forward reads the
+// N^3 mass values (int64 in the precision form) and writes H, the x, y(+Green)
+// and x passes read and write H in place, z inverse reads H and writes the
+// N^3 potential.
+#include "pm_poisson.h"
+
+#include "pm_common.cuh"
+#include "pm_fft.cuh"
+#include "pm_tma.cuh"
+
+#include <cuda.h>
+
+#include <cmath>
+#include <new>
+
+namespace hyowon {
+namespace poisson {
+
+// Tensor maps of the chunked half spectrum viewed as a 3-D array of 8-byte
+// units: (units per row = CC complex, ky, kc * N + kx). `y` loads a y-pass
+// tile in boxes of (units, box, 1), `x` an x-pass tile in boxes of
+// (units, 1, box).
+struct Plan {
+    CUtensorMap y;
+    CUtensorMap x;
+    int N = 0;
+    bool fp32 = false;
+};
+
+namespace {
+
+using fft::cx_t;
+using fft::mk;
+
+// Tuning: sequences per block of the z passes (rows) and of the y/x passes
+// (columns), and the blocks per SM the register budget is sized for.
+#ifndef HYOWON_FFT_CZ32
+#define HYOWON_FFT_CZ32 16
+#endif
+#ifndef HYOWON_FFT_CZ64
+#define HYOWON_FFT_CZ64 8
+#endif
+#ifndef HYOWON_FFT_CC32
+#define HYOWON_FFT_CC32 8
+#endif
+#ifndef HYOWON_FFT_CC64
+#define HYOWON_FFT_CC64 4
+#endif
+#ifndef HYOWON_FFT_MINB_Z
+#define HYOWON_FFT_MINB_Z 2
+#endif
+#ifndef HYOWON_FFT_MINB_C
+#define HYOWON_FFT_MINB_C 1
+#endif
+
+template <typename T, int LOG2N> struct Shape;
+template <int LOG2N> struct Shape<float, LOG2N> {
+    static constexpr int CZ = LOG2N >= 11 ? (HYOWON_FFT_CZ32 > 8 ? 8 : HYOWON_FFT_CZ32) : HYOWON_FFT_CZ32;
+    static constexpr int CC = LOG2N >= 11 ? (HYOWON_FFT_CC32 > 4 ? 4 : HYOWON_FFT_CC32) : HYOWON_FFT_CC32;
+};
+template <int LOG2N> struct Shape<double, LOG2N> {
+    static constexpr int CZ = LOG2N >= 11 ? (HYOWON_FFT_CZ64 > 4 ? 4 : HYOWON_FFT_CZ64) : HYOWON_FFT_CZ64;
+    static constexpr int CC = LOG2N >= 11 ? (HYOWON_FFT_CC64 > 2 ? 2 : HYOWON_FFT_CC64) : HYOWON_FFT_CC64;
+};
+
+template <typename T, int LOG2N> struct Geo {
+    using C = cx_t<T>;
+    static constexpr int N = 1 << LOG2N;
+    static constexpr int M = N / 2;          // complex length of a packed row
+    static constexpr int Hz = M + 1;         // half-complex row length
+    static constexpr int K = M / 2 + 1;      // (k, M-k) pairs of a row
+    static constexpr int CZ = Shape<T, LOG2N>::CZ;
+    static constexpr int CC = Shape<T, LOG2N>::CC;
+    static constexpr int SZ = CZ + 1;
+    static constexpr int TZ = CZ * M / 16;   // threads of a z-pass block
+    static constexpr int TC = CC * N / 16;   // threads of a y/x-pass block
+    static constexpr int PZ = CZ * M / TZ;   // row pairs each z-pass thread loads (16)
+    static constexpr int KC = (Hz + CC - 1) / CC;        // kz chunks
+    static constexpr int QZ = (KC * CZ * CC + TZ - 1) / TZ;  // chunked values per z-pass thread
+    static constexpr size_t chunk = static_cast<size_t>(N) * N * CC;  // elements per kz chunk
+    // element (kx, ky, kz) of the chunked half spectrum
+    __device__ static __forceinline__ size_t at(int kx, int ky, int kz) {
+        return static_cast<size_t>(kz / CC) * chunk + (static_cast<size_t>(kx) * N + ky) * CC + (kz % CC);
+    }
+    static constexpr size_t smem_zf = sizeof(C) * M * SZ;
+    static constexpr size_t smem_zi = sizeof(C) * Hz * SZ;
+    static constexpr unsigned tile_bytes = sizeof(C) * N * CC;   // one y/x-pass tile
+    static constexpr size_t smem_c = 2ull * tile_bytes;           // double buffered
+    static constexpr int box = N < 256 ? N : 256;                 // TMA box rows
+    static constexpr int units = CC * static_cast<int>(sizeof(C)) / 8;  // 8-byte units per row
+};
+
+template <typename S> struct Raw;   // 16-byte raw row pair of the z forward input
+template <> struct Raw<double> { using type = double2; };
+template <> struct Raw<long long> { using type = longlong2; };
+
+__device__ __forceinline__ double2 to_complex(double2 v, unsigned long long&) { return v; }
+__device__ __forceinline__ float2 to_complex(longlong2 v, unsigned long long& sum) {
+    sum += static_cast<unsigned long long>(v.x) + static_cast<unsigned long long>(v.y);
+    return make_float2(__ll2float_rn(v.x), __ll2float_rn(v.y));
+}
+
+// r2c of CZ rows per block: pack the N reals of a row as N/2 complex values,
+// transform, and unpack X[k] = E[k] + W_N^k O[k] with E/O the transforms of
+// the even/odd samples, for k = 0..N/2. Each thread issues all its row loads
+// before the first shared-memory store.
+template <typename T, typename SRC, int LOG2N>
+__global__ void __launch_bounds__(Geo<T, LOG2N>::TZ, HYOWON_FFT_MINB_Z)
+k_z_forward(const SRC* __restrict__ in, cx_t<T>* __restrict__ H, const cx_t<T>* __restrict__ tw,
+            unsigned long long* qsum) {
+    using G = Geo<T, LOG2N>;
+    using C = cx_t<T>;
+    using RawT = typename Raw<SRC>::type;
+    constexpr int S = G::SZ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw);
+    const int tid = threadIdx.x;
+    const size_t row0 = static_cast<size_t>(blockIdx.x) * G::CZ;
+    const RawT* src = reinterpret_cast<const RawT*>(in + row0 * G::N);
+    RawT raw[G::PZ];
+#pragma unroll
+    for (int i = 0; i < G::PZ; ++i) raw[i] = __ldcs(&src[tid + i * G::TZ]);
+    unsigned long long sum = 0;
+#pragma unroll
+    for (int i = 0; i < G::PZ; ++i) {
+        const int e = tid + i * G::TZ;
+        sm[(e % G::M) * S + e / G::M] = to_complex(raw[i], sum);
+    }
+    if (qsum) {
+        if constexpr (G::TZ >= 32) {
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if ((tid & 31) == 0 && sum) atomicAdd(qsum, sum);
+        } else {
+            if (sum) atomicAdd(qsum, sum);
+        }
+    }
+    __syncthreads();
+    fft::smem_fft<LOG2N - 1, -1, G::CZ, G::SZ>(sm, tw, G::N, tid % G::CZ, tid / G::CZ);
+    const T half = static_cast<T>(0.5);
+    const int x = static_cast<int>(row0 / G::N);
+    const int y0 = static_cast<int>(row0 % G::N);
+    constexpr int KP = (G::K + G::CC - 1) / G::CC;   // chunks covering k = 0..M/2
+    for (int e = tid; e < KP * G::CZ * G::CC; e += G::TZ) {
+        const int ki = e % G::CC;
+        const int r = (e / G::CC) % G::CZ;
+        const int k = (e / (G::CC * G::CZ)) * G::CC + ki;
+        if (k >= G::K) continue;
+        const C zk = sm[k * S + r];
+        const C zm = sm[((G::M - k) & (G::M - 1)) * S + r];
+        const C w = __ldg(&tw[k]);
+        const C E = mk(half * (zk.x + zm.x), half * (zk.y - zm.y));
+        const T dx = zk.x - zm.x;
+        const T dy = zk.y + zm.y;
+        const C O = mk(half * dy, -half * dx);        // (zk - conj(zm)) / 2i
+        H[G::at(x, y0 + r, k)] = fft::cadd(E, fft::cmul(w, O));
+        if (G::M - k != k) {
+            const C E2 = mk(E.x, -E.y);
+            const C O2 = mk(half * dy, half * dx);    // (zm - conj(zk)) / 2i
+            const C w2 = mk(-w.x, w.y);               // W_N^(M-k) = -conj(W_N^k)
+            H[G::at(x, y0 + r, G::M - k)] = fft::cadd(E2, fft::cmul(w2, O2));
+        }
+    }
+}
+
+// c2r of CZ rows per block: Z[k] = (X[k] + conj X[M-k]) + i W_N^-k (X[k] - conj X[M-k]),
+// inverse length-M transform, real output pairs (Re, Im).
+template <typename T, int LOG2N>
+__global__ void __launch_bounds__(Geo<T, LOG2N>::TZ, HYOWON_FFT_MINB_Z)
+k_z_inverse(const cx_t<T>* __restrict__ H, T* __restrict__ out, const cx_t<T>* __restrict__ tw) {
+    using G = Geo<T, LOG2N>;
+    using C = cx_t<T>;
+    constexpr int S = G::SZ;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw);
+    const int tid = threadIdx.x;
+    const size_t row0 = static_cast<size_t>(blockIdx.x) * G::CZ;
+    const int x = static_cast<int>(row0 / G::N);
+    const int y0 = static_cast<int>(row0 % G::N);
+    C v[G::QZ];
+#pragma unroll
+    for (int i = 0; i < G::QZ; ++i) {
+        const int e = tid + i * G::TZ;
+        const int k = (e / (G::CC * G::CZ)) * G::CC + e % G::CC;
+        if (e < G::KC * G::CZ * G::CC && k < G::Hz)
+            v[i] = __ldcs(&H[G::at(x, y0 + (e / G::CC) % G::CZ, k)]);
+    }
+#pragma unroll
+    for (int i = 0; i < G::QZ; ++i) {
+        const int e = tid + i * G::TZ;
+        const int k = (e / (G::CC * G::CZ)) * G::CC + e % G::CC;
+        if (e < G::KC * G::CZ * G::CC && k < G::Hz) sm[k * S + (e / G::CC) % G::CZ] = v[i];
+    }
+    __syncthreads();
+    for (int e = tid; e < G::CZ * G::K; e += G::TZ) {
+        const int r = e / G::K;
+        const int k = e % G::K;
+        const C xk = sm[k * S + r];
+        const C xm = sm[(G::M - k) * S + r];
+        const C w = __ldg(&tw[k]);
+        const C Ep = mk(xk.x + xm.x, xk.y - xm.y);
+        const C Dp = mk(xk.x - xm.x, xk.y + xm.y);
+        const C Op = fft::cmul(Dp, fft::conj(w));
+        sm[k * S + r] = mk(Ep.x - Op.y, Ep.y + Op.x);
+        if (k != 0 && G::M - k != k) {
+            const C Op2 = fft::cmul(mk(-Dp.x, Dp.y), mk(-w.x, -w.y));
+            sm[(G::M - k) * S + r] = mk(Ep.x - Op2.y, -Ep.y + Op2.x);
+        }
+    }
+    __syncthreads();
+    fft::smem_fft<LOG2N - 1, +1, G::CZ, G::SZ>(sm, tw, G::N, tid % G::CZ, tid / G::CZ);
+    for (int e = tid; e < G::CZ * G::M; e += G::TZ) {
+        const int r = e / G::M;
+        const int jj = e % G::M;
+        __stcs(reinterpret_cast<C*>(out + (row0 + r) * G::N + 2 * jj), sm[jj * S + r]);
+    }
+}
+
+struct NoGreen {
+    template <typename C>
+    __device__ __forceinline__ C operator()(int, int, int, C v) const { return v; }
+};
+
+// Green's multiply of the binary64 form, operation for operation as k_green.
+struct DevGreenF64 {
+    GreenF64 g;
+    __device__ __forceinline__ double2 operator()(int ix, int iy, int iz, double2 v) const {
+        if ((ix | iy | iz) == 0) {
+            if (!(fabs(v.x - g.input_mass) <= g.mass_tol)) raise_status(g.status, ST_MASS);
+            return make_double2(0.0, 0.0);
+        }
+        const double Dk = g.lap[ix] + g.lap[iy] + g.lap[iz];
+        double f = g.four_pi_G / Dk;
+        if (g.deconvolve) {
+            const double wt = g.win[ix] * g.win[iy] * g.win[iz];
+            f /= (wt * wt);
+        }
+        f *= g.scale;
+        v.x *= f;
+        v.y *= f;
+        return v;
+    }
+};
+
+struct DevGreenF32 {
+    GreenF32 g;
+    __device__ __forceinline__ float2 operator()(int ix, int iy, int iz, float2 v) const {
+        if ((ix | iy | iz) == 0) return make_float2(0.f, 0.f);
+        float f = *g.c_green / (g.lap[ix] + g.lap[iy] + g.lap[iz]);
+        if (g.deconvolve) {
+            const float wt = g.win[ix] * g.win[iy] * g.win[iz];
+            f /= wt * wt;
+        }
+        v.x *= f;
+        v.y *= f;
+        return v;
+    }
+};
+
+// Bounded polls of a pipeline barrier before a block gives up (each poll may
+// suspend for a hardware-chosen interval; a healthy wait needs a few).
+constexpr unsigned kWaitLimit = 1u << 24;
+
+// Complex transforms of the CC columns of each tile of the chunked half
+// spectrum: tile t = (kc, s) with kc = t / N, s = t % N; y pass (AXIS 1):
+// s = kx, the tile is the contiguous block H[kc][kx][.][.]; x pass (AXIS 0):
+// s = ky, elements H[kc][.][ky][.] (128-byte-or-less runs N*CC apart).
+// Persistent blocks; one thread streams the next tile into the second
+// shared-memory buffer with TMA loads while the block transforms the current
+// one (dense rows, no padding: a half/quarter warp reads one 64-byte row).
+// With GREEN (the y pass): forward transform, Green's multiply, inverse
+// transform. Results are stored from registers.
+template <typename T, int LOG2N, int AXIS, int SIGN, bool GREEN, typename GF>
+__global__ void __launch_bounds__(Geo<T, LOG2N>::TC, 1)
+k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
+          const cx_t<T>* __restrict__ tw, GF green, unsigned int* status) {
+    using G = Geo<T, LOG2N>;
+    using C = cx_t<T>;
+    constexpr int P = G::N / 16;
+    constexpr int S = G::CC;
+    constexpr size_t axis_stride = AXIS == 1 ? static_cast<size_t>(G::CC)
+                                             : static_cast<size_t>(G::N) * G::CC;
+    constexpr size_t seq_stride = AXIS == 1 ? static_cast<size_t>(G::N) * G::CC
+                                            : static_cast<size_t>(G::CC);
+    extern __shared__ __align__(1024) unsigned char smem_tiles[];
+    __shared__ __align__(8) uint64_t full[2];
+    const int tid = threadIdx.x;
+    const int c = tid % G::CC;
+    const int j = tid / G::CC;
+    const unsigned tiles = static_cast<unsigned>(G::KC) * G::N;
+    auto tile_buf = [&](int b) { return reinterpret_cast<C*>(smem_tiles + b * G::tile_bytes); };
+    auto issue = [&](unsigned tile, int b) {
+        const int kc = static_cast<int>(tile / G::N);
+        const int sq = static_cast<int>(tile % G::N);
+        C* dst = tile_buf(b);
+        tma::mbar_arrive_expect_tx(&full[b], G::tile_bytes);
+#pragma unroll
+        for (int g = 0; g < G::N / G::box; ++g) {
+            if (AXIS == 1)
+                tma::load_3d(dst + g * G::box * G::CC, &map, 0, g * G::box, kc * G::N + sq, &full[b]);
+            else
+                tma::load_3d(dst + g * G::box * G::CC, &map, 0, sq, kc * G::N + g * G::box, &full[b]);
+        }
+    };
+    if (tid == 0) {
+        tma::mbar_init(&full[0], 1);
+        tma::mbar_init(&full[1], 1);
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    unsigned t = blockIdx.x;
+    if (tid == 0 && t < tiles) issue(t, 0);
+    for (unsigned i = 0; t < tiles; ++i, t += gridDim.x) {
+        const int b = static_cast<int>(i & 1u);
+        const unsigned nt = t + gridDim.x;
+        if (tid == 0 && nt < tiles) {
+            tma::fence_proxy_async();
+            issue(nt, b ^ 1);
+        }
+        const bool ok = tma::mbar_wait(&full[b], (i >> 1) & 1u, kWaitLimit);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicOr(status, ST_PIPELINE);
+                // let this block's copies in flight land before it exits
+                tma::mbar_wait(&full[b], (i >> 1) & 1u, kWaitLimit);
+                if (nt < tiles) tma::mbar_wait(&full[b ^ 1], ((i + 1) >> 1) & 1u, kWaitLimit);
+            }
+            return;
+        }
+        C* sm = tile_buf(b);
+        const int kc = static_cast<int>(t / G::N);
+        const int seq = static_cast<int>(t % G::N);
+        const int kz = kc * G::CC + c;
+        C v[16];
+        fft::smem_to_registers<LOG2N, SIGN, G::CC, S>(sm, tw, G::N, c, j, v);
+        if constexpr (GREEN) {
+            if (kz < G::Hz) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    v[q] = AXIS == 0 ? green(j + q * P, seq, kz, v[q]) : green(seq, j + q * P, kz, v[q]);
+            }
+            __syncthreads();
+            fft::first_stage_to_smem<LOG2N, -SIGN, G::CC, S>(v, sm, c, j);
+            fft::rest_to_registers<LOG2N, -SIGN, G::CC, S>(sm, tw, G::N, c, j, v);
+        }
+        if (kz < G::Hz) {
+            C* dst = H + static_cast<size_t>(kc) * G::chunk + static_cast<size_t>(seq) * seq_stride + c;
+#pragma unroll
+            for (int q = 0; q < 16; ++q) __stcs(&dst[static_cast<size_t>(j + q * P) * axis_stride], v[q]);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename K>
+bool prepare(K kernel, size_t smem) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(smem)) == cudaSuccess;
+}
+
+template <typename T, typename SRC, int LOG2N>
+int z_forward(const SRC* in, cx_t<T>* H, const cx_t<T>* tw, unsigned long long* qsum,
+              cudaStream_t s) {
+    using G = Geo<T, LOG2N>;
+    if (!prepare(k_z_forward<T, SRC, LOG2N>, G::smem_zf)) return -1;
+    const unsigned blocks = static_cast<unsigned>(static_cast<size_t>(G::N) * G::N / G::CZ);
+    k_z_forward<T, SRC, LOG2N><<<blocks, G::TZ, G::smem_zf, s>>>(in, H, tw, qsum);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+template <typename T, int LOG2N>
+int z_inverse(const cx_t<T>* H, T* out, const cx_t<T>* tw, cudaStream_t s) {
+    using G = Geo<T, LOG2N>;
+    if (!prepare(k_z_inverse<T, LOG2N>, G::smem_zi)) return -1;
+    const unsigned blocks = static_cast<unsigned>(static_cast<size_t>(G::N) * G::N / G::CZ);
+    k_z_inverse<T, LOG2N><<<blocks, G::TZ, G::smem_zi, s>>>(H, out, tw);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+// AXIS 1: y transforms of every (kc, kx) block; AXIS 0: x transforms of
+// every (kc, ky) column set.
+template <typename T, int LOG2N, int AXIS, int SIGN, bool GREEN, typename GF>
+int columns(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF green, unsigned int* status,
+            cudaStream_t s);
+
+// The complex pass that also applies the Green's function (0: x, 1: y); the
+// other axis is transformed forward after the z pass and inverse before it.
+#ifndef HYOWON_FFT_GREEN_AXIS
+#define HYOWON_FFT_GREEN_AXIS 0
+#endif
+constexpr int kGreenAxis = HYOWON_FFT_GREEN_AXIS;
+constexpr int kPlainAxis = 1 - kGreenAxis;
+
+template <typename T, typename SRC, int LOG2N>
+int forward_t(const Plan* p, const SRC* in, cx_t<T>* H, const cx_t<T>* tw, unsigned long long* qsum,
+              unsigned int* status, cudaStream_t s) {
+    if (z_forward<T, SRC, LOG2N>(in, H, tw, qsum, s) < 0) return -1;
+    if (columns<T, LOG2N, kPlainAxis, -1, false>(p, H, tw, NoGreen{}, status, s) < 0) return -1;
+    return 2;
+}
+
+template <typename T, int LOG2N, typename GF>
+int green_t(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF g, unsigned int* status,
+            cudaStream_t s) {
+    return columns<T, LOG2N, kGreenAxis, -1, true>(p, H, tw, g, status, s);
+}
+
+template <typename T, int LOG2N>
+int inverse_t(const Plan* p, cx_t<T>* H, T* out, const cx_t<T>* tw, unsigned int* status,
+              cudaStream_t s) {
+    if (columns<T, LOG2N, kPlainAxis, +1, false>(p, H, tw, NoGreen{}, status, s) < 0) return -1;
+    if (z_inverse<T, LOG2N>(H, out, tw, s) < 0) return -1;
+    return 2;
+}
+
+template <typename T, int LOG2N, int AXIS, int SIGN, bool GREEN, typename GF>
+int columns(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF green, unsigned int* status,
+            cudaStream_t s) {
+    using G = Geo<T, LOG2N>;
+    if (!p || p->N != G::N) return -1;
+    auto kernel = k_columns<T, LOG2N, AXIS, SIGN, GREEN, GF>;
+    if (!prepare(kernel, G::smem_c)) return -1;
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess
+        || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess
+        || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, G::TC, G::smem_c) != cudaSuccess
+        || per_sm < 1)
+        return -1;
+    const unsigned tiles = static_cast<unsigned>(G::KC) * G::N;
+    const unsigned full = static_cast<unsigned>(sms) * static_cast<unsigned>(per_sm);
+    const unsigned grid = tiles < full ? tiles : full;
+    kernel<<<grid, G::TC, G::smem_c, s>>>(AXIS == 1 ? p->y : p->x, H, tw, green, status);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+    static EncodeTiled fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess
+            || q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return static_cast<EncodeTiled>(nullptr);
+        }
+        return reinterpret_cast<EncodeTiled>(f);
+    }();
+    return fn;
+}
+
+template <typename T, int LOG2N>
+bool encode_maps(Plan* p, void* modes) {
+    using G = Geo<T, LOG2N>;
+    EncodeTiled enc = encode_fn();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(G::units), static_cast<cuuint64_t>(G::N),
+                                static_cast<cuuint64_t>(G::KC) * G::N};
+    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(G::units) * 8,
+                                   static_cast<cuuint64_t>(G::units) * 8 * G::N};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const cuuint32_t box_y[3] = {static_cast<cuuint32_t>(G::units), static_cast<cuuint32_t>(G::box), 1};
+    const cuuint32_t box_x[3] = {static_cast<cuuint32_t>(G::units), 1, static_cast<cuuint32_t>(G::box)};
+    return enc(&p->y, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, modes, dims, strides, box_y, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS
+        && enc(&p->x, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, modes, dims, strides, box_x, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int log2_of(int N) {
+    int l = 0;
+    while ((1 << l) < N) ++l;
+    return l;
+}
+
+#define HYOWON_DISPATCH(N, CALL)              \
+    switch (log2_of(N)) {                     \
+    case 5: { constexpr int LG = 5; return CALL; }   \
+    case 6: { constexpr int LG = 6; return CALL; }   \
+    case 7: { constexpr int LG = 7; return CALL; }   \
+    case 8: { constexpr int LG = 8; return CALL; }   \
+    case 9: { constexpr int LG = 9; return CALL; }   \
+    case 10: { constexpr int LG = 10; return CALL; } \
+    case 11: { constexpr int LG = 11; return CALL; } \
+    default: return -1;                       \
+    }
+
+}  // namespace
+
+bool supported(int N) { return N >= 32 && N <= 2048 && (N & (N - 1)) == 0; }
+
+namespace {
+template <typename T, int LG> constexpr size_t chunked_elements() {
+    return Geo<T, LG>::chunk * Geo<T, LG>::KC;
+}
+template <typename T> size_t chunked_elements(int N) {
+    switch (log2_of(N)) {
+    case 5: return chunked_elements<T, 5>();
+    case 6: return chunked_elements<T, 6>();
+    case 7: return chunked_elements<T, 7>();
+    case 8: return chunked_elements<T, 8>();
+    case 9: return chunked_elements<T, 9>();
+    case 10: return chunked_elements<T, 10>();
+    case 11: return chunked_elements<T, 11>();
+    default: return 0;
+    }
+}
+}  // namespace
+
+size_t modes_elements_f64(int N) { return supported(N) ? chunked_elements<double>(N) : 0; }
+size_t modes_elements_f32(int N) { return supported(N) ? chunked_elements<float>(N) : 0; }
+
+void twiddles(int N, double* re_im) {
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int m = 0; m < N; ++m) {
+        const long double a = two_pi * static_cast<long double>(m) / static_cast<long double>(N);
+        re_im[2 * m] = static_cast<double>(cosl(a));
+        re_im[2 * m + 1] = static_cast<double>(-sinl(a));
+    }
+}
+
+Plan* create_plan(int N, bool fp32, void* modes, const char** err) {
+    if (!supported(N)) {
+        *err = "mesh size not supported by the five-pass solve";
+        return nullptr;
+    }
+    Plan* p = new (std::nothrow) Plan();
+    if (!p) {
+        *err = "out of host memory";
+        return nullptr;
+    }
+    p->N = N;
+    p->fp32 = fp32;
+    bool ok = false;
+    switch (log2_of(N)) {
+    case 5: ok = fp32 ? encode_maps<float, 5>(p, modes) : encode_maps<double, 5>(p, modes); break;
+    case 6: ok = fp32 ? encode_maps<float, 6>(p, modes) : encode_maps<double, 6>(p, modes); break;
+    case 7: ok = fp32 ? encode_maps<float, 7>(p, modes) : encode_maps<double, 7>(p, modes); break;
+    case 8: ok = fp32 ? encode_maps<float, 8>(p, modes) : encode_maps<double, 8>(p, modes); break;
+    case 9: ok = fp32 ? encode_maps<float, 9>(p, modes) : encode_maps<double, 9>(p, modes); break;
+    case 10: ok = fp32 ? encode_maps<float, 10>(p, modes) : encode_maps<double, 10>(p, modes); break;
+    case 11: ok = fp32 ? encode_maps<float, 11>(p, modes) : encode_maps<double, 11>(p, modes); break;
+    default: break;
+    }
+    if (!ok) {
+        delete p;
+        *err = "cuTensorMapEncodeTiled failed for the half-spectrum buffer";
+        return nullptr;
+    }
+    return p;
+}
+
+void destroy_plan(Plan* p) { delete p; }
+
+int forward_f64(const Plan* p, int N, const double* mass, double2* modes, const double2* tw,
+                unsigned int* status, cudaStream_t s) {
+    if (!supported(N) || !p || p->fp32) return -1;
+    HYOWON_DISPATCH(N, (forward_t<double, double, LG>(p, mass, modes, tw, nullptr, status, s)))
+}
+
+int green_f64(const Plan* p, int N, double2* modes, const double2* tw, const GreenF64& g,
+              cudaStream_t s) {
+    if (!supported(N) || !p || p->fp32) return -1;
+    HYOWON_DISPATCH(N, (green_t<double, LG>(p, modes, tw, DevGreenF64{g}, g.status, s)))
+}
+
+int inverse_f64(const Plan* p, int N, double2* modes, double* phi, const double2* tw,
+                unsigned int* status, cudaStream_t s) {
+    if (!supported(N) || !p || p->fp32) return -1;
+    HYOWON_DISPATCH(N, (inverse_t<double, LG>(p, modes, phi, tw, status, s)))
+}
+
+int forward_f32_fixed(const Plan* p, int N, const long long* q, float2* modes, const float2* tw,
+                      unsigned long long* qsum, unsigned int* status, cudaStream_t s) {
+    if (!supported(N) || !p || !p->fp32) return -1;
+    HYOWON_DISPATCH(N, (forward_t<float, long long, LG>(p, q, modes, tw, qsum, status, s)))
+}
+
+int green_f32(const Plan* p, int N, float2* modes, const float2* tw, const GreenF32& g,
+              unsigned int* status, cudaStream_t s) {
+    if (!supported(N) || !p || !p->fp32) return -1;
+    HYOWON_DISPATCH(N, (green_t<float, LG>(p, modes, tw, DevGreenF32{g}, status, s)))
+}
+
+int inverse_f32(const Plan* p, int N, float2* modes, float* phi, const float2* tw,
+                unsigned int* status, cudaStream_t s) {
+    if (!supported(N) || !p || !p->fp32) return -1;
+    HYOWON_DISPATCH(N, (inverse_t<float, LG>(p, modes, phi, tw, status, s)))
+}
+
+}  // namespace poisson
+}  // namespace hyowon

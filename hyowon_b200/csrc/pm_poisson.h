@@ -1,0 +1,82 @@
+// pm_poisson.h -- the pure-PM potential solve on power-of-two meshes
+// (internal interface): mass mesh -> r2c -> Green's multiply -> c2r, as five
+// passes over HBM instead of separate transforms and a Green's kernel.
+//
+//   forward : z pass (real rows -> half-complex rows, r2c of each row) and
+//             y pass (complex transform of every y column),
+//   green   : x pass (forward x transform, Green's multiply in registers,
+//             inverse x transform),
+//   inverse : y pass (inverse) and z pass (c2r of each row).
+//
+// The half spectrum between the passes is kz-chunk-major (see pm_poisson.cu);
+// results equal an unnormalised r2c / c2r pair with the Green's multiply
+// between them.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hyowon {
+namespace poisson {
+
+// Power of two in [32, 2048].
+bool supported(int N);
+
+// Complex elements the half-spectrum buffer must hold (N^2 (N/2+1) rounded up
+// to whole kz chunks).
+size_t modes_elements_f64(int N);
+size_t modes_elements_f32(int N);
+
+// TMA tensor maps of one half-spectrum buffer (built on the host once per
+// buffer). create_plan returns nullptr and sets *err on failure.
+struct Plan;
+Plan* create_plan(int N, bool fp32, void* modes, const char** err);
+void destroy_plan(Plan* p);
+
+// exp(-2 pi i m / N) for m < N as (re, im) pairs, rounded from long double.
+void twiddles(int N, double* re_im);
+
+// Pure-PM Green's function of the binary64 form, evaluated exactly as the
+// separate Green's kernel does (src/mesh/green_function.cpp:165-207): mode
+// (0,0,0) carries the deposited mass, which is checked against input_mass and
+// then zeroed.
+struct GreenF64 {
+    const double* lap;
+    const double* win;
+    double four_pi_G;
+    double scale;
+    int deconvolve;
+    double input_mass;
+    double mass_tol;
+    unsigned int* status;
+};
+
+// Precision form: factor *c_green / (lap sum) [/ W^2], mode (0,0,0) zeroed.
+struct GreenF32 {
+    const float* lap;
+    const float* win;
+    int deconvolve;
+    const float* c_green;
+};
+
+// Each returns the number of kernels launched, or -1 if a launch failed.
+// status receives ST_PIPELINE if a pipelined pass gives up waiting.
+int forward_f64(const Plan* p, int N, const double* mass, double2* modes, const double2* tw,
+                unsigned int* status, cudaStream_t s);
+int green_f64(const Plan* p, int N, double2* modes, const double2* tw, const GreenF64& g,
+              cudaStream_t s);
+int inverse_f64(const Plan* p, int N, double2* modes, double* phi, const double2* tw,
+                unsigned int* status, cudaStream_t s);
+
+// The z pass reads the int64 fixed-point mass offsets directly (rounded to
+// FP32 on load) and adds them, modulo 2^64, into *qsum for the exact mass check.
+int forward_f32_fixed(const Plan* p, int N, const long long* q, float2* modes, const float2* tw,
+                      unsigned long long* qsum, unsigned int* status, cudaStream_t s);
+int green_f32(const Plan* p, int N, float2* modes, const float2* tw, const GreenF32& g,
+              unsigned int* status, cudaStream_t s);
+int inverse_f32(const Plan* p, int N, float2* modes, float* phi, const float2* tw,
+                unsigned int* status, cudaStream_t s);
+
+}  // namespace poisson
+}  // namespace hyowon
