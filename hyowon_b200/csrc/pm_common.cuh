@@ -106,4 +106,57 @@ __device__ __forceinline__ void raise_status(unsigned int* status, unsigned int 
     atomicOr(status, bits);
 }
 
+// Block-wide maximum of non-negative 64-bit values folded into *out with one
+// atomic per block (not per warp: a single address serialises its atomics).
+// Every thread of the block calls it; blockDim.x is a multiple of 32.
+__device__ __forceinline__ void block_max_to(unsigned long long v, unsigned long long* out) {
+    __shared__ unsigned long long part[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    if (lane == 0) part[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < static_cast<int>(blockDim.x >> 5) ? part[lane] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = w > v ? w : v;
+        }
+        if (lane == 0 && v != 0ull) atomicMax(out, v);
+    }
+}
+
+// Block-wide sum modulo 2^64 folded into *out with one atomic per block.
+__device__ __forceinline__ void block_sum_to(unsigned long long v, unsigned long long* out) {
+    __shared__ unsigned long long part[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    if (lane == 0) part[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < static_cast<int>(blockDim.x >> 5) ? part[lane] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v != 0ull) atomicAdd(out, v);
+    }
+}
+
+// Blocks of `threads` for a grid-stride pass over n items: enough to fill
+// every SM with resident blocks, never more than the items need.
+inline unsigned stream_blocks(uint64_t n, int threads) {
+    static int sms = [] {
+        int dev = 0, v = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess
+            || cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            v = 148;
+        return v;
+    }();
+    const uint64_t need = (n + threads - 1) / threads;
+    const uint64_t fill = static_cast<uint64_t>(sms) * (2048 / threads);
+    return static_cast<unsigned>(need < fill ? (need ? need : 1) : fill);
+}
+
 }  // namespace hyowon

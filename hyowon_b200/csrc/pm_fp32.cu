@@ -120,9 +120,9 @@ __global__ void k_kick_drift_key(uint32_t n, const uint32_t* __restrict__ ux,
                                  uint32_t* __restrict__ rank, uint32_t* __restrict__ count,
                                  uint32_t* max_count, unsigned long long* max_drift_bits,
                                  unsigned int* status) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    double drift_norm = 0.0;
-    if (i < n) {
+    double drift_max = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double drift_norm = 0.0;
         const float qx = fmaf(ax[i], K1, px[i]);
         const float qy = fmaf(ay[i], K1, py[i]);
         const float qz = fmaf(az[i], K1, pz[i]);
@@ -162,13 +162,9 @@ __global__ void k_kick_drift_key(uint32_t n, const uint32_t* __restrict__ ux,
             if ((threadIdx.x & 31) == __ffs(peers) - 1)
                 atomicAdd(&count[b], static_cast<uint32_t>(__popc(peers)));
         }
+        drift_max = drift_norm > drift_max ? drift_norm : drift_max;
     }
-    unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(drift_norm));
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
-        bits = other > bits ? other : bits;
-    }
-    if ((threadIdx.x & 31) == 0 && bits != 0ull) atomicMax(max_drift_bits, bits);
+    block_max_to(static_cast<unsigned long long>(__double_as_longlong(drift_max)), max_drift_bits);
 }
 
 __global__ void k_max_count(uint32_t nb, const uint32_t* __restrict__ count, uint32_t* max_count) {
@@ -253,8 +249,7 @@ __global__ void k_convert(uint64_t cells, const long long* __restrict__ q, float
         r[i] = __ll2float_rn(v);
         local += static_cast<unsigned long long>(v);
     }
-    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(qsum, local);
+    block_sum_to(local, qsum);
 }
 
 __global__ void k_check_mass(const unsigned long long* qsum, const FixedPlan* plan,
@@ -904,7 +899,7 @@ int kdk_step(State* st, cudaStream_t s, unsigned int* d_status, unsigned long lo
     rec(ev, 0, s);
     const int pc = st->pc, mc = st->mc;
     ++st->launches;
-    k_kick_drift_key<<<blocks_for(n), kThreads, 0, s>>>(
+    k_kick_drift_key<<<stream_blocks(n, kThreads), kThreads, 0, s>>>(
         n, st->pos[pc][0], st->pos[pc][1], st->pos[pc][2], st->mom[mc][0], st->mom[mc][1],
         st->mom[mc][2], st->acc[0], st->acc[1], st->acc[2], static_cast<float>(K1), D,
         kTwo32 / st->L, st->N, st->pos[1 - pc][0], st->pos[1 - pc][1], st->pos[1 - pc][2],

@@ -74,9 +74,9 @@ __global__ void k_kick_drift_key(uint32_t n, const double* __restrict__ x,
                                  uint32_t* __restrict__ rank, uint32_t* __restrict__ count,
                                  int shift, int with_key, unsigned long long* max_drift_bits,
                                  unsigned int* status) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    double drift_norm = 0.0;
-    if (i < n) {
+    double drift_max = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double drift_norm = 0.0;
         const double qx = px[i] + ax[i] * K1;
         const double qy = py[i] + ay[i] * K1;
         const double qz = pz[i] + az[i] * K1;
@@ -112,14 +112,10 @@ __global__ void k_kick_drift_key(uint32_t n, const double* __restrict__ x,
             key[i] = b;
             rank[i] = bucket_rank(count, b);
         }
+        drift_max = drift_norm > drift_max ? drift_norm : drift_max;
     }
     // Non-negative doubles order like their bit patterns.
-    unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(drift_norm));
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
-        bits = other > bits ? other : bits;
-    }
-    if ((threadIdx.x & 31) == 0 && bits != 0ull) atomicMax(max_drift_bits, bits);
+    block_max_to(static_cast<unsigned long long>(__double_as_longlong(drift_max)), max_drift_bits);
 }
 
 // CIC deposit (src/mesh/mass_assignment_deposit.inc:193-240): each particle adds
@@ -487,7 +483,7 @@ void launch_kick_drift_key_f64(uint32_t n, const ParticlesF64& cur, const double
                                bool with_key, unsigned long long* max_drift_bits,
                                unsigned int* status, cudaStream_t s) {
     if (n == 0) return;
-    k_kick_drift_key<<<blocks_for(n), kThreads, 0, s>>>(
+    k_kick_drift_key<<<stream_blocks(n, kThreads), kThreads, 0, s>>>(
         n, cur.x, cur.y, cur.z, cur.px, cur.py, cur.pz, ax, ay, az, K1, D, a, cand.x, cand.y,
         cand.z, cand.px, cand.py, cand.pz, w.key, w.rank, w.count, w.shift, with_key ? 1 : 0,
         max_drift_bits, status);

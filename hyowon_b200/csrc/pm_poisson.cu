@@ -140,9 +140,8 @@ k_z_forward(const SRC* __restrict__ in, cx_t<T>* __restrict__ H, const cx_t<T>* 
         sm[(e % G::M) * S + e / G::M] = to_complex(raw[i], sum);
     }
     if (qsum) {
-        if constexpr (G::TZ >= 32) {
-            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-            if ((tid & 31) == 0 && sum) atomicAdd(qsum, sum);
+        if constexpr (G::TZ >= 32 && G::TZ % 32 == 0) {
+            block_sum_to(sum, qsum);
         } else {
             if (sum) atomicAdd(qsum, sum);
         }
