@@ -197,59 +197,140 @@ __global__ void k_plan(uint32_t n, uint64_t cells, const uint32_t* max_count, do
     plan->c_green = static_cast<float>(ldexp(c0, -3 * B));
 }
 
-__global__ void k_fill(uint64_t cells, long long* __restrict__ q, const FixedPlan* plan) {
-    const long long v = -plan->mean_q;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cells;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        q[i] = v;
-}
+__device__ __forceinline__ void store_cell(float* out, long long q) { *out = __ll2float_rn(q); }
+__device__ __forceinline__ void store_cell(long long* out, long long q) { *out = q; }
 
-__global__ void k_deposit(uint32_t n, const uint32_t* __restrict__ ux,
-                          const uint32_t* __restrict__ uy, const uint32_t* __restrict__ uz, int N,
-                          unsigned long long* __restrict__ q, const FixedPlan* plan,
-                          const unsigned int* status) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+// Owner-computes fixed-point deposit: one block per tile of TY mesh rows
+// (x0, y0 .. y0+TY-1, all z) accumulating int64 weights in shared memory
+// (integer atomics: the result does not depend on their order), then writing
+// each cell once as its offset from the mean, q - mean_q (FP32 for the
+// transform, or int64 exactly), and folding the offsets into *qsum (mod 2^64)
+// for the exact mass check. Contributors are the particles whose base cell
+// lies in rows (x0 or x0-1, y0-1 .. y0+TY-1), found through the cell order of
+// the current positions (`offset` bucket starts; `order` sorted slot ->
+// particle, or null when the arrays are in cell order). The contributor
+// ranges of all rows are concatenated so every thread walks one flat list,
+// loading kDepositBatch particles at a time.
+constexpr int kDepositThreads = 256;
+constexpr int kDepositBatch = 4;
+constexpr int kMaxTileRows = 2 * (90 + 1);   // 2 (TY + 1) with TY <= max(8192 / N, N <= 90)
+
+template <typename OUT>
+__global__ void __launch_bounds__(kDepositThreads)
+k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy,
+                const uint32_t* __restrict__ uz, const uint32_t* __restrict__ order,
+                const uint32_t* __restrict__ offset, int shift, int N, int TY,
+                const FixedPlan* plan, OUT* __restrict__ out, unsigned long long* qsum,
+                const unsigned int* status) {
+    extern __shared__ unsigned long long qtile[];
+    __shared__ uint32_t r_p0[kMaxTileRows];
+    __shared__ uint32_t r_cum[kMaxTileRows + 1];
+    __shared__ uint32_t warp_tot[kDepositThreads / 32];
+    if (*status & ST_BLOCKS_PUBLISH) return;
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.y;
+    const int y0 = blockIdx.x * TY;
+    const int ty = N - y0 < TY ? N - y0 : TY;
+    // contributor rows: r = xr * nyr + k, xb = x0 - xr, yb = y0 + k - halo
+    const int halo = ty == N ? 0 : 1;   // a tile spanning all rows has no halo
+    const int nyr = ty + halo;
+    const int nrows = 2 * nyr;
+    uint32_t len = 0;
+    if (tid < nrows) {
+        const int xr = tid / nyr;
+        const uint32_t xb = xr == 0 ? x0 : (x0 == 0 ? N - 1 : x0 - 1);
+        const int yy = y0 + tid % nyr - halo;
+        const uint32_t yb = static_cast<uint32_t>(yy < 0 ? yy + N : yy);
+        const uint64_t c0 = (static_cast<uint64_t>(xb) * N + yb) * N;
+        const uint32_t p0 = offset[c0 >> shift];
+        r_p0[tid] = p0;
+        len = offset[((c0 + N - 1) >> shift) + 1] - p0;
+    }
+    // block-wide inclusive scan of the range lengths (nrows <= blockDim)
+    uint32_t incl = len;
+    const int lane = tid & 31;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[tid >> 5] = incl;
+    for (int e = tid; e < ty * N; e += kDepositThreads) qtile[e] = 0ull;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < (tid >> 5); ++w) before += warp_tot[w];
+    if (tid < nrows) r_cum[tid + 1] = before + incl;
+    if (tid == 0) r_cum[0] = 0;
+    __syncthreads();
+    const uint32_t total = r_cum[nrows];
     const int B = plan->B;
     const unsigned one = 1u << B;
-    uint32_t fx, fy, fz;
-    const uint32_t ix = cell_of(ux[i], N, fx);
-    const uint32_t iy = cell_of(uy[i], N, fy);
-    const uint32_t iz = cell_of(uz[i], N, fz);
-    fx >>= (32 - B);
-    fy >>= (32 - B);
-    fz >>= (32 - B);
-    const unsigned long long wx[2] = {one - fx, fx};
-    const unsigned long long wy[2] = {one - fy, fy};
-    const unsigned long long wz[2] = {one - fz, fz};
-    const uint32_t gx[2] = {ix, ix + 1 == static_cast<uint32_t>(N) ? 0u : ix + 1};
-    const uint32_t gy[2] = {iy, iy + 1 == static_cast<uint32_t>(N) ? 0u : iy + 1};
-    const uint32_t gz[2] = {iz, iz + 1 == static_cast<uint32_t>(N) ? 0u : iz + 1};
+    int r = 0;
+    for (uint32_t v0 = tid; v0 < total; v0 += kDepositBatch * kDepositThreads) {
+        uint32_t idx[kDepositBatch];
+        int row[kDepositBatch];
 #pragma unroll
-    for (int a = 0; a < 2; ++a) {
+        for (int k = 0; k < kDepositBatch; ++k) {
+            const uint32_t v = v0 + k * kDepositThreads;
+            row[k] = -1;
+            if (v < total) {
+                while (r_cum[r + 1] <= v) ++r;
+                row[k] = r;
+                const uint32_t q = r_p0[r] + (v - r_cum[r]);
+                idx[k] = order ? order[q] : q;
+            }
+        }
+        uint32_t u[kDepositBatch][3];
 #pragma unroll
-        for (int b = 0; b < 2; ++b) {
-            const unsigned long long wab = wx[a] * wy[b];
+        for (int k = 0; k < kDepositBatch; ++k) {
+            if (row[k] >= 0) {
+                u[k][0] = ux[idx[k]];
+                u[k][1] = uy[idx[k]];
+                u[k][2] = uz[idx[k]];
+            }
+        }
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                const unsigned long long w = wab * wz[c];
-                if (w) atomicAdd(&q[cell_index(gx[a], gy[b], gz[c], N)], w);
+        for (int k = 0; k < kDepositBatch; ++k) {
+            if (row[k] < 0) continue;
+            const int xr = row[k] / nyr;
+            const uint32_t xb = xr == 0 ? x0 : (x0 == 0 ? N - 1 : x0 - 1);
+            const int yy = y0 + row[k] % nyr - halo;
+            const uint32_t yb = static_cast<uint32_t>(yy < 0 ? yy + N : yy);
+            uint32_t fx, fy, fz;
+            const uint32_t ix = cell_of(u[k][0], N, fx);
+            const uint32_t iy = cell_of(u[k][1], N, fy);
+            const uint32_t iz = cell_of(u[k][2], N, fz);
+            if (ix != xb || iy != yb) continue;  // a bucket wider than this row
+            fx >>= (32 - B);
+            fy >>= (32 - B);
+            fz >>= (32 - B);
+            const unsigned long long wx = xr == 0 ? one - fx : fx;
+            const unsigned long long wy[2] = {one - fy, fy};
+            const unsigned long long wz[2] = {one - fz, fz};
+            const uint32_t gz[2] = {iz, iz + 1 == static_cast<uint32_t>(N) ? 0u : iz + 1};
+#pragma unroll
+            for (int oy = 0; oy < 2; ++oy) {
+                const uint32_t ys = yb + oy == static_cast<uint32_t>(N) ? 0u : yb + oy;
+                const int ly = static_cast<int>(ys) - y0;
+                if (ly < 0 || ly >= ty) continue;
+                const unsigned long long wxy = wx * wy[oy];
+#pragma unroll
+                for (int oz = 0; oz < 2; ++oz) {
+                    const unsigned long long w = wxy * wz[oz];
+                    if (w) atomicAdd(&qtile[ly * N + gz[oz]], w);
+                }
             }
         }
     }
-}
-
-// int64 offsets -> FP32 real mesh, with the exact (modular) mesh-sum check.
-__global__ void k_convert(uint64_t cells, const long long* __restrict__ q, float* __restrict__ r,
-                          unsigned long long* qsum) {
+    __syncthreads();
+    const long long mean = plan->mean_q;
+    OUT* o = out + (static_cast<uint64_t>(x0) * N + y0) * N;
     unsigned long long local = 0;
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < cells;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const long long v = q[i];
-        r[i] = __ll2float_rn(v);
+    for (int e = tid; e < ty * N; e += kDepositThreads) {
+        const long long v = static_cast<long long>(qtile[e]) - mean;
+        store_cell(&o[e], v);
         local += static_cast<unsigned long long>(v);
     }
-    block_sum_to(local, qsum);
+    if (qsum) block_sum_to(local, qsum);
 }
 
 __global__ void k_check_mass(const unsigned long long* qsum, const FixedPlan* plan,
@@ -493,7 +574,10 @@ struct State {
     uint32_t* d_max_count = nullptr;
     FixedPlan* d_plan = nullptr;
     unsigned long long* d_qsum = nullptr;
-    long long* qmesh = nullptr;
+    uint32_t* order = nullptr;   // cell order of unmoved particles (steps between re-sorts)
+    bool order_perm = false;     // the current positions' cell order is `order` (else identity)
+    bool step_perm = false;      // same, for the positions of the step in flight
+    bool order_state_invalid = true;  // offsets/order do not describe the current positions
     float* rmesh = nullptr;
     float2* modes = nullptr;
     float2* phi_k = nullptr;
@@ -557,6 +641,8 @@ void free_particles(State* st) {
     }
     cudaFree(st->sort.key);
     cudaFree(st->sort.rank);
+    cudaFree(st->order);
+    st->order = nullptr;
     st->sort.key = st->sort.rank = nullptr;
     st->cap = 0;
 }
@@ -574,6 +660,7 @@ int ensure(State* st, uint32_t n) {
         for (int a = 0; a < 3; ++a) CK(dalloc(&st->acc[a], n));
         CK(dalloc(&st->sort.key, n));
         CK(dalloc(&st->sort.rank, n));
+        CK(dalloc(&st->order, n));
         st->cap = n;
     }
     const uint64_t cells = static_cast<uint64_t>(st->N) * st->N * st->N;
@@ -618,7 +705,6 @@ int create(State** out, double L, int N, int method, int deconvolve, double r_s,
     st->four_pi_G = four_pi_G;
     const size_t cells = static_cast<size_t>(N) * N * N;
     const size_t half = static_cast<size_t>(N) * N * (N / 2 + 1);
-    CK(dalloc(&st->qmesh, cells));
     CK(dalloc(&st->rmesh, cells));
     const size_t modes_n = method == HYOWON_PURE_PM && poisson::supported(N)
         ? std::max(half, poisson::modes_elements_f32(N)) : half;
@@ -677,7 +763,6 @@ void destroy(State* st) {
     cudaFree(st->fft_work);
     cudaFree(st->tw);
     poisson::destroy_plan(st->fft_plan);
-    cudaFree(st->qmesh);
     cudaFree(st->rmesh);
     cudaFree(st->modes);
     cudaFree(st->phi_k);
@@ -775,22 +860,48 @@ int sort_current(State* st, cudaStream_t s, unsigned int* d_status) {
     st->pc = 1 - st->pc;
     st->mc = 1 - st->mc;
     st->ic = 1 - st->ic;
+    st->order_perm = false;
+    st->order_state_invalid = false;
     return HYOWON_OK;
 }
 
 namespace {
 int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool kick, double K2,
-                       cudaEvent_t* ev, int P, int M);
+                       cudaEvent_t* ev, int P, int M, const uint32_t* order);
+
+// Owner-computes deposit of position set P into `out` (FP32 offsets for the
+// transform, or exact int64), see k_deposit_tiles.
+template <typename OUT>
+int deposit_tiles(State* st, int P, const uint32_t* order, OUT* out, unsigned long long* qsum,
+                  const unsigned int* d_status, cudaStream_t s) {
+    const int N = st->N;
+    const int TY = deposit_tile_rows(N);
+    const size_t smem = sizeof(unsigned long long) * static_cast<size_t>(TY) * N;
+    CK(cudaFuncSetAttribute(k_deposit_tiles<OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(smem)));
+    const dim3 grid((N + TY - 1) / TY, N);
+    ++st->launches;
+    k_deposit_tiles<OUT><<<grid, kDepositThreads, smem, s>>>(st->pos[P][0], st->pos[P][1], st->pos[P][2],
+                                                 order, st->sort.offset, st->sort.shift, N, TY,
+                                                 st->d_plan, out, qsum, d_status);
+    CK(cudaPeekAtLastError());
+    return HYOWON_OK;
+}
 }
 
 int enqueue_force(State* st, cudaStream_t s, unsigned int* d_status, bool kick, double K2,
                   cudaEvent_t* ev) {
-    return enqueue_force_sets(st, s, d_status, kick, K2, ev, st->pc, st->mc);
+    if (st->order_state_invalid) {
+        const int rc = sort_current(st, s, d_status);
+        if (rc) return rc;
+    }
+    return enqueue_force_sets(st, s, d_status, kick, K2, ev, st->pc, st->mc,
+                              st->order_perm ? st->order : nullptr);
 }
 
 namespace {
 int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool kick, double K2,
-                       cudaEvent_t* ev, int P, int M) {
+                       cudaEvent_t* ev, int P, int M, const uint32_t* order) {
     const uint32_t n = st->n;
     const int N = st->N;
     const uint64_t cells = static_cast<uint64_t>(N) * N * N;
@@ -798,25 +909,20 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
     rec(ev, 1, s);
     ++st->launches;
     k_plan<<<1, 32, 0, s>>>(n, cells, st->d_max_count, green_c0(st), 1, st->d_plan);
-    ++st->launches;
-    k_fill<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->d_plan);
-    ++st->launches;
-    k_deposit<<<blocks_for(n), kThreads, 0, s>>>(
-        n, st->pos[P][0], st->pos[P][1], st->pos[P][2], N,
-        reinterpret_cast<unsigned long long*>(st->qmesh), st->d_plan, d_status);
     CK(cudaMemsetAsync(st->d_qsum, 0, sizeof(unsigned long long), s));
+    int rc = deposit_tiles<float>(st, P, order, st->rmesh, st->d_qsum, d_status, s);
+    if (rc) return rc;
+    ++st->launches;
+    k_check_mass<<<1, 32, 0, s>>>(st->d_qsum, st->d_plan, d_status);
     float* const pxo = st->mom[1 - M][0];
     float* const pyo = st->mom[1 - M][1];
     float* const pzo = st->mom[1 - M][2];
     const float K2f = static_cast<float>(K2);
     if (st->five_pass) {
         rec(ev, 2, s);
-        int k = poisson::forward_f32_fixed(st->fft_plan, N, st->qmesh, st->modes, st->tw, st->d_qsum,
-                                           d_status, s);
+        int k = poisson::forward_f32(st->fft_plan, N, st->rmesh, st->modes, st->tw, d_status, s);
         if (k < 0) return fail(st, HYOWON_ECUDA, "potential solve: forward pass launch failed");
         st->launches += k;
-        ++st->launches;
-        k_check_mass<<<1, 32, 0, s>>>(st->d_qsum, st->d_plan, d_status);
         rec(ev, 3, s);
         const float* c_green = reinterpret_cast<const float*>(
             reinterpret_cast<const char*>(st->d_plan) + offsetof(FixedPlan, c_green));
@@ -838,10 +944,6 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
         rec(ev, 6, s);
         return HYOWON_OK;
     }
-    ++st->launches;
-    k_convert<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->rmesh, st->d_qsum);
-    ++st->launches;
-    k_check_mass<<<1, 32, 0, s>>>(st->d_qsum, st->d_plan, d_status);
     rec(ev, 2, s);
     CKFFT(cufftExecR2C(st->r2c, st->rmesh, reinterpret_cast<cufftComplex*>(st->modes)));
     rec(ev, 3, s);
@@ -904,14 +1006,20 @@ int kdk_step(State* st, cudaStream_t s, unsigned int* d_status, unsigned long lo
         st->mom[mc][2], st->acc[0], st->acc[1], st->acc[2], static_cast<float>(K1), D,
         kTwo32 / st->L, st->N, st->pos[1 - pc][0], st->pos[1 - pc][1], st->pos[1 - pc][2],
         st->mom[1 - mc][0], st->mom[1 - mc][1], st->mom[1 - mc][2], st->sort.shift,
-        sort_now ? 1 : 0, st->sort.key, st->sort.rank, st->sort.count, st->d_max_count,
-        d_maxdrift, d_status);
+        1, st->sort.key, st->sort.rank, st->sort.count, st->d_max_count, d_maxdrift, d_status);
     st->step_sorted = sort_now;
     st->ic_before = st->ic;
     int P = 1 - pc, M = 1 - mc;
+    // cell order of the candidate positions: bucket offsets every step; the
+    // particle arrays themselves are permuted only on re-sort steps
+    st->launches += launch_exclusive_scan(st->sort.count, st->sort.offset, st->sort.n_buckets + 1,
+                                          st->sort.scan_tmp, s);
+    st->step_perm = !sort_now;
+    if (!sort_now) {
+        ++st->launches;
+        launch_order(n, st->sort.key, st->sort.rank, st->sort.offset, st->order, d_status, s);
+    }
     if (sort_now) {
-        st->launches += launch_exclusive_scan(st->sort.count, st->sort.offset, st->sort.n_buckets + 1,
-                              st->sort.scan_tmp, s);
         const uint32_t* src[7];
         uint32_t* dst[7];
         for (int a = 0; a < 3; ++a) {
@@ -934,7 +1042,8 @@ int kdk_step(State* st, cudaStream_t s, unsigned int* d_status, unsigned long lo
                                                      st->d_max_count);
     st->step_P = P;
     st->step_M = M;
-    return enqueue_force_sets(st, s, d_status, true, K2, ev, P, M);
+    return enqueue_force_sets(st, s, d_status, true, K2, ev, P, M,
+                              st->step_perm ? st->order : nullptr);
 }
 
 uint64_t launches(const State* st) { return st->launches; }
@@ -944,8 +1053,11 @@ void set_sort_interval(State* st, int steps) { st->sort_interval = steps < 1 ? 1
 void commit_step(State* st, bool published, bool ok) {
     if (!published) {
         st->ic = st->ic_before;
+        st->order_state_invalid = true;  // offsets describe the unpublished candidate
         return;
     }
+    st->order_perm = st->step_perm;
+    st->order_state_invalid = false;
     st->pc = st->step_P;
     st->mc = ok ? 1 - st->step_M : st->step_M;
     st->since_sort = st->step_sorted ? 0 : st->since_sort + 1;
@@ -995,25 +1107,29 @@ int download_potential(State* st, cudaStream_t s, double* phi) {
 int download_mass_mesh(State* st, cudaStream_t s, unsigned int* d_status, double* mesh) {
     const uint32_t n = st->n;
     const uint64_t cells = static_cast<uint64_t>(st->N) * st->N * st->N;
+    if (st->order_state_invalid) {
+        const int rc = sort_current(st, s, d_status);
+        if (rc) return rc;
+    }
     ++st->launches;
     k_plan<<<1, 32, 0, s>>>(n, cells, st->d_max_count, green_c0(st), 0, st->d_plan);
-    ++st->launches;
-    k_fill<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->d_plan);
-    cudaMemsetAsync(d_status, 0, sizeof(unsigned int), s);
-    ++st->launches;
-    k_deposit<<<blocks_for(n), kThreads, 0, s>>>(n, st->pos[st->pc][0], st->pos[st->pc][1],
-                                                 st->pos[st->pc][2], st->N,
-                                                 reinterpret_cast<unsigned long long*>(st->qmesh),
-                                                 st->d_plan, d_status);
+    CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned int), s));
+    long long* q = nullptr;
+    CK(dalloc(&q, cells));
+    int rc = deposit_tiles<long long>(st, st->pc, st->order_perm ? st->order : nullptr, q, nullptr,
+                                      d_status, s);
     double* d = nullptr;
-    CK(dalloc(&d, cells));
-    ++st->launches;
-    k_mass_mesh<<<st->fill_blocks, kThreads, 0, s>>>(cells, st->qmesh, st->d_plan, st->uniform_mass, d);
-    const cudaError_t e = cudaMemcpyAsync(mesh, d, sizeof(double) * cells, cudaMemcpyDeviceToHost, s);
-    const cudaError_t e2 = cudaStreamSynchronize(s);
+    if (rc == HYOWON_OK && dalloc(&d, cells) != cudaSuccess) rc = fail(st, HYOWON_ENOMEM, "mass mesh staging");
+    if (rc == HYOWON_OK) {
+        ++st->launches;
+        k_mass_mesh<<<st->fill_blocks, kThreads, 0, s>>>(cells, q, st->d_plan, st->uniform_mass, d);
+        const cudaError_t e = cudaMemcpyAsync(mesh, d, sizeof(double) * cells, cudaMemcpyDeviceToHost, s);
+        const cudaError_t e2 = cudaStreamSynchronize(s);
+        if (e != cudaSuccess || e2 != cudaSuccess) rc = fail(st, HYOWON_ECUDA, "mass mesh copy failed");
+    }
     cudaFree(d);
-    if (e != cudaSuccess || e2 != cudaSuccess) return fail(st, HYOWON_ECUDA, "mass mesh copy failed");
-    return HYOWON_OK;
+    cudaFree(q);
+    return rc;
 }
 
 }  // namespace hyowon::fp32

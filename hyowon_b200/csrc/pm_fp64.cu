@@ -338,13 +338,64 @@ __device__ __forceinline__ void gather_axis(const double (&c)[2][2][2], const do
     }
 }
 
+// Binary exponent field of |v| (0 for zero and subnormals).
+__device__ __forceinline__ int exp_field(double v) {
+    return static_cast<int>((static_cast<unsigned long long>(__double_as_longlong(v)) >> 52) & 0x7ffu);
+}
+
+// Fast form of one gather axis: -(sum_corners w * dphi) / (2 dx), corners in
+// the reference's order, one scaling at the end. Used when no product can
+// reach the subnormal range: every non-zero weight factor >= 2^-250 (so
+// w >= 2^-750), every non-zero potential difference >= 2^-200 and
+// 1/(2dx) >= 2^-50, so |w dphi / (2dx)| >= 2^-1000 stays normal and the
+// reference's lost-product checks cannot fire. Differs from the per-corner
+// quotient sequence only in rounding (a few ulp of the axis sum). Returns
+// false (nothing accumulated) when the exact sequence is needed instead.
+template <int AXIS>
+__device__ __forceinline__ bool gather_axis_fast(const double (&c)[2][2][2], const double (&lo)[2][2],
+                                                 const double (&hi)[2][2], const double (&w)[2][2][2],
+                                                 double inv_two_dx, double& sum) {
+    double dv[2][2][2];
+    bool ok = true;
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox)
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy)
+#pragma unroll
+            for (int oz = 0; oz < 2; ++oz) {
+                double d;
+                if (AXIS == 0)
+                    d = (ox == 0 ? c[1][oy][oz] : hi[oy][oz]) - (ox == 0 ? lo[oy][oz] : c[0][oy][oz]);
+                else if (AXIS == 1)
+                    d = (oy == 0 ? c[ox][1][oz] : hi[ox][oz]) - (oy == 0 ? lo[ox][oz] : c[ox][0][oz]);
+                else
+                    d = (oz == 0 ? c[ox][oy][1] : hi[ox][oy]) - (oz == 0 ? lo[ox][oy] : c[ox][oy][0]);
+                const int e = exp_field(d);
+                ok &= d == 0.0 || e >= 1023 - 200;
+                dv[ox][oy][oz] = d;
+            }
+    if (!ok) return false;
+    double s = 0.0;
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox)
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy)
+#pragma unroll
+            for (int oz = 0; oz < 2; ++oz) s = fma(w[ox][oy][oz], dv[ox][oy][oz], s);
+    sum = -(s * inv_two_dx);
+    return true;
+}
+
 // interpolate_centered_gradient3_add_full_mesh
 // (src/mesh/mass_assignment_gradient.cpp:117-206) into zeroed accelerations,
 // fused with the K2 kick (leapfrog_integrator.cpp:240-278). The 32 distinct
 // potential values of the 4x4x4 stencil footprint are loaded once: the 2x2x2
 // block first, then the two outer faces of one axis at a time, so each axis
 // sum is formed in the reference's corner order with few values live.
-__global__ void __launch_bounds__(kThreads, 3)
+#ifndef HYOWON_GATHER64_MINB
+#define HYOWON_GATHER64_MINB 3
+#endif
+__global__ void __launch_bounds__(kThreads, HYOWON_GATHER64_MINB)
 k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restrict__ x,
               const double* __restrict__ y, const double* __restrict__ z,
               const double* __restrict__ px, const double* __restrict__ py,
@@ -382,6 +433,22 @@ k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restri
     const double two_dx = 2.0 * a.dx;
     double gx_sum = 0.0, gy_sum = 0.0, gz_sum = 0.0;
     bool lost = false;
+    // weights in the reference's product order, and whether every non-zero
+    // factor is far from the subnormal range (see gather_axis_fast)
+    double w[2][2][2];
+    bool fast = exp_field(inv_two_dx) >= 1023 - 50 && exp_field(inv_two_dx) < 0x7ff;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        fast &= (wx[q] == 0.0 || exp_field(wx[q]) >= 1023 - 250)
+            && (wy[q] == 0.0 || exp_field(wy[q]) >= 1023 - 250)
+            && (wz[q] == 0.0 || exp_field(wz[q]) >= 1023 - 250);
+    }
+#pragma unroll
+    for (int ox = 0; ox < 2; ++ox)
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy)
+#pragma unroll
+            for (int oz = 0; oz < 2; ++oz) w[ox][oy][oz] = wx[ox] * wy[oy] * wz[oz];
     double lo[2][2], hi[2][2];
 #pragma unroll
     for (int u = 0; u < 2; ++u)
@@ -390,7 +457,8 @@ k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restri
             lo[u][v] = PHI(0, u + 1, v + 1);
             hi[u][v] = PHI(3, u + 1, v + 1);
         }
-    gather_axis<0>(c, lo, hi, wx, wy, wz, two_dx, inv_two_dx, gx_sum, lost);
+    if (!(fast && gather_axis_fast<0>(c, lo, hi, w, inv_two_dx, gx_sum)))
+        gather_axis<0>(c, lo, hi, wx, wy, wz, two_dx, inv_two_dx, gx_sum, lost);
 #pragma unroll
     for (int u = 0; u < 2; ++u)
 #pragma unroll
@@ -398,7 +466,8 @@ k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restri
             lo[u][v] = PHI(u + 1, 0, v + 1);
             hi[u][v] = PHI(u + 1, 3, v + 1);
         }
-    gather_axis<1>(c, lo, hi, wx, wy, wz, two_dx, inv_two_dx, gy_sum, lost);
+    if (!(fast && gather_axis_fast<1>(c, lo, hi, w, inv_two_dx, gy_sum)))
+        gather_axis<1>(c, lo, hi, wx, wy, wz, two_dx, inv_two_dx, gy_sum, lost);
 #pragma unroll
     for (int u = 0; u < 2; ++u)
 #pragma unroll
@@ -406,7 +475,8 @@ k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restri
             lo[u][v] = PHI(u + 1, v + 1, 0);
             hi[u][v] = PHI(u + 1, v + 1, 3);
         }
-    gather_axis<2>(c, lo, hi, wx, wy, wz, two_dx, inv_two_dx, gz_sum, lost);
+    if (!(fast && gather_axis_fast<2>(c, lo, hi, w, inv_two_dx, gz_sum)))
+        gather_axis<2>(c, lo, hi, wx, wy, wz, two_dx, inv_two_dx, gz_sum, lost);
 #undef PHI
     if (lost) raise_status(status, ST_UNDERFLOW);
     // The evolution path adds into zeroed accelerations (leapfrog_integrator.cpp:75-83).
@@ -496,6 +566,8 @@ void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,
     k_deposit<<<blocks_for(n), kThreads, 0, s>>>(n, p.x, p.y, p.z, mass, uniform_mass, a,
                                                  mesh, status);
 }
+
+
 
 void launch_green_f64(int N, double2* modes, const double* lap, const double* win,
                       double four_pi_G, double scale, int deconvolve, double input_mass,

@@ -473,6 +473,7 @@ int kdk_step_impl(hyowon_pm_t h, double K1, double D, double K2, double* max_dri
         collect_timing(h);
         const bool published = (st & ST_BLOCKS_PUBLISH) == 0;
         fp32::commit_step(h->f32, published, st == 0);
+        if (!published) h->sorted = false;  // the form re-sorts before its next solve
         if (st) {
             h->acc_valid = false;
             return status_to_code(h, st);

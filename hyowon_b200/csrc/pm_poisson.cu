@@ -12,7 +12,7 @@
 // (memory and transform work +1/(N/(2 CC)+1)).
 //
 // Bytes moved per solve on an N^3 mesh with b-byte reals: z forward reads the
-// N^3 mass values (int64 in the precision form) and writes H, the x, y(+Green)
+// N^3 mass values and writes H, the x, y(+Green)
 // and x passes read and write H in place, z inverse reads H and writes the
 // N^3 potential.
 #include "pm_poisson.h"
@@ -103,15 +103,12 @@ template <typename T, int LOG2N> struct Geo {
     static constexpr int units = CC * static_cast<int>(sizeof(C)) / 8;  // 8-byte units per row
 };
 
-template <typename S> struct Raw;   // 16-byte raw row pair of the z forward input
+template <typename S> struct Raw;   // raw row pair of the z forward input
 template <> struct Raw<double> { using type = double2; };
-template <> struct Raw<long long> { using type = longlong2; };
+template <> struct Raw<float> { using type = float2; };
 
 __device__ __forceinline__ double2 to_complex(double2 v, unsigned long long&) { return v; }
-__device__ __forceinline__ float2 to_complex(longlong2 v, unsigned long long& sum) {
-    sum += static_cast<unsigned long long>(v.x) + static_cast<unsigned long long>(v.y);
-    return make_float2(__ll2float_rn(v.x), __ll2float_rn(v.y));
-}
+__device__ __forceinline__ float2 to_complex(float2 v, unsigned long long&) { return v; }
 
 // r2c of CZ rows per block: pack the N reals of a row as N/2 complex values,
 // transform, and unpack X[k] = E[k] + W_N^k O[k] with E/O the transforms of
@@ -586,10 +583,10 @@ int inverse_f64(const Plan* p, int N, double2* modes, double* phi, const double2
     HYOWON_DISPATCH(N, (inverse_t<double, LG>(p, modes, phi, tw, status, s)))
 }
 
-int forward_f32_fixed(const Plan* p, int N, const long long* q, float2* modes, const float2* tw,
-                      unsigned long long* qsum, unsigned int* status, cudaStream_t s) {
+int forward_f32(const Plan* p, int N, const float* mesh, float2* modes, const float2* tw,
+                unsigned int* status, cudaStream_t s) {
     if (!supported(N) || !p || !p->fp32) return -1;
-    HYOWON_DISPATCH(N, (forward_t<float, long long, LG>(p, q, modes, tw, qsum, status, s)))
+    HYOWON_DISPATCH(N, (forward_t<float, float, LG>(p, mesh, modes, tw, nullptr, status, s)))
 }
 
 int green_f32(const Plan* p, int N, float2* modes, const float2* tw, const GreenF32& g,

@@ -69,10 +69,8 @@ int green_f64(const Plan* p, int N, double2* modes, const double2* tw, const Gre
 int inverse_f64(const Plan* p, int N, double2* modes, double* phi, const double2* tw,
                 unsigned int* status, cudaStream_t s);
 
-// The z pass reads the int64 fixed-point mass offsets directly (rounded to
-// FP32 on load) and adds them, modulo 2^64, into *qsum for the exact mass check.
-int forward_f32_fixed(const Plan* p, int N, const long long* q, float2* modes, const float2* tw,
-                      unsigned long long* qsum, unsigned int* status, cudaStream_t s);
+int forward_f32(const Plan* p, int N, const float* mesh, float2* modes, const float2* tw,
+                unsigned int* status, cudaStream_t s);
 int green_f32(const Plan* p, int N, float2* modes, const float2* tw, const GreenF32& g,
               unsigned int* status, cudaStream_t s);
 int inverse_f32(const Plan* p, int N, float2* modes, float* phi, const float2* tw,

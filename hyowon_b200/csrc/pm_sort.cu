@@ -127,6 +127,16 @@ __global__ void k_unpermute(uint32_t n, const uint32_t* __restrict__ id,
     dst[id[i]] = src[i];
 }
 
+// Cell order of the particles without moving them: order[offset[key]+rank] = i.
+__global__ void k_order(uint32_t n, const uint32_t* __restrict__ key,
+                        const uint32_t* __restrict__ rank, const uint32_t* __restrict__ offset,
+                        uint32_t* __restrict__ order, const unsigned int* status) {
+    if (status && (*status & ST_BLOCKS_PUBLISH)) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    order[offset[key[i]] + rank[i]] = i;
+}
+
 __global__ void k_iota(uint32_t n, uint32_t* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = i;
@@ -224,6 +234,12 @@ void launch_unpermute_f64(uint32_t n, const uint32_t* id, const double* src, dou
                           cudaStream_t s) {
     if (n == 0) return;
     k_unpermute<<<blocks_for(n, 256), 256, 0, s>>>(n, id, src, dst);
+}
+
+void launch_order(uint32_t n, const uint32_t* key, const uint32_t* rank, const uint32_t* offset,
+                  uint32_t* order, const unsigned int* status, cudaStream_t s) {
+    if (n == 0) return;
+    k_order<<<blocks_for(n, 256), 256, 0, s>>>(n, key, rank, offset, order, status);
 }
 
 void launch_iota_u32(uint32_t n, uint32_t* out, cudaStream_t s) {
