@@ -121,22 +121,25 @@ def setup_dist():
 def algorithmic_bytes(form, n_particles, n_mesh):
     """Algorithmic HBM bytes of one KDK step (particles sorted, gather reading
     the mesh once, Green's function fused between the transforms):
-    B = Np (9 bx + 6 bp) + Ng^3 (b_dep + [b_dep + b_fft if the int->float
-    conversion is its own pass] + 5 b_fft)."""
+    B = Np (9 bx + 6 bp) + Ng^3 (b_dep + 5 b_fft).
+    The precision form accumulates its int64 fixed-point cells in shared
+    memory and writes each cell once as an FP32 offset, so b_dep = 4 there
+    (no int64 mesh and no conversion pass reach HBM); binary64: b_dep = 8."""
     G = n_mesh ** 3
     if form == "fp64":
         return n_particles * (9 * 8 + 6 * 8) + G * (8 + 5 * 8)
-    return n_particles * (9 * 4 + 6 * 4) + G * (8 + (8 + 4) + 5 * 4)
+    return n_particles * (9 * 4 + 6 * 4) + G * (4 + 5 * 4)
 
 
 def phase_bytes(form, n, N, sort_fraction):
     """Algorithmic HBM bytes of one launch of each phase of ours (per step).
 
     kick/drift: read x, p, a; write candidate x, p (+ keys / ranks, and the
-      scatter of x, p, id on sort steps, weighted by how often they occur);
-    deposit: read positions once, write the mesh once (binary64) -- the
-      precision form also fills and converts its int64 cells (write 8, read 8,
-      write 4 per cell);
+      scatter of x, p, id on sort steps or the cell-order index on the other
+      steps, weighted by how often they occur);
+    deposit: read positions once, write the mesh once (binary64 cells; the
+      precision form writes FP32 offsets, its int64 accumulators live in
+      shared memory);
     green: read + write the half-complex spectrum;
     gather: read x, p and the potential once; write a and p.
     """
@@ -149,11 +152,12 @@ def phase_bytes(form, n, N, sort_fraction):
         gather = n * (3 * bx + 3 * bp + 3 * bp + 3 * bp) + G * 8
     else:
         bx = bp = 4
-        dep = n * 3 * bx + G * (8 + 8 + 8 + 4)
+        dep = n * 3 * bx + G * 4
         green = H * 8 * 2
         gather = n * (3 * bx + 3 * bp + 3 * bp + 3 * bp) + G * 4
     kick = n * (3 * bx + 3 * bp + 3 * bp + 3 * bx + 3 * bp + 8)
     kick += sort_fraction * n * 2 * (3 * bx + 3 * bp + 4 + 8)
+    kick += (1.0 - sort_fraction) * n * (4 + 4 + 4)   # cell order: key, rank in; order out
     return {"sort": kick, "deposit": dep, "green": green, "gather": gather}
 
 
@@ -312,25 +316,28 @@ def main():
     e2e = None
     if not args.no_e2e:
         import torch
-        pinned = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-                  for k in ("x", "y", "z", "px", "py", "pz", "ax", "ay", "az")}
-        for k in ("x", "y", "z", "px", "py", "pz"):
+        comps = ("x", "y", "z", "px", "py", "pz")
+        pinned = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in comps}
+        result = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in comps}
+        for k in comps:
             pinned[k][:] = ics[k]
+            result[k][:] = 0.0   # touch the pages before the timed region
         e2e_solver = solver
         t0 = time.perf_counter()
         e2e_solver.upload(pinned["x"], pinned["y"], pinned["z"], pinned["px"], pinned["py"],
                           pinned["pz"], uniform_mass=m_p)
         for s in range(args.steps):
             e2e_solver.kdk_step(K1[s], D[s], K2[s])
-        out = e2e_solver.download()
+        e2e_solver.download(out=result)
         e2e_secs = time.perf_counter() - t0
-        h2d = 6 * 8 * n
-        d2h = 9 * 8 * n + 8 * args.steps
+        h2d = 6 * 8 * n + 24 * args.steps
+        d2h = 6 * 8 * n + 8 * args.steps
         e2e = {"value": world * n * args.steps / e2e_secs, "unit": "particle-steps/s",
-               "h2d_bytes_per_step": h2d / args.steps + 24,
+               "h2d_bytes_per_step": h2d / args.steps,
                "d2h_bytes_per_step": d2h / args.steps,
-               "note": "upload IC state + K kdk_step calls + download final state"}
-        del out
+               "note": "pinned host buffers: upload of the IC positions and momenta, K "
+                       "hyowon_pm_kdk_step calls (K1, D, K2 in, max drift out), download of "
+                       "the final positions and momenta"}
 
     solver.close()
     compare = None

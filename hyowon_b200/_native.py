@@ -52,6 +52,14 @@ _EXC = {
     ENOMEM: MemoryError,
 }
 
+class Diagnostics(ctypes.Structure):
+    """hyowon_pm_diagnostics_t (include/hyowon_pm.h)."""
+    _fields_ = [("potential_energy_comoving", c_double), ("kinetic_energy", c_double),
+                ("momentum", c_double * 3), ("mass_weighted_force", c_double * 3),
+                ("force_norm_sum", c_double), ("force_balance", c_double),
+                ("momentum_force_contraction", c_double)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "hyowon_pm_create": (c_int, [c_double, c_u64, c_int, c_int, c_double, c_int,
@@ -75,6 +83,7 @@ _SIGS = {
     "hyowon_pm_set_timing": (c_int, [c_void_p, c_int]),
     "hyowon_pm_set_sort_interval": (c_int, [c_void_p, c_int]),
     "hyowon_pm_last_timing": (c_int, [c_void_p, P_double]),
+    "hyowon_pm_diagnostics": (c_int, [c_void_p, c_double, ctypes.POINTER(Diagnostics)]),
     "hyowon_vjp_1lpt_pm": (c_int, [c_void_p, P_double, P_double, P_double, P_double,
                                    P_double, P_double]),
     "hyowon_vjp_last_error": (ctypes.c_char_p, []),

@@ -37,6 +37,7 @@ UNITS = [
     ("pm_fp32.cu", []),
     ("pm_poisson.cu", []),
     ("pm_noalloc.cu", ["--fmad=false"]),
+    ("pm_diag.cu", ["--fmad=false"]),
     ("cosmology.cpp", []),
 ]
 

@@ -27,6 +27,11 @@
 
 namespace hyowon::b200 {
 
+// gravity::PMForceDiagnostics (include/cosmo_nbody/gravity/pm_solver.hpp:30-35).
+struct PMForceDiagnostics {
+    double potential_energy_comoving = 0.0;
+};
+
 enum class Method { PurePM = HYOWON_PURE_PM, TreePMLongRange = HYOWON_TREEPM_LONG_RANGE };
 enum class Precision { FP64 = HYOWON_FP64, FP32Fixed = HYOWON_FP32_FIXED };
 
@@ -75,10 +80,13 @@ public:
     // PMSolver::compute_forces (src/gravity/pm_solver.cpp:494-567) on host
     // spans: ADDS the PM acceleration to acc_*; masses empty means uniform_mass.
     // The device particle state is replaced by these positions.
-    void compute_forces(std::span<const double> pos_x, std::span<const double> pos_y,
-                        std::span<const double> pos_z, std::span<const double> masses,
-                        std::optional<double> uniform_mass, std::span<double> acc_x,
-                        std::span<double> acc_y, std::span<double> acc_z) {
+    // With collect_potential_energy the reference's PMForceDiagnostics is
+    // returned (0.5 sum_i m_i phi(x_i), src/gravity/pm_solver.cpp:812-840).
+    std::optional<PMForceDiagnostics> compute_forces(
+        std::span<const double> pos_x, std::span<const double> pos_y,
+        std::span<const double> pos_z, std::span<const double> masses,
+        std::optional<double> uniform_mass, std::span<double> acc_x, std::span<double> acc_y,
+        std::span<double> acc_z, bool collect_potential_energy = false) {
         const std::size_t n = pos_x.size();
         if (pos_y.size() != n || pos_z.size() != n || acc_x.size() != n || acc_y.size() != n
             || acc_z.size() != n)
@@ -91,6 +99,16 @@ public:
                                     masses.empty() ? nullptr : masses.data(),
                                     uniform_mass.value_or(0.0), acc_x.data(), acc_y.data(),
                                     acc_z.data()));
+        if (!collect_potential_energy) return std::nullopt;
+        return PMForceDiagnostics{diagnostics(1.0).potential_energy_comoving};
+    }
+
+    // Binary64 global sums of the state at the last force solve (kinetic and
+    // potential energy, momentum, force balance; hyowon_pm_diagnostics).
+    hyowon_pm_diagnostics_t diagnostics(double a) const {
+        hyowon_pm_diagnostics_t d{};
+        check(hyowon_pm_diagnostics(h_, a, &d));
+        return d;
     }
 
     // ParticleStore -> device. Momenta may be empty (zero).

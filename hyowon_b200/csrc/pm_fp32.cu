@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "hyowon_pm.h"
+#include "pm_diag.h"
 #include "pm_fp32.h"
 #include "pm_poisson.h"
 #include "pm_kernels.h"
@@ -580,6 +581,8 @@ struct State {
     bool order_state_invalid = true;  // offsets/order do not describe the current positions
     float* rmesh = nullptr;
     float2* modes = nullptr;
+    size_t modes_elems = 0;   // 8-byte slots of `modes` (host staging between solves)
+    unsigned int* d_flag = nullptr;  // input validation flag of upload
     float2* phi_k = nullptr;
     float* lap = nullptr;
     float* win = nullptr;
@@ -709,6 +712,8 @@ int create(State** out, double L, int N, int method, int deconvolve, double r_s,
     const size_t modes_n = method == HYOWON_PURE_PM && poisson::supported(N)
         ? std::max(half, poisson::modes_elements_f32(N)) : half;
     CK(dalloc(&st->modes, modes_n));
+    st->modes_elems = modes_n;
+    CK(dalloc(&st->d_flag, 1));
     if (method == HYOWON_TREEPM_LONG_RANGE) CK(dalloc(&st->phi_k, half));
     CK(dalloc(&st->lap, N));
     CK(dalloc(&st->win, N));
@@ -771,6 +776,7 @@ void destroy(State* st) {
     cudaFree(st->d_max_count);
     cudaFree(st->d_plan);
     cudaFree(st->d_qsum);
+    cudaFree(st->d_flag);
     free_particles(st);
     cudaFree(st->sort.count);
     cudaFree(st->sort.offset);
@@ -788,19 +794,17 @@ int upload_device(State* st, uint32_t n, double* const pos[3], double* const mom
     st->uniform_mass = uniform_mass;
     st->input_mass = total_mass;
     st->pc = st->mc = st->ic = 0;
-    unsigned int* d_status = nullptr;
-    CK(dalloc(&d_status, 1));
-    cudaMemsetAsync(d_status, 0, sizeof(unsigned int), s);
+    CK(cudaMemsetAsync(st->d_flag, 0, sizeof(unsigned int), s));
     ++st->launches;
     k_to_fixed<<<blocks_for(n), kThreads, 0, s>>>(n, pos[0], pos[1], pos[2], mom[0], mom[1], mom[2],
                                                   st->L, st->pos[0][0], st->pos[0][1], st->pos[0][2],
-                                                  st->mom[0][0], st->mom[0][1], st->mom[0][2], d_status);
+                                                  st->mom[0][0], st->mom[0][1], st->mom[0][2], st->d_flag);
     ++st->launches;
     launch_iota_u32(n, st->id[0], s);
     unsigned int h = 0;
-    cudaMemcpyAsync(&h, d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&h, st->d_flag, sizeof(unsigned int), cudaMemcpyDeviceToHost, s);
     const cudaError_t e = cudaStreamSynchronize(s);
-    cudaFree(d_status);
+    st->order_state_invalid = true;
     if (e != cudaSuccess) return fail(st, HYOWON_ECUDA, cudaGetErrorString(e));
     if (h) return fail(st, HYOWON_EINVAL, "particle positions and momenta must be finite");
     return HYOWON_OK;
@@ -808,24 +812,45 @@ int upload_device(State* st, uint32_t n, double* const pos[3], double* const mom
 
 int upload(State* st, uint32_t n, const double* x, const double* y, const double* z,
            const double* px, const double* py, const double* pz, const double* masses,
-           double uniform_mass, double total_mass, double mass_tol, cudaStream_t s) {
+           double uniform_mass, double total_mass, double, cudaStream_t s) {
     if (masses) return fail(st, HYOWON_EINVAL, "the FP32 fixed-point form requires a uniform particle mass");
-    double* tmp[6] = {};
+    int rc = ensure(st, n);
+    if (rc) return rc;
+    st->n = n;
+    st->uniform_mass = uniform_mass;
+    st->input_mass = total_mass;
+    st->pc = st->mc = st->ic = 0;
+    // The binary64 host arrays are staged through the half-spectrum buffer,
+    // which holds nothing live between force solves, in chunks of up to
+    // modes_elems / 6 particles, and converted on the device chunk by chunk.
     const double* src[6] = {x, y, z, px, py, pz};
-    int rc = HYOWON_OK;
-    for (int a = 0; a < 6 && rc == HYOWON_OK; ++a) {
-        if (!src[a]) continue;
-        if (dalloc(&tmp[a], n) != cudaSuccess
-            || cudaMemcpyAsync(tmp[a], src[a], sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
-            rc = fail(st, HYOWON_ENOMEM, "staging allocation failed");
+    const uint64_t per = st->modes_elems / 6;
+    const uint32_t chunk = static_cast<uint32_t>(per < n ? (per > 0 ? per : 1) : n);
+    double* stage = reinterpret_cast<double*>(st->modes);
+    CK(cudaMemsetAsync(st->d_flag, 0, sizeof(unsigned int), s));
+    for (uint32_t off = 0; off < n; off += chunk) {
+        const uint32_t c = n - off < chunk ? n - off : chunk;
+        const double* d[6] = {};
+        for (int a = 0; a < 6; ++a) {
+            if (!src[a]) continue;
+            double* slot = stage + static_cast<size_t>(a) * c;
+            CK(cudaMemcpyAsync(slot, src[a] + off, sizeof(double) * c, cudaMemcpyHostToDevice, s));
+            d[a] = slot;
+        }
+        ++st->launches;
+        k_to_fixed<<<blocks_for(c), kThreads, 0, s>>>(
+            c, d[0], d[1], d[2], d[3], d[4], d[5], st->L, st->pos[0][0] + off, st->pos[0][1] + off,
+            st->pos[0][2] + off, st->mom[0][0] + off, st->mom[0][1] + off, st->mom[0][2] + off,
+            st->d_flag);
     }
-    if (rc == HYOWON_OK) {
-        double* const p3[3] = {tmp[0], tmp[1], tmp[2]};
-        double* const m3[3] = {tmp[3], tmp[4], tmp[5]};
-        rc = upload_device(st, n, p3, m3, uniform_mass, total_mass, mass_tol, s);
-    }
-    for (auto* t : tmp) cudaFree(t);
-    return rc;
+    ++st->launches;
+    launch_iota_u32(n, st->id[0], s);
+    unsigned int h = 0;
+    CK(cudaMemcpyAsync(&h, st->d_flag, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    st->order_state_invalid = true;
+    if (h) return fail(st, HYOWON_EINVAL, "particle positions and momenta must be finite");
+    return HYOWON_OK;
 }
 
 void validate(State*, cudaStream_t, unsigned int*) {}
@@ -1066,8 +1091,18 @@ void commit_step(State* st, bool published, bool ok) {
 int download(State* st, cudaStream_t s, double* x, double* y, double* z, double* px, double* py,
              double* pz, double* ax, double* ay, double* az) {
     const uint32_t n = st->n;
+    // Widened components are scattered back to the original particle order in
+    // a staging array of n doubles: the half-spectrum buffer when it is large
+    // enough (it holds nothing live between force solves; the potential mesh
+    // is left intact), else a temporary allocation.
     double* stage = nullptr;
-    CK(dalloc(&stage, n));
+    bool owned = false;
+    if (st->modes_elems >= n) {
+        stage = reinterpret_cast<double*>(st->modes);
+    } else {
+        CK(dalloc(&stage, n));
+        owned = true;
+    }
     double* outs[9] = {x, y, z, px, py, pz, ax, ay, az};
     const double pos_scale = st->L / kTwo32;
     int rc = HYOWON_OK;
@@ -1087,8 +1122,32 @@ int download(State* st, cudaStream_t s, double* x, double* y, double* z, double*
             || cudaStreamSynchronize(s) != cudaSuccess)
             rc = fail(st, HYOWON_ECUDA, "download copy failed");
     }
-    cudaFree(stage);
+    if (owned) cudaFree(stage);
     return rc;
+}
+
+int diagnostics(State* st, cudaStream_t s, bool with_potential, double* scratch, double* sums) {
+    diag::InputsF32 in{};
+    in.n = st->n;
+    in.ux = st->pos[st->pc][0];
+    in.uy = st->pos[st->pc][1];
+    in.uz = st->pos[st->pc][2];
+    in.px = st->mom[st->mc][0];
+    in.py = st->mom[st->mc][1];
+    in.pz = st->mom[st->mc][2];
+    in.ax = st->acc[0];
+    in.ay = st->acc[1];
+    in.az = st->acc[2];
+    in.uniform_mass = st->uniform_mass;
+    in.phi = with_potential ? st->rmesh : nullptr;
+    in.N = st->N;
+    const int k = diag::launch_f32(in, scratch, s);
+    if (k < 0) return fail(st, HYOWON_ECUDA, "diagnostics launch failed");
+    st->launches += k;
+    CK(cudaMemcpyAsync(sums, scratch + diag::partial_doubles(), sizeof(double) * diag::kTerms,
+                       cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return HYOWON_OK;
 }
 
 int download_potential(State* st, cudaStream_t s, double* phi) {

@@ -50,6 +50,9 @@ void commit_step(State* st, bool published, bool ok);
 int download(State* st, cudaStream_t s, double* x, double* y, double* z, double* px,
              double* py, double* pz, double* ax, double* ay, double* az);
 int download_potential(State* st, cudaStream_t s, double* phi);
+// Global binary64 sums of the current state (pm_diag.h order) into host
+// sums[kTerms], using the device scratch `scratch` (diag::scratch_doubles()).
+int diagnostics(State* st, cudaStream_t s, bool with_potential, double* scratch, double* sums);
 int download_mass_mesh(State* st, cudaStream_t s, unsigned int* d_status, double* mesh);
 
 }  // namespace fp32

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "hyowon_pm.h"
+#include "pm_diag.h"
 #include "pm_fp32.h"
 #include "pm_poisson.h"
 #include "pm_kernels.h"
@@ -98,6 +99,7 @@ struct hyowon_pm_s {
 
     unsigned int* d_status = nullptr;
     unsigned long long* d_maxdrift = nullptr;
+    double* d_diag = nullptr;                   // diagnostics scratch (pm_diag.h)
     unsigned int* h_status = nullptr;           // pinned
     unsigned long long* h_maxdrift = nullptr;   // pinned
 
@@ -601,7 +603,8 @@ int hyowon_pm_create(double box_size, uint64_t mesh_size, int method, int deconv
         return bail(HYOWON_ECUDA);
     if (cudaMallocHost(reinterpret_cast<void**>(&h->h_status), sizeof(unsigned int)) != cudaSuccess
         || cudaMallocHost(reinterpret_cast<void**>(&h->h_maxdrift), sizeof(unsigned long long)) != cudaSuccess
-        || dalloc(&h->d_status, 1) != cudaSuccess || dalloc(&h->d_maxdrift, 1) != cudaSuccess)
+        || dalloc(&h->d_status, 1) != cudaSuccess || dalloc(&h->d_maxdrift, 1) != cudaSuccess
+        || dalloc(&h->d_diag, diag::scratch_doubles()) != cudaSuccess)
         return bail(HYOWON_ENOMEM);
     for (auto& e : h->ev) {
         if (cudaEventCreate(&e) != cudaSuccess) return bail(HYOWON_ECUDA);
@@ -713,6 +716,7 @@ int hyowon_pm_destroy(hyowon_pm_t h) {
     cudaFree(h->sort.scan_tmp);
     cudaFree(h->d_status);
     cudaFree(h->d_maxdrift);
+    cudaFree(h->d_diag);
     if (h->h_status) cudaFreeHost(h->h_status);
     if (h->h_maxdrift) cudaFreeHost(h->h_maxdrift);
     for (auto& e : h->ev) {
@@ -1070,6 +1074,66 @@ int hyowon_pm_set_timing(hyowon_pm_t h, int enabled) {
 int hyowon_pm_last_timing(hyowon_pm_t h, double* times) {
     if (!h || !times) return HYOWON_EINVAL;
     for (int i = 0; i < 9; ++i) times[i] = h->last_times[i];
+    return HYOWON_OK;
+}
+
+
+int hyowon_pm_diagnostics(hyowon_pm_t h, double a, hyowon_pm_diagnostics_t* out) {
+    if (!h || !out) return HYOWON_EINVAL;
+    if (!std::isfinite(a) || a <= 0.0)
+        return fail(h, HYOWON_EINVAL, "diagnostics scale factor must be finite and positive");
+    if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
+    if (!h->acc_valid)
+        return fail(h, HYOWON_ELOGIC, "diagnostics need a valid force solve at the current positions");
+    const bool with_phi = h->method == HYOWON_PURE_PM;
+    double r[diag::kTerms] = {};
+    if (h->precision == HYOWON_FP32_FIXED) {
+        int rc = fp32::diagnostics(h->f32, h->stream, with_phi, h->d_diag, r);
+        if (rc) return status_or_cuda(h, rc);
+    } else {
+        diag::InputsF64 in{};
+        in.n = h->n;
+        in.x = h->pos[h->pc][0];
+        in.y = h->pos[h->pc][1];
+        in.z = h->pos[h->pc][2];
+        in.px = h->mom[h->mc][0];
+        in.py = h->mom[h->mc][1];
+        in.pz = h->mom[h->mc][2];
+        in.ax = h->acc[0];
+        in.ay = h->acc[1];
+        in.az = h->acc[2];
+        in.mass = h->has_masses ? h->mass[h->ic] : nullptr;
+        in.uniform_mass = h->uniform_mass;
+        in.phi = with_phi ? h->mesh : nullptr;
+        in.axis = h->axis;
+        CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
+        const int k = diag::launch_f64(in, h->d_diag, h->d_status, h->stream);
+        if (k < 0) return fail(h, HYOWON_ECUDA, "diagnostics launch failed");
+        h->launches += k;
+        CK(cudaMemcpyAsync(r, h->d_diag + diag::partial_doubles(), sizeof(r), cudaMemcpyDeviceToHost,
+                           h->stream));
+        unsigned int st = 0;
+        int rc = read_status(h, &st);
+        if (rc) return rc;
+        if (st) return status_to_code(h, st);
+    }
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    out->potential_energy_comoving = with_phi ? 0.5 * r[0] : nan;
+    out->kinetic_energy = r[1] / (a * a);
+    for (int d = 0; d < 3; ++d) {
+        out->momentum[d] = r[2 + d];
+        out->mass_weighted_force[d] = r[5 + d];
+    }
+    out->force_norm_sum = r[8];
+    const double net = std::sqrt(r[5] * r[5] + r[6] * r[6] + r[7] * r[7]);
+    out->force_balance = r[8] > 0.0 ? net / r[8] : 0.0;
+    out->momentum_force_contraction = r[9];
+    for (int t = 1; t < diag::kTerms; ++t)
+        if (!std::isfinite(r[t])) return fail(h, HYOWON_EOVERFLOW, "diagnostic sum is non-finite");
+    if (with_phi && !std::isfinite(out->potential_energy_comoving))
+        return fail(h, HYOWON_EOVERFLOW, "PMSolver potential-energy diagnostic is non-finite");
+    if (with_phi && r[0] != 0.0 && out->potential_energy_comoving == 0.0)
+        return fail(h, HYOWON_EUNDERFLOW, "PMSolver potential-energy diagnostic underflowed");
     return HYOWON_OK;
 }
 

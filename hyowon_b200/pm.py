@@ -112,8 +112,13 @@ class PMSolver:
         nat.raise_for(rc, self._h, where)
 
     # -- PMSolver::compute_forces ------------------------------------------
-    def compute_forces(self, pos_x, pos_y, pos_z, masses, uniform_mass, acc_x, acc_y, acc_z):
-        """Adds the PM acceleration at the given positions to acc_* (in place)."""
+    def compute_forces(self, pos_x, pos_y, pos_z, masses, uniform_mass, acc_x, acc_y, acc_z,
+                       collect_potential_energy=False):
+        """Adds the PM acceleration at the given positions to acc_* (in place).
+
+        With collect_potential_energy, returns the reference's PMForceDiagnostics
+        as a dict {"potential_energy_comoving": 0.5 sum_i m_i phi(x_i)}
+        (src/gravity/pm_solver.cpp:812-840); otherwise None."""
         n = len(pos_x)
         if not (len(pos_y) == len(pos_z) == len(acc_x) == len(acc_y) == len(acc_z) == n):
             raise ValueError("PMSolver position and acceleration component sizes must match")
@@ -135,6 +140,9 @@ class PMSolver:
                                              nat.dptr(m), float(uniform_mass or 0.0),
                                              nat.dptr(acc_x), nat.dptr(acc_y), nat.dptr(acc_z))
         self._check(rc, "PMSolver.compute_forces")
+        if collect_potential_energy:
+            return {"potential_energy_comoving": self.diagnostics(1.0)["potential_energy_comoving"]}
+        return None
 
     # -- device-resident state --------------------------------------------
     def upload(self, x, y, z, px=None, py=None, pz=None, masses=None, uniform_mass=None):
@@ -157,11 +165,23 @@ class PMSolver:
                                              ctypes.byref(p), ctypes.byref(mth)), "info")
         return n.value, N.value, p.value, mth.value
 
-    def download(self, acc=True):
+    def download(self, acc=True, out=None):
+        """Particle state in the original particle order. With `out` (a dict of
+        C-contiguous float64 arrays of the particle count, e.g. pinned host
+        buffers), only the components it names are copied, into those arrays."""
         n = self.info()[0]
-        out = {k: np.empty(n) for k in ("x", "y", "z", "px", "py", "pz")}
-        if acc:
-            out.update({k: np.empty(n) for k in ("ax", "ay", "az")})
+        if out is None:
+            out = {k: np.empty(n) for k in ("x", "y", "z", "px", "py", "pz")}
+            if acc:
+                out.update({k: np.empty(n) for k in ("ax", "ay", "az")})
+        else:
+            for k, a in out.items():
+                if k not in ("x", "y", "z", "px", "py", "pz", "ax", "ay", "az"):
+                    raise ValueError(f"unknown particle component {k!r}")
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float64
+                        and a.flags["C_CONTIGUOUS"] and a.size == n):
+                    raise ValueError("download outputs must be C-contiguous float64 arrays "
+                                     "of the particle count")
         g = out.get
         rc = nat.lib().hyowon_pm_download(
             self._h, nat.dptr(g("x")), nat.dptr(g("y")), nat.dptr(g("z")), nat.dptr(g("px")),
@@ -209,6 +229,21 @@ class PMSolver:
 
     def set_sort_interval(self, steps: int):
         self._check(nat.lib().hyowon_pm_set_sort_interval(self._h, int(steps)), "set_sort_interval")
+
+    def diagnostics(self, a: float) -> dict:
+        """Binary64 global sums of the state at the last force solve
+        (hyowon_pm_diagnostics): potential_energy_comoving, kinetic_energy
+        (sum 0.5 m p^2 / a^2), momentum, mass_weighted_force, force_norm_sum,
+        force_balance (|sum m a| / sum m |a|), momentum_force_contraction."""
+        d = nat.Diagnostics()
+        self._check(nat.lib().hyowon_pm_diagnostics(self._h, float(a), ctypes.byref(d)),
+                    "diagnostics")
+        return {"potential_energy_comoving": d.potential_energy_comoving,
+                "kinetic_energy": d.kinetic_energy,
+                "momentum": np.array(d.momentum[:]),
+                "mass_weighted_force": np.array(d.mass_weighted_force[:]),
+                "force_norm_sum": d.force_norm_sum, "force_balance": d.force_balance,
+                "momentum_force_contraction": d.momentum_force_contraction}
 
     def set_timing(self, on: bool):
         self._check(nat.lib().hyowon_pm_set_timing(self._h, int(on)), "set_timing")

@@ -165,6 +165,41 @@ int hyowon_pm_set_sort_interval(hyowon_pm_t h, int steps);
 int hyowon_pm_set_timing(hyowon_pm_t h, int enabled);
 int hyowon_pm_last_timing(hyowon_pm_t h, double* times);
 
+/* Global diagnostics of the device state at the last force solve, reduced in
+ * binary64 in both arithmetic forms, deterministic run to run (fixed
+ * reduction order with compensated partial sums).
+ *   potential_energy_comoving  0.5 sum_i m_i phi(x_i), phi CIC-interpolated from
+ *       the potential mesh of the last force solve: PMForceDiagnostics of
+ *       PMSolver::compute_forces(..., collect_potential_energy = true)
+ *       (include/cosmo_nbody/gravity/pm_solver.hpp:30-35,
+ *       src/gravity/pm_solver.cpp:812-840, per-particle arithmetic of
+ *       src/mesh/mass_assignment_gather.inc:283-391). Pure PM only; NaN for
+ *       HYOWON_TREEPM_LONG_RANGE, whose solve keeps no real-space potential.
+ *   kinetic_energy  sum_i 0.5 m_i |p_i|^2 / a^2
+ *       (ConservationChecks::compute_kinetic_energy,
+ *       src/validation/conservation_checks.cpp:589-625,1376-1480).
+ *   momentum  sum_i m_i p_i.
+ *   mass_weighted_force  sum_i m_i a_i;  force_norm_sum  sum_i m_i |a_i|;
+ *   force_balance  |sum_i m_i a_i| / sum_i m_i |a_i|, the force-balance
+ *       residual R_F (include/cosmo_nbody/validation/force_balance_diagnostics.hpp:19-27).
+ *   momentum_force_contraction  sum_i m_i p_i . a_i
+ *       (ConservationChecks::compute_momentum_force_contraction,
+ *       include/cosmo_nbody/validation/conservation_checks.hpp).
+ * a is the scale factor of the state (finite, > 0). HYOWON_ELOGIC when no
+ * force solve is valid for the current positions; HYOWON_EOVERFLOW for a
+ * non-finite sum; HYOWON_EUNDERFLOW when a non-zero CIC product is lost
+ * (the reference's std::underflow_error). */
+typedef struct hyowon_pm_diagnostics {
+    double potential_energy_comoving;
+    double kinetic_energy;
+    double momentum[3];
+    double mass_weighted_force[3];
+    double force_norm_sum;
+    double force_balance;
+    double momentum_force_contraction;
+} hyowon_pm_diagnostics_t;
+int hyowon_pm_diagnostics(hyowon_pm_t h, double a, hyowon_pm_diagnostics_t* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -209,6 +209,40 @@ class Reference:
         self._check(rc, "ref_pm_forces")
         return ax, ay, az
 
+    def pm_forces_energy(self, L, N, x, y, z, masses=None, uniform_mass=1.0, deconvolve=False):
+        """PMSolver::compute_forces(..., collect_potential_energy=true): returns
+        (ax, ay, az, potential_energy_comoving)."""
+        n = len(x)
+        x, y, z = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z))
+        ax, ay, az = np.zeros(n), np.zeros(n), np.zeros(n)
+        e = ctypes.c_double(0.0)
+        m = None if masses is None else np.ascontiguousarray(masses, dtype=np.float64)
+        rc = self.lib.ref_pm_forces_energy(
+            _c_double(L), _c_u64(N), _c_int(int(deconvolve)), _c_u64(n), _dp(x), _dp(y), _dp(z),
+            _dp(m), _c_double(uniform_mass), _dp(ax), _dp(ay), _dp(az), ctypes.byref(e))
+        self._check(rc, "ref_pm_forces_energy")
+        return ax, ay, az, e.value
+
+    def conservation(self, L, N, px, py, pz, ax, ay, az, mass, a):
+        """ConservationChecks: (kinetic energy at a, sum m p . g)."""
+        arr = [np.ascontiguousarray(v, dtype=np.float64) for v in (px, py, pz, ax, ay, az)]
+        out = np.zeros(2)
+        rc = self.lib.ref_conservation(_c_double(L), _c_u64(N), _c_u64(arr[0].size),
+                                       *[_dp(v) for v in arr], _c_double(mass), _c_double(a),
+                                       _dp(out))
+        self._check(rc, "ref_conservation")
+        return float(out[0]), float(out[1])
+
+    def force_balance(self, ax, ay, az, masses=None, uniform_mass=1.0):
+        """validation::compute_force_balance_diagnostics: |sum m a| / sum m |a|."""
+        ax, ay, az = (np.ascontiguousarray(v, dtype=np.float64) for v in (ax, ay, az))
+        m = None if masses is None else np.ascontiguousarray(masses, dtype=np.float64)
+        r = ctypes.c_double(0.0)
+        rc = self.lib.ref_force_balance(_c_u64(len(ax)), _dp(m), _c_double(uniform_mass),
+                                        _dp(ax), _dp(ay), _dp(az), ctypes.byref(r))
+        self._check(rc, "ref_force_balance")
+        return r.value
+
     def short_range_pair(self, r_s, cutoff_multiplier, eps, mass, dx, dy, dz):
         dx, dy, dz = (np.ascontiguousarray(a, dtype=np.float64) for a in (dx, dy, dz))
         out = [np.zeros(dx.size) for _ in range(3)]

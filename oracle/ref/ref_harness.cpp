@@ -27,6 +27,8 @@
 #include "cosmo_nbody/mesh/pm_force_method.hpp"
 #include "cosmo_nbody/time/leapfrog_integrator.hpp"
 #include "cosmo_nbody/time/time_stepper.hpp"
+#include "cosmo_nbody/validation/conservation_checks.hpp"
+#include "cosmo_nbody/validation/force_balance_diagnostics.hpp"
 #include "mesh/cic_coordinate.hpp"
 
 #include <chrono>
@@ -187,6 +189,82 @@ int ref_pm_forces(double L, std::uint64_t N, int method, int deconvolve, double 
             std::span<const double>(z, n), mass_span(masses, n),
             uniform_or_none(masses, uniform_mass), std::span<double>(ax, n),
             std::span<double>(ay, n), std::span<double>(az, n), false);
+    });
+}
+
+// PMSolver::compute_forces with collect_potential_energy = true: ADDS the PM
+// acceleration and returns PMForceDiagnostics::potential_energy_comoving
+// (src/gravity/pm_solver.cpp:812-840) in *energy.
+int ref_pm_forces_energy(double L, std::uint64_t N, int deconvolve, std::uint64_t n,
+                         const double* x, const double* y, const double* z,
+                         const double* masses, double uniform_mass, double* ax, double* ay,
+                         double* az, double* energy) {
+    return guarded([&] {
+        mesh::MeshGeometry geom(L, N);
+        gravity::PMSolver solver(geom, mesh::PMForceMethod::pure_pm(deconvolve != 0), false,
+                                 config::MemoryPolicyParams{});
+        const auto d = solver.compute_forces(
+            std::span<const double>(x, n), std::span<const double>(y, n),
+            std::span<const double>(z, n), mass_span(masses, n),
+            uniform_or_none(masses, uniform_mass), std::span<double>(ax, n),
+            std::span<double>(ay, n), std::span<double>(az, n), true);
+        if (!d.has_value()) throw std::logic_error("no PMForceDiagnostics returned");
+        *energy = d->potential_energy_comoving;
+    });
+}
+
+// validation::compute_force_balance_diagnostics
+// (include/cosmo_nbody/validation/force_balance_diagnostics.hpp:677-710).
+int ref_force_balance(std::uint64_t n, const double* masses, double uniform_mass,
+                      const double* ax, const double* ay, const double* az, double* residual) {
+    return guarded([&] {
+        const std::span<const double> gx(ax, n), gy(ay, n), gz(az, n);
+        const auto d = masses
+            ? validation::compute_force_balance_diagnostics(std::span<const double>(masses, n),
+                                                            gx, gy, gz)
+            : validation::compute_force_balance_diagnostics(uniform_mass, gx, gy, gz);
+        *residual = d.relative_residual;
+    });
+}
+
+// ConservationChecks::compute_kinetic_energy (src/validation/conservation_checks.cpp:1376)
+// and ::compute_momentum_force_contraction
+// (src/validation/conservation_force_energy.cpp:148) of a ParticleStore holding
+// the given momenta and accelerations with uniform mass m: out[0] = K(a),
+// out[1] = sum m p . g.
+int ref_conservation(double L, std::uint64_t n_mesh, std::uint64_t n, const double* px,
+                     const double* py, const double* pz, const double* ax, const double* ay,
+                     const double* az, double mass, double a, double* out) {
+    return guarded([&] {
+        config::GravityParams g;
+        g.solver = "PM";
+        g.deconvolve_cic = core::ExplicitBoolean(false);
+        config::BoxParams b;
+        b.L = L;
+        b.N = 1;
+        b.N_mesh = n_mesh;
+        config::TimeParams t;
+        t.z_start = 49.0;
+        t.z_final = 0.0;
+        t.delta_ln_a = 0.1;
+        config::ICParams ic;
+        ic.mode = "snapshot";
+        ic.snapshot_file = "unused.hdf5";
+        config::OutputParams o;
+        config::SimulationParameters cfg(flat_lcdm(0.3, 0.7), b, g, t, ic, o);
+        core::ParticleStore store;
+        store.set_uniform_mass(mass);
+        store.resize(n);
+        std::memcpy(store.get_momenta_x().data(), px, sizeof(double) * n);
+        std::memcpy(store.get_momenta_y().data(), py, sizeof(double) * n);
+        std::memcpy(store.get_momenta_z().data(), pz, sizeof(double) * n);
+        std::memcpy(store.mutable_accelerations_x().data(), ax, sizeof(double) * n);
+        std::memcpy(store.mutable_accelerations_y().data(), ay, sizeof(double) * n);
+        std::memcpy(store.mutable_accelerations_z().data(), az, sizeof(double) * n);
+        store.set_acceleration_validity(core::FieldValidity::VALID);
+        validation::ConservationChecks checks(cfg);
+        out[0] = checks.compute_kinetic_energy(store, a);
+        out[1] = checks.compute_momentum_force_contraction(store);
     });
 }
 

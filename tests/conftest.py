@@ -43,3 +43,8 @@ def c1_kdk():
 @pytest.fixture(scope="session")
 def schedules():
     return load_golden("c1_schedule.npz")
+
+
+@pytest.fixture(scope="session")
+def c1_diag():
+    return load_golden("c1_diag.npz")

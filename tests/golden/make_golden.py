@@ -18,6 +18,12 @@ Fixtures:
                       random particles incl. boundary positions (bit-level)
   c1_kdk.npz          c1 ICs, force at a_start, state after 1 and after 32 KDK
                       steps of the reference integrator
+  c1_diag.npz         global diagnostics of the reference at the c1 ICs and after
+                      32 steps (PMForceDiagnostics potential energy, kinetic
+                      energy, force balance, momentum-force contraction) and the
+                      potential energy / force balance of small_pm with masses
+
+    python tests/golden/make_golden.py --only diag    # c1_diag.npz alone
 """
 from __future__ import annotations
 
@@ -46,12 +52,39 @@ def edge_positions(rng, n, L):
     return x
 
 
+def diag_fixture(ref):
+    """c1_diag.npz from the reference's PMSolver (collect_potential_energy),
+    ConservationChecks and compute_force_balance_diagnostics, evaluated on the
+    c1 states and the small_pm inputs already stored in the fixtures."""
+    d = np.load(os.path.join(HERE, "c1_kdk.npz"))
+    L, N, m = float(d["box"]), int(d["mesh"]), float(d["particle_mass"])
+    out = {}
+    for tag, a in (("ic", float(d["a_start"])), ("s32", 1.0)):
+        x, y, z = d[tag + "_x"], d[tag + "_y"], d[tag + "_z"]
+        px, py, pz = d[tag + "_px"], d[tag + "_py"], d[tag + "_pz"]
+        ax, ay, az, e = ref.pm_forces_energy(L, N, x, y, z, uniform_mass=m)
+        K, C = ref.conservation(L, N, px, py, pz, ax, ay, az, m, a)
+        out.update({tag + "_a": a, tag + "_potential_energy": e, tag + "_kinetic_energy": K,
+                    tag + "_momentum_force_contraction": C,
+                    tag + "_force_balance": ref.force_balance(ax, ay, az, uniform_mass=m)})
+    sp = np.load(os.path.join(HERE, "small_pm.npz"))
+    Ls, Ns = float(sp["L"]), int(sp["N"])
+    ax, ay, az, e = ref.pm_forces_energy(Ls, Ns, sp["x"], sp["y"], sp["z"], masses=sp["masses"])
+    out.update(small_masses_potential_energy=e,
+               small_masses_force_balance=ref.force_balance(ax, ay, az, masses=sp["masses"]))
+    np.savez_compressed(os.path.join(HERE, "c1_diag.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--only", choices=["diag"], default=None)
     args = ap.parse_args()
     build_reference(args.ref_root)
     ref = Reference()
+    if args.only == "diag":
+        diag_fixture(ref)
+        return
 
     # -- schedules --------------------------------------------------------
     sched = {}
@@ -139,6 +172,7 @@ def main():
     tree_out.update(c_targets=ct, c_ax=cf[0], c_ay=cf[1], c_az=cf[2], c_r_s=1.25 * dxc,
                     c_r_cut=4.5 * 1.25 * dxc, c_eps=c["box"] / c["n_side"] / 30.0)
     np.savez_compressed(os.path.join(HERE, "treepm_tree.npz"), **tree_out)
+    diag_fixture(ref)
     print(f"c1 reference evolution: {c['steps']} steps in {secs:.2f} s")
 
 
