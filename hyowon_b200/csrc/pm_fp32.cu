@@ -206,15 +206,27 @@ __device__ __forceinline__ void store_cell(long long* out, long long q) { *out =
 // (integer atomics: the result does not depend on their order), then writing
 // each cell once as its offset from the mean, q - mean_q (FP32 for the
 // transform, or int64 exactly), and folding the offsets into *qsum (mod 2^64)
-// for the exact mass check. Contributors are the particles whose base cell
-// lies in rows (x0 or x0-1, y0-1 .. y0+TY-1), found through the cell order of
-// the current positions (`offset` bucket starts; `order` sorted slot ->
-// particle, or null when the arrays are in cell order). The contributor
-// ranges of all rows are concatenated so every thread walks one flat list,
-// loading kDepositBatch particles at a time.
+// for the exact mass check.
+//
+// Contributors are the particles whose base cell lies in planes x0 or x0-1
+// and rows y0-1 .. y0+TY-1. In cell order the rows of one plane are a single
+// contiguous range (two when row y0-1 wraps to N-1), so the tile reads at most
+// four contiguous segments of the cell-ordered particles, located through the
+// bucket starts `offset` (`order`: sorted slot -> particle, or null when the
+// arrays are in cell order). A bucket can straddle a segment edge, so each
+// particle is kept only if its own base cell lies in the segment's plane and
+// rows: segments are disjoint in (plane, row), hence every contributor is
+// counted exactly once. Threads walk the concatenated segments
+// kDepositBatch particles at a time.
 constexpr int kDepositThreads = 256;
 constexpr int kDepositBatch = 4;
-constexpr int kMaxTileRows = 2 * (90 + 1);   // 2 (TY + 1) with TY <= max(8192 / N, N <= 90)
+
+// Rows of a deposit tile: 8-byte accumulators, at most 64 KiB per tile.
+inline int deposit_rows(int N) {
+    int ty = 8192 / N;
+    if (ty < 1) ty = 1;
+    return ty > N ? N : ty;
+}
 
 template <typename OUT>
 __global__ void __launch_bounds__(kDepositThreads)
@@ -223,67 +235,84 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
                 const uint32_t* __restrict__ offset, int shift, int N, int TY,
                 const FixedPlan* plan, OUT* __restrict__ out, unsigned long long* qsum,
                 const unsigned int* status) {
-    extern __shared__ unsigned long long qtile[];
-    __shared__ uint32_t r_p0[kMaxTileRows];
-    __shared__ uint32_t r_cum[kMaxTileRows + 1];
-    __shared__ uint32_t warp_tot[kDepositThreads / 32];
+    extern __shared__ __align__(16) unsigned long long qtile[];
+    __shared__ uint32_t seg_p0[4];
+    __shared__ uint32_t seg_cum[5];
+    __shared__ int seg_plane[4], seg_row_lo[4], seg_row_hi[4], seg_xr[4];
     if (*status & ST_BLOCKS_PUBLISH) return;
     const int tid = threadIdx.x;
     const int x0 = blockIdx.y;
     const int y0 = blockIdx.x * TY;
     const int ty = N - y0 < TY ? N - y0 : TY;
-    // contributor rows: r = xr * nyr + k, xb = x0 - xr, yb = y0 + k - halo
     const int halo = ty == N ? 0 : 1;   // a tile spanning all rows has no halo
-    const int nyr = ty + halo;
-    const int nrows = 2 * nyr;
-    uint32_t len = 0;
-    if (tid < nrows) {
-        const int xr = tid / nyr;
-        const uint32_t xb = xr == 0 ? x0 : (x0 == 0 ? N - 1 : x0 - 1);
-        const int yy = y0 + tid % nyr - halo;
-        const uint32_t yb = static_cast<uint32_t>(yy < 0 ? yy + N : yy);
-        const uint64_t c0 = (static_cast<uint64_t>(xb) * N + yb) * N;
-        const uint32_t p0 = offset[c0 >> shift];
-        r_p0[tid] = p0;
-        len = offset[((c0 + N - 1) >> shift) + 1] - p0;
+    if (tid == 0) {
+        // segments: (plane x0 then x0-1) x (row ranges); a wrapped halo row
+        // N-1 is its own segment
+        int ns = 0;
+        uint32_t cum = 0;
+        for (int xr = 0; xr < 2; ++xr) {
+            const int p = xr == 0 ? x0 : (x0 == 0 ? N - 1 : x0 - 1);
+            int lo[2], hi[2], nr = 0;
+            if (halo && y0 == 0) {
+                lo[nr] = N - 1; hi[nr++] = N - 1;
+                lo[nr] = 0; hi[nr++] = ty - 1;
+            } else {
+                lo[nr] = y0 - halo; hi[nr++] = y0 + ty - 1;
+            }
+            for (int k = 0; k < nr; ++k) {
+                const uint64_t c_lo = (static_cast<uint64_t>(p) * N + lo[k]) * N;
+                const uint64_t c_hi = (static_cast<uint64_t>(p) * N + hi[k]) * N + (N - 1);
+                const uint32_t a = offset[c_lo >> shift];
+                const uint32_t b = offset[(c_hi >> shift) + 1];
+                seg_p0[ns] = a;
+                seg_cum[ns] = cum;
+                seg_plane[ns] = p;
+                seg_row_lo[ns] = lo[k];
+                seg_row_hi[ns] = hi[k];
+                seg_xr[ns] = xr;
+                cum += b - a;
+                ++ns;
+            }
+        }
+        for (int k = ns; k < 4; ++k) {
+            seg_p0[k] = 0;
+            seg_cum[k] = cum;
+            seg_plane[k] = -1;
+            seg_row_lo[k] = 1;
+            seg_row_hi[k] = 0;
+            seg_xr[k] = 0;
+        }
+        seg_cum[4] = cum;
     }
-    // block-wide inclusive scan of the range lengths (nrows <= blockDim)
-    uint32_t incl = len;
-    const int lane = tid & 31;
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
+    const int tcells = ty * N;
+    {
+        ulonglong2* q2 = reinterpret_cast<ulonglong2*>(qtile);
+        for (int e = tid; e < tcells / 2; e += kDepositThreads) q2[e] = make_ulonglong2(0ull, 0ull);
+        if ((tcells & 1) && tid == 0) qtile[tcells - 1] = 0ull;
     }
-    if (lane == 31) warp_tot[tid >> 5] = incl;
-    for (int e = tid; e < ty * N; e += kDepositThreads) qtile[e] = 0ull;
     __syncthreads();
-    uint32_t before = 0;
-    for (int w = 0; w < (tid >> 5); ++w) before += warp_tot[w];
-    if (tid < nrows) r_cum[tid + 1] = before + incl;
-    if (tid == 0) r_cum[0] = 0;
-    __syncthreads();
-    const uint32_t total = r_cum[nrows];
+    const uint32_t c1 = seg_cum[1], c2 = seg_cum[2], c3 = seg_cum[3];
+    const uint32_t total = seg_cum[4];
     const int B = plan->B;
     const unsigned one = 1u << B;
-    int r = 0;
     for (uint32_t v0 = tid; v0 < total; v0 += kDepositBatch * kDepositThreads) {
         uint32_t idx[kDepositBatch];
-        int row[kDepositBatch];
+        int sg[kDepositBatch];
 #pragma unroll
         for (int k = 0; k < kDepositBatch; ++k) {
             const uint32_t v = v0 + k * kDepositThreads;
-            row[k] = -1;
+            sg[k] = -1;
             if (v < total) {
-                while (r_cum[r + 1] <= v) ++r;
-                row[k] = r;
-                const uint32_t q = r_p0[r] + (v - r_cum[r]);
+                const int g = (v >= c1) + (v >= c2) + (v >= c3);
+                sg[k] = g;
+                const uint32_t q = seg_p0[g] + (v - seg_cum[g]);
                 idx[k] = order ? order[q] : q;
             }
         }
         uint32_t u[kDepositBatch][3];
 #pragma unroll
         for (int k = 0; k < kDepositBatch; ++k) {
-            if (row[k] >= 0) {
+            if (sg[k] >= 0) {
                 u[k][0] = ux[idx[k]];
                 u[k][1] = uy[idx[k]];
                 u[k][2] = uz[idx[k]];
@@ -291,26 +320,26 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
         }
 #pragma unroll
         for (int k = 0; k < kDepositBatch; ++k) {
-            if (row[k] < 0) continue;
-            const int xr = row[k] / nyr;
-            const uint32_t xb = xr == 0 ? x0 : (x0 == 0 ? N - 1 : x0 - 1);
-            const int yy = y0 + row[k] % nyr - halo;
-            const uint32_t yb = static_cast<uint32_t>(yy < 0 ? yy + N : yy);
+            if (sg[k] < 0) continue;
+            const int g = sg[k];
             uint32_t fx, fy, fz;
             const uint32_t ix = cell_of(u[k][0], N, fx);
             const uint32_t iy = cell_of(u[k][1], N, fy);
             const uint32_t iz = cell_of(u[k][2], N, fz);
-            if (ix != xb || iy != yb) continue;  // a bucket wider than this row
+            // keep the particle only in the segment of its own base cell
+            if (static_cast<int>(ix) != seg_plane[g] || static_cast<int>(iy) < seg_row_lo[g]
+                || static_cast<int>(iy) > seg_row_hi[g])
+                continue;
             fx >>= (32 - B);
             fy >>= (32 - B);
             fz >>= (32 - B);
-            const unsigned long long wx = xr == 0 ? one - fx : fx;
+            const unsigned long long wx = seg_xr[g] == 0 ? one - fx : fx;
             const unsigned long long wy[2] = {one - fy, fy};
             const unsigned long long wz[2] = {one - fz, fz};
             const uint32_t gz[2] = {iz, iz + 1 == static_cast<uint32_t>(N) ? 0u : iz + 1};
 #pragma unroll
             for (int oy = 0; oy < 2; ++oy) {
-                const uint32_t ys = yb + oy == static_cast<uint32_t>(N) ? 0u : yb + oy;
+                const uint32_t ys = iy + oy == static_cast<uint32_t>(N) ? 0u : iy + oy;
                 const int ly = static_cast<int>(ys) - y0;
                 if (ly < 0 || ly >= ty) continue;
                 const unsigned long long wxy = wx * wy[oy];
@@ -326,7 +355,7 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
     const long long mean = plan->mean_q;
     OUT* o = out + (static_cast<uint64_t>(x0) * N + y0) * N;
     unsigned long long local = 0;
-    for (int e = tid; e < ty * N; e += kDepositThreads) {
+    for (int e = tid; e < tcells; e += kDepositThreads) {
         const long long v = static_cast<long long>(qtile[e]) - mean;
         store_cell(&o[e], v);
         local += static_cast<unsigned long long>(v);
@@ -900,8 +929,8 @@ template <typename OUT>
 int deposit_tiles(State* st, int P, const uint32_t* order, OUT* out, unsigned long long* qsum,
                   const unsigned int* d_status, cudaStream_t s) {
     const int N = st->N;
-    const int TY = deposit_tile_rows(N);
-    const size_t smem = sizeof(unsigned long long) * static_cast<size_t>(TY) * N;
+    const int TY = deposit_rows(N);
+    const size_t smem = 8 * static_cast<size_t>(TY) * N;
     CK(cudaFuncSetAttribute(k_deposit_tiles<OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(smem)));
     const dim3 grid((N + TY - 1) / TY, N);

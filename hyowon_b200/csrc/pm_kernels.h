@@ -54,14 +54,6 @@ void launch_iota_u32(uint32_t n, uint32_t* out, cudaStream_t s);
 void launch_order(uint32_t n, const uint32_t* key, const uint32_t* rank, const uint32_t* offset,
                   uint32_t* order, const unsigned int* status, cudaStream_t s);
 
-// Rows of a deposit tile (a tile is TY mesh rows of one x plane, held in
-// shared memory as 8-byte accumulators: TY * N * 8 <= 64 KiB).
-inline int deposit_tile_rows(int N) {
-    int ty = 8192 / N;
-    if (ty < 1) ty = 1;
-    return ty > N ? N : ty;
-}
-
 // ---- FP64 form (pm_fp64.cu) -----------------------------------------------
 void launch_validate_inputs_f64(uint32_t n, const double* x, const double* y,
                                 const double* z, const double* mass, unsigned int* status,

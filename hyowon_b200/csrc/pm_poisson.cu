@@ -62,6 +62,9 @@ using fft::mk;
 #ifndef HYOWON_FFT_MINB_Z
 #define HYOWON_FFT_MINB_Z 2
 #endif
+#ifndef HYOWON_FFT_NBUF
+#define HYOWON_FFT_NBUF 2
+#endif
 #ifndef HYOWON_FFT_MINB_C
 #define HYOWON_FFT_MINB_C 1
 #endif
@@ -98,7 +101,9 @@ template <typename T, int LOG2N> struct Geo {
     static constexpr size_t smem_zf = sizeof(C) * M * SZ;
     static constexpr size_t smem_zi = sizeof(C) * Hz * SZ;
     static constexpr unsigned tile_bytes = sizeof(C) * N * CC;   // one y/x-pass tile
-    static constexpr size_t smem_c = 2ull * tile_bytes;           // double buffered
+    // tile buffers of the y/x passes: HYOWON_FFT_NBUF deep where shared memory allows
+    static constexpr int nbuf = (HYOWON_FFT_NBUF * tile_bytes <= 200u * 1024u) ? HYOWON_FFT_NBUF : 2;
+    static constexpr size_t smem_c = static_cast<size_t>(nbuf) * tile_bytes;
     static constexpr int box = N < 256 ? N : 256;                 // TMA box rows
     static constexpr int units = CC * static_cast<int>(sizeof(C)) / 8;  // 8-byte units per row
 };
@@ -273,11 +278,11 @@ constexpr unsigned kWaitLimit = 1u << 24;
 // spectrum: tile t = (kc, s) with kc = t / N, s = t % N; y pass (AXIS 1):
 // s = kx, the tile is the contiguous block H[kc][kx][.][.]; x pass (AXIS 0):
 // s = ky, elements H[kc][.][ky][.] (128-byte-or-less runs N*CC apart).
-// Persistent blocks; one thread streams the next tile into the second
-// shared-memory buffer with TMA loads while the block transforms the current
-// one (dense rows, no padding: a half/quarter warp reads one 64-byte row).
-// With GREEN (the y pass): forward transform, Green's multiply, inverse
-// transform. Results are stored from registers.
+// Persistent blocks; one thread keeps the next nbuf-1 tiles of the block
+// streaming into the other shared-memory buffers with TMA loads while the
+// block transforms the current one (dense rows, no padding: a half/quarter
+// warp reads one 64-byte row). With GREEN (the x pass): forward transform,
+// Green's multiply, inverse transform. Results are stored from registers.
 template <typename T, int LOG2N, int AXIS, int SIGN, bool GREEN, typename GF>
 __global__ void __launch_bounds__(Geo<T, LOG2N>::TC, 1)
 k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
@@ -286,12 +291,13 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
     using C = cx_t<T>;
     constexpr int P = G::N / 16;
     constexpr int S = G::CC;
+    constexpr int NB = G::nbuf;
     constexpr size_t axis_stride = AXIS == 1 ? static_cast<size_t>(G::CC)
                                              : static_cast<size_t>(G::N) * G::CC;
     constexpr size_t seq_stride = AXIS == 1 ? static_cast<size_t>(G::N) * G::CC
                                             : static_cast<size_t>(G::CC);
     extern __shared__ __align__(1024) unsigned char smem_tiles[];
-    __shared__ __align__(8) uint64_t full[2];
+    __shared__ __align__(8) uint64_t full[NB];
     const int tid = threadIdx.x;
     const int c = tid % G::CC;
     const int j = tid / G::CC;
@@ -311,27 +317,39 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
         }
     };
     if (tid == 0) {
-        tma::mbar_init(&full[0], 1);
-        tma::mbar_init(&full[1], 1);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) tma::mbar_init(&full[b], 1);
         tma::fence_barrier_init();
     }
     __syncthreads();
     unsigned t = blockIdx.x;
-    if (tid == 0 && t < tiles) issue(t, 0);
+    if (tid == 0) {
+        // prologue: the first nbuf-1 tiles of this block
+#pragma unroll
+        for (int b = 0; b < NB - 1; ++b) {
+            const unsigned tb = t + static_cast<unsigned>(b) * gridDim.x;
+            if (tb < tiles) issue(tb, b);
+        }
+    }
     for (unsigned i = 0; t < tiles; ++i, t += gridDim.x) {
-        const int b = static_cast<int>(i & 1u);
-        const unsigned nt = t + gridDim.x;
+        const int b = static_cast<int>(i % NB);
+        const unsigned parity = (i / NB) & 1u;
+        // refill the buffer the previous iteration finished with
+        const unsigned nt = t + static_cast<unsigned>(NB - 1) * gridDim.x;
         if (tid == 0 && nt < tiles) {
             tma::fence_proxy_async();
-            issue(nt, b ^ 1);
+            issue(nt, static_cast<int>((i + NB - 1) % NB));
         }
-        const bool ok = tma::mbar_wait(&full[b], (i >> 1) & 1u, kWaitLimit);
+        const bool ok = tma::mbar_wait(&full[b], parity, kWaitLimit);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
                 atomicOr(status, ST_PIPELINE);
                 // let this block's copies in flight land before it exits
-                tma::mbar_wait(&full[b], (i >> 1) & 1u, kWaitLimit);
-                if (nt < tiles) tma::mbar_wait(&full[b ^ 1], ((i + 1) >> 1) & 1u, kWaitLimit);
+                for (int k = 0; k < NB; ++k) {
+                    const unsigned ik = i + static_cast<unsigned>(k);
+                    const unsigned tk = t + static_cast<unsigned>(k) * gridDim.x;
+                    if (tk < tiles) tma::mbar_wait(&full[ik % NB], (ik / NB) & 1u, kWaitLimit);
+                }
             }
             return;
         }
