@@ -8,7 +8,7 @@ Mpc/h, flat LCDM (Om 0.3, OL 0.7), 1LPT at z = 49 from seeded white noise
 inputs: no public dataset is involved.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp64|fp32]
-                    [--config c1|c2|c3] [--impl ours|reference]
+                    [--config c1|c2|c3|c3h] [--impl ours|reference]
 
 Prints one JSON line (rank 0). `value` = particle-steps/s over the K timed steps
 with the state resident in HBM, timed with CUDA events on the library's stream
@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--form", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--no-compare", action="store_true",
                     help="skip timing the other arithmetic form")
-    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c3h"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -212,7 +212,7 @@ def cpu_baseline_sample(cfg_name):
     except Exception as e:  # pragma: no cover
         return {"value": None, "unit": "particle-steps/s", "cores": os.cpu_count(),
                 "kind": "reference", "sample": f"unavailable: {e}"}
-    name = "c2" if cfg_name == "c3" else cfg_name
+    name = "c2" if cfg_name in ("c3", "c3h") else cfg_name
     c = ic.CONFIGS[name]
     a0, dl = ic.config_schedule(name)
     st = lpt_ics(ic.white_noise(c["n_side"], c["seed"]), c["n_side"], c["box"], a0)

@@ -65,8 +65,11 @@ using fft::mk;
 #ifndef HYOWON_FFT_NBUF
 #define HYOWON_FFT_NBUF 2
 #endif
-#ifndef HYOWON_FFT_MINB_C
-#define HYOWON_FFT_MINB_C 1
+#ifndef HYOWON_FFT_MINB_C32
+#define HYOWON_FFT_MINB_C32 1
+#endif
+#ifndef HYOWON_FFT_MINB_C64
+#define HYOWON_FFT_MINB_C64 1
 #endif
 
 template <typename T, int LOG2N> struct Shape;
@@ -284,7 +287,7 @@ constexpr unsigned kWaitLimit = 1u << 24;
 // warp reads one 64-byte row). With GREEN (the x pass): forward transform,
 // Green's multiply, inverse transform. Results are stored from registers.
 template <typename T, int LOG2N, int AXIS, int SIGN, bool GREEN, typename GF>
-__global__ void __launch_bounds__(Geo<T, LOG2N>::TC, 1)
+__global__ void __launch_bounds__(Geo<T, LOG2N>::TC, sizeof(T) == 4 ? HYOWON_FFT_MINB_C32 : HYOWON_FFT_MINB_C64)
 k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
           const cx_t<T>* __restrict__ tw, GF green, unsigned int* status) {
     using G = Geo<T, LOG2N>;

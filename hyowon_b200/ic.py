@@ -172,6 +172,10 @@ CONFIGS = {
     "c2": dict(n_side=128, box=256.0, mesh=256, z_start=49.0, steps=64, seed=1),
     "c3": dict(n_side=512, box=1000.0, mesh=1024, z_start=49.0, steps=64, seed=7),
     "c4": dict(n_side=128, box=256.0, mesh=128, z_start=19.0, steps=16, seed=3),
+    # c3 at half the side length: same cell size and particle density, 1/8 of
+    # the volume (meshes still far larger than L2); the size profiling
+    # captures of the step kernels use
+    "c3h": dict(n_side=256, box=500.0, mesh=512, z_start=49.0, steps=64, seed=7),
 }
 
 
