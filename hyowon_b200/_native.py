@@ -60,6 +60,14 @@ class Diagnostics(ctypes.Structure):
                 ("momentum_force_contraction", c_double)]
 
 
+class PkBin(ctypes.Structure):
+    """hyowon_pk_bin_t (include/hyowon_pm.h)."""
+    _fields_ = [("k_low", c_double), ("k_mean", c_double), ("k_high", c_double),
+                ("p_raw", c_double), ("p_corrected", c_double),
+                ("mean_cic_power_deconvolution_factor", c_double),
+                ("shot_noise_reference", c_double), ("mode_count", c_u64)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "hyowon_pm_create": (c_int, [c_double, c_u64, c_int, c_int, c_double, c_int,
@@ -84,6 +92,8 @@ _SIGS = {
     "hyowon_pm_set_sort_interval": (c_int, [c_void_p, c_int]),
     "hyowon_pm_last_timing": (c_int, [c_void_p, P_double]),
     "hyowon_pm_diagnostics": (c_int, [c_void_p, c_double, ctypes.POINTER(Diagnostics)]),
+    "hyowon_pm_power_spectrum": (c_int, [c_void_p, c_u64, c_int, c_double, c_int, c_int,
+                                         ctypes.POINTER(PkBin)]),
     "hyowon_vjp_1lpt_pm": (c_int, [c_void_p, P_double, P_double, P_double, P_double,
                                    P_double, P_double]),
     "hyowon_vjp_last_error": (ctypes.c_char_p, []),

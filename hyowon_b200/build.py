@@ -38,6 +38,7 @@ UNITS = [
     ("pm_poisson.cu", []),
     ("pm_noalloc.cu", ["--fmad=false"]),
     ("pm_diag.cu", ["--fmad=false"]),
+    ("pm_pk.cu", ["--fmad=false"]),
     ("cosmology.cpp", []),
 ]
 

@@ -1155,6 +1155,23 @@ int download(State* st, cudaStream_t s, double* x, double* y, double* z, double*
     return rc;
 }
 
+__global__ void k_widen_positions(uint32_t n, const uint32_t* __restrict__ u, double scale,
+                                  double* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = static_cast<double>(u[i]) * scale;
+}
+
+int positions_f64(State* st, cudaStream_t s, double* x, double* y, double* z) {
+    double* outs[3] = {x, y, z};
+    for (int a = 0; a < 3; ++a) {
+        ++st->launches;
+        k_widen_positions<<<blocks_for(st->n), kThreads, 0, s>>>(st->n, st->pos[st->pc][a],
+                                                                 st->L / kTwo32, outs[a]);
+    }
+    CK(cudaPeekAtLastError());
+    return HYOWON_OK;
+}
+
 int diagnostics(State* st, cudaStream_t s, bool with_potential, double* scratch, double* sums) {
     diag::InputsF32 in{};
     in.n = st->n;

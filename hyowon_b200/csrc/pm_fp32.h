@@ -53,6 +53,9 @@ int download_potential(State* st, cudaStream_t s, double* phi);
 // Global binary64 sums of the current state (pm_diag.h order) into host
 // sums[kTerms], using the device scratch `scratch` (diag::scratch_doubles()).
 int diagnostics(State* st, cudaStream_t s, bool with_potential, double* scratch, double* sums);
+// Positions widened to binary64 (x = u L / 2^32, exact) into device arrays of
+// the particle count, in the current storage order.
+int positions_f64(State* st, cudaStream_t s, double* x, double* y, double* z);
 int download_mass_mesh(State* st, cudaStream_t s, unsigned int* d_status, double* mesh);
 
 }  // namespace fp32

@@ -28,6 +28,7 @@
 #include "pm_poisson.h"
 #include "pm_kernels.h"
 #include "pm_lpt.h"
+#include "pm_pk.h"
 
 using namespace hyowon;
 
@@ -1135,6 +1136,101 @@ int hyowon_pm_diagnostics(hyowon_pm_t h, double a, hyowon_pm_diagnostics_t* out)
     if (with_phi && r[0] != 0.0 && out->potential_energy_comoving == 0.0)
         return fail(h, HYOWON_EUNDERFLOW, "PMSolver potential-energy diagnostic underflowed");
     return HYOWON_OK;
+}
+
+int hyowon_pm_power_spectrum(hyowon_pm_t h, uint64_t mesh_size, int num_bins,
+                             double max_k_fraction_nyquist, int subtract_shot_noise,
+                             int interlaced, hyowon_pk_bin_t* bins) {
+    if (!h || !bins) return HYOWON_EINVAL;
+    if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
+    const uint64_t N = mesh_size ? mesh_size : static_cast<uint64_t>(h->N);
+    if (N < 2 || N > 4096) return fail(h, HYOWON_EINVAL, "MatterPowerSpectrum mesh_size must be in [2, 4096]");
+    if (num_bins < 1 || num_bins > 256)
+        return fail(h, HYOWON_EINVAL, "MatterPowerSpectrum num_bins must be in [1, 256]");
+    if (!std::isfinite(max_k_fraction_nyquist) || max_k_fraction_nyquist <= 0.0
+        || max_k_fraction_nyquist > 1.0)
+        return fail(h, HYOWON_EINVAL, "MatterPowerSpectrum max_k_fraction_nyquist must be in (0,1]");
+    if (interlaced && subtract_shot_noise)
+        return fail(h, HYOWON_EINVAL,
+                    "Interlaced shot-noise subtraction is disabled until the estimator uses an "
+                    "interlacing-matched alias model");
+    const uint32_t n = h->n;
+    double* pos = nullptr;       // widened positions of the precision form
+    double* weights = nullptr;   // m_i / max m, explicit masses only
+    double weight_sum = static_cast<double>(n);
+    double msf = 1.0 / static_cast<double>(n);
+    int rc = HYOWON_OK;
+    const double *x = nullptr, *y = nullptr, *z = nullptr;
+    if (h->precision == HYOWON_FP32_FIXED) {
+        if (dalloc(&pos, 3ull * n) != cudaSuccess) return fail(h, HYOWON_ENOMEM, "power spectrum: staging");
+        rc = status_or_cuda(h, fp32::positions_f64(h->f32, h->stream, pos, pos + n, pos + 2ull * n));
+        x = pos;
+        y = pos + n;
+        z = pos + 2ull * n;
+    } else {
+        x = h->pos[h->pc][0];
+        y = h->pos[h->pc][1];
+        z = h->pos[h->pc][2];
+        if (h->has_masses) {
+            // FourierDensityBuilder::build: weights in units of the largest
+            // mass, compensated sums of w and w^2 (fourier_density_field.cpp:170-230)
+            std::vector<double> m(n);
+            if (cudaMemcpyAsync(m.data(), h->mass[h->ic], sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                h->stream) != cudaSuccess
+                || cudaStreamSynchronize(h->stream) != cudaSuccess)
+                return fail(h, HYOWON_ECUDA, "power spectrum: mass copy failed");
+            double unit = 0.0;
+            for (double v : m) unit = std::max(unit, v);
+            if (!(unit > 0.0) || !std::isfinite(unit))
+                return fail(h, HYOWON_EINVAL, "FourierDensityBuilder masses must be finite and positive");
+            long double s1 = 0.0L, c1 = 0.0L, s2 = 0.0L, c2 = 0.0L;
+            auto add = [](long double& s, long double& c, long double v) {
+                const long double t = s + v;
+                c += std::fabs(s) >= std::fabs(v) ? (s - t) + v : (v - t) + s;
+                s = t;
+            };
+            for (double& v : m) {
+                v = v / unit;
+                add(s1, c1, static_cast<long double>(v));
+                add(s2, c2, static_cast<long double>(v) * static_cast<long double>(v));
+            }
+            const long double ws = s1 + c1;
+            weight_sum = static_cast<double>(ws);
+            msf = std::min(1.0, static_cast<double>((s2 + c2) / (ws * ws)));
+            if (dalloc(&weights, n) != cudaSuccess
+                || cudaMemcpyAsync(weights, m.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
+                                   h->stream) != cudaSuccess
+                || cudaStreamSynchronize(h->stream) != cudaSuccess) {
+                cudaFree(weights);
+                return fail(h, HYOWON_ENOMEM, "power spectrum: weight staging");
+            }
+        }
+    }
+    if (rc == HYOWON_OK) {
+        const pk::Request req{num_bins, max_k_fraction_nyquist, subtract_shot_noise != 0,
+                              interlaced != 0};
+        std::vector<pk::Bin> out(num_bins);
+        std::string err;
+        rc = pk::compute(h->L, static_cast<int>(N), n, x, y, z, weights, weight_sum, msf, req,
+                         out.data(), &err, h->stream);
+        if (rc) {
+            fail(h, rc, err);
+        } else {
+            for (int b = 0; b < num_bins; ++b) {
+                bins[b].k_low = out[b].k_low;
+                bins[b].k_mean = out[b].k_mean;
+                bins[b].k_high = out[b].k_high;
+                bins[b].p_raw = out[b].p_raw;
+                bins[b].p_corrected = out[b].p_corrected;
+                bins[b].mean_cic_power_deconvolution_factor = out[b].mean_deconvolution;
+                bins[b].shot_noise_reference = out[b].shot_noise;
+                bins[b].mode_count = out[b].mode_count;
+            }
+        }
+    }
+    cudaFree(pos);
+    cudaFree(weights);
+    return rc;
 }
 
 }  // extern "C"

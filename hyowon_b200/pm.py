@@ -245,6 +245,23 @@ class PMSolver:
                 "force_norm_sum": d.force_norm_sum, "force_balance": d.force_balance,
                 "momentum_force_contraction": d.momentum_force_contraction}
 
+    def power_spectrum(self, num_bins: int, max_k_fraction_nyquist: float = 1.0,
+                       subtract_shot_noise: bool = False, interlaced: bool = False,
+                       mesh_size: int = 0) -> dict:
+        """MatterPowerSpectrum::compute_pk of the device state
+        (hyowon_pm_power_spectrum): per-bin arrays k_low, k_mean, k_high,
+        p_raw, p_corrected, mean_cic_power_deconvolution_factor,
+        shot_noise_reference, mode_count. mesh_size 0 uses the solver's mesh."""
+        bins = (nat.PkBin * int(num_bins))()
+        self._check(nat.lib().hyowon_pm_power_spectrum(
+            self._h, int(mesh_size), int(num_bins), float(max_k_fraction_nyquist),
+            int(bool(subtract_shot_noise)), int(bool(interlaced)), bins), "power_spectrum")
+        keys = ("k_low", "k_mean", "k_high", "p_raw", "p_corrected",
+                "mean_cic_power_deconvolution_factor", "shot_noise_reference")
+        out = {k: np.array([getattr(b, k) for b in bins]) for k in keys}
+        out["mode_count"] = np.array([b.mode_count for b in bins], dtype=np.uint64)
+        return out
+
     def set_timing(self, on: bool):
         self._check(nat.lib().hyowon_pm_set_timing(self._h, int(on)), "set_timing")
 

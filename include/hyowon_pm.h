@@ -200,6 +200,33 @@ typedef struct hyowon_pm_diagnostics {
 } hyowon_pm_diagnostics_t;
 int hyowon_pm_diagnostics(hyowon_pm_t h, double a, hyowon_pm_diagnostics_t* out);
 
+/* Matter power spectrum of the device particle state, the estimator of
+ * analysis::MatterPowerSpectrum::compute_pk (src/analysis/matter_power_spectrum.cpp:50-226,
+ * include/cosmo_nbody/analysis/matter_power_spectrum.hpp:16-60) over
+ * FourierDensityBuilder::build (src/analysis/fourier_density_field.cpp:110-376):
+ * CIC density contrast on its own mesh of side mesh_size (0: the handle's
+ * mesh), r2c / N^3, optional interlacing, CIC-window deconvolution,
+ * optional aliased shot-noise subtraction, num_bins logarithmic bins from
+ * 2 pi / L to max_k_fraction_nyquist * pi N / L. Binary64 in both arithmetic
+ * forms (the precision form's fixed-point positions are widened exactly).
+ * bins[num_bins] receives PowerSpectrumBin's fields. 1 <= num_bins <= 256;
+ * max_k_fraction_nyquist in (0, 1]; interlaced together with
+ * subtract_shot_noise is rejected (HYOWON_EINVAL), as the reference does.
+ * Allocates its meshes and transform plan for the call. */
+typedef struct hyowon_pk_bin {
+    double k_low;
+    double k_mean;
+    double k_high;
+    double p_raw;
+    double p_corrected;
+    double mean_cic_power_deconvolution_factor;
+    double shot_noise_reference;
+    uint64_t mode_count;
+} hyowon_pk_bin_t;
+int hyowon_pm_power_spectrum(hyowon_pm_t h, uint64_t mesh_size, int num_bins,
+                             double max_k_fraction_nyquist, int subtract_shot_noise,
+                             int interlaced, hyowon_pk_bin_t* bins);
+
 #ifdef __cplusplus
 }
 #endif

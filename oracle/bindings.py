@@ -223,6 +223,26 @@ class Reference:
         self._check(rc, "ref_pm_forces_energy")
         return ax, ay, az, e.value
 
+    def power_spectrum(self, L, mesh, x, y, z, masses=None, uniform_mass=1.0, num_bins=16,
+                       subtract_shot_noise=False, interlaced=False, max_k_fraction_nyquist=1.0):
+        """MatterPowerSpectrum::compute_pk: dict of per-bin arrays."""
+        x, y, z = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z))
+        m = None if masses is None else np.ascontiguousarray(masses, dtype=np.float64)
+        out = np.zeros(7 * num_bins)
+        counts = np.zeros(num_bins, dtype=np.uint64)
+        rc = self.lib.ref_power_spectrum(
+            _c_double(L), _c_u64(mesh), _c_u64(x.size), _dp(x), _dp(y), _dp(z), _dp(m),
+            _c_double(uniform_mass), _c_int(num_bins), _c_int(int(subtract_shot_noise)),
+            _c_int(int(interlaced)), _c_double(max_k_fraction_nyquist), _dp(out),
+            _ip(counts, ctypes.c_uint64))
+        self._check(rc, "ref_power_spectrum")
+        o = out.reshape(num_bins, 7)
+        keys = ("k_low", "k_mean", "k_high", "p_raw", "p_corrected",
+                "mean_cic_power_deconvolution_factor", "shot_noise_reference")
+        res = {k: o[:, i].copy() for i, k in enumerate(keys)}
+        res["mode_count"] = counts
+        return res
+
     def conservation(self, L, N, px, py, pz, ax, ay, az, mass, a):
         """ConservationChecks: (kinetic energy at a, sum m p . g)."""
         arr = [np.ascontiguousarray(v, dtype=np.float64) for v in (px, py, pz, ax, ay, az)]

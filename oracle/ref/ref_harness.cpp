@@ -8,6 +8,8 @@
 // Every entry returns 0 on success or a nonzero code naming the reference
 // exception type that was thrown (see ref_error_code); ref_last_error() gives
 // its message. Nothing here is shipped in the product library.
+#include "cosmo_nbody/analysis/matter_power_spectrum.hpp"
+#include "cosmo_nbody/analysis/periodic_domain.hpp"
 #include "cosmo_nbody/config/memory_policy.hpp"
 #include "cosmo_nbody/config/simulation_parameters.hpp"
 #include "cosmo_nbody/core/particle_store.hpp"
@@ -210,6 +212,42 @@ int ref_pm_forces_energy(double L, std::uint64_t N, int deconvolve, std::uint64_
             std::span<double>(ay, n), std::span<double>(az, n), true);
         if (!d.has_value()) throw std::logic_error("no PMForceDiagnostics returned");
         *energy = d->potential_energy_comoving;
+    });
+}
+
+// analysis::MatterPowerSpectrum::compute_pk (src/analysis/matter_power_spectrum.cpp)
+// on a ParticleStore with these positions and masses (or a uniform mass), with
+// its own CIC mesh of side mesh_size. out[7 * num_bins] receives per bin
+// {k_low, k_mean, k_high, p_raw, p_corrected, mean_cic_power_deconvolution_factor,
+// shot_noise_reference}; counts[num_bins] the mode counts.
+int ref_power_spectrum(double L, std::uint64_t mesh_size, std::uint64_t n, const double* x,
+                       const double* y, const double* z, const double* masses,
+                       double uniform_mass, int num_bins, int subtract_shot_noise,
+                       int interlaced, double max_k_fraction_nyquist, double* out,
+                       std::uint64_t* counts) {
+    return guarded([&] {
+        core::ParticleStore store;
+        if (!masses) store.set_uniform_mass(uniform_mass);
+        store.resize(n);
+        std::memcpy(store.get_positions_x().data(), x, sizeof(double) * n);
+        std::memcpy(store.get_positions_y().data(), y, sizeof(double) * n);
+        std::memcpy(store.get_positions_z().data(), z, sizeof(double) * n);
+        if (masses) std::memcpy(store.get_masses().data(), masses, sizeof(double) * n);
+        analysis::PowerSpectrumOptions options;
+        options.num_bins = num_bins;
+        options.subtract_shot_noise = subtract_shot_noise != 0;
+        options.interlaced = interlaced != 0;
+        options.max_k_fraction_nyquist = max_k_fraction_nyquist;
+        const analysis::MatterPowerSpectrum pk(analysis::PeriodicDomain(L),
+                                               static_cast<int>(mesh_size));
+        const auto bins = pk.compute_pk(store, options);
+        for (std::size_t b = 0; b < bins.size(); ++b) {
+            const auto& v = bins[b];
+            const double row[7] = {v.k_low, v.k_mean, v.k_high, v.p_raw, v.p_corrected,
+                                   v.mean_cic_power_deconvolution_factor, v.shot_noise_reference};
+            std::memcpy(out + 7 * b, row, sizeof(row));
+            counts[b] = v.mode_count;
+        }
     });
 }
 

@@ -48,3 +48,8 @@ def schedules():
 @pytest.fixture(scope="session")
 def c1_diag():
     return load_golden("c1_diag.npz")
+
+
+@pytest.fixture(scope="session")
+def pk_golden():
+    return load_golden("pk.npz")

@@ -23,7 +23,12 @@ Fixtures:
                       energy, force balance, momentum-force contraction) and the
                       potential energy / force balance of small_pm with masses
 
+  pk.npz              MatterPowerSpectrum::compute_pk of the c1 states (own mesh
+                      64 and 32; raw, shot-noise-subtracted, interlaced) and of
+                      small_pm with explicit masses
+
     python tests/golden/make_golden.py --only diag    # c1_diag.npz alone
+    python tests/golden/make_golden.py --only pk      # pk.npz alone
 """
 from __future__ import annotations
 
@@ -75,15 +80,49 @@ def diag_fixture(ref):
     np.savez_compressed(os.path.join(HERE, "c1_diag.npz"), **out)
 
 
+PK_CASES = [  # (name, state, mesh, bins, shot, interlaced, max_k_fraction_nyquist)
+    ("ic_raw", "ic", 64, 12, False, False, 1.0),
+    ("s32_raw", "s32", 64, 12, False, False, 1.0),
+    ("s32_shot", "s32", 64, 12, True, False, 1.0),
+    ("s32_interlaced", "s32", 64, 12, False, True, 1.0),
+    ("s32_mesh32", "s32", 32, 8, True, False, 0.5),
+]
+PK_FIELDS = ("k_low", "k_mean", "k_high", "p_raw", "p_corrected",
+             "mean_cic_power_deconvolution_factor", "shot_noise_reference", "mode_count")
+
+
+def pk_fixture(ref):
+    """pk.npz from the reference's MatterPowerSpectrum on the stored c1 states
+    and the small_pm inputs with explicit masses."""
+    d = np.load(os.path.join(HERE, "c1_kdk.npz"))
+    L, m = float(d["box"]), float(d["particle_mass"])
+    out = {}
+    for name, tag, mesh, nb, shot, il, frac in PK_CASES:
+        r = ref.power_spectrum(L, mesh, d[tag + "_x"], d[tag + "_y"], d[tag + "_z"],
+                               uniform_mass=m, num_bins=nb, subtract_shot_noise=shot,
+                               interlaced=il, max_k_fraction_nyquist=frac)
+        out.update({f"{name}__{k}": r[k] for k in PK_FIELDS})
+    sp = np.load(os.path.join(HERE, "small_pm.npz"))
+    for name, shot, il in (("masses_shot", True, False), ("masses_interlaced", False, True)):
+        r = ref.power_spectrum(float(sp["L"]), int(sp["N"]), sp["x"], sp["y"], sp["z"],
+                               masses=sp["masses"], num_bins=5, subtract_shot_noise=shot,
+                               interlaced=il, max_k_fraction_nyquist=0.8)
+        out.update({f"{name}__{k}": r[k] for k in PK_FIELDS})
+    np.savez_compressed(os.path.join(HERE, "pk.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
-    ap.add_argument("--only", choices=["diag"], default=None)
+    ap.add_argument("--only", choices=["diag", "pk"], default=None)
     args = ap.parse_args()
     build_reference(args.ref_root)
     ref = Reference()
     if args.only == "diag":
         diag_fixture(ref)
+        return
+    if args.only == "pk":
+        pk_fixture(ref)
         return
 
     # -- schedules --------------------------------------------------------
@@ -173,6 +212,7 @@ def main():
                     c_r_cut=4.5 * 1.25 * dxc, c_eps=c["box"] / c["n_side"] / 30.0)
     np.savez_compressed(os.path.join(HERE, "treepm_tree.npz"), **tree_out)
     diag_fixture(ref)
+    pk_fixture(ref)
     print(f"c1 reference evolution: {c['steps']} steps in {secs:.2f} s")
 
 
