@@ -140,25 +140,41 @@ def phase_bytes(form, n, N, sort_fraction):
     deposit: read positions once, write the mesh once (binary64 cells; the
       precision form writes FP32 offsets, its int64 accumulators live in
       shared memory);
-    green: read + write the half-complex spectrum;
+    fft_forward / green / fft_inverse: the five-pass transform on a power-of-two
+      mesh, each pass reading and writing its array once -- z r2c (mesh in,
+      half spectrum out) + y pass (half spectrum in and out); x pass with the
+      Green's multiply (in and out); y pass + z c2r (half spectrum in, mesh out);
     gather: read x, p and the potential once; write a and p.
     """
     G = N ** 3
     H = N * N * (N // 2 + 1)
     if form == "fp64":
-        bx = bp = 8
+        bx = bp = b = 8
         dep = n * 3 * bx + G * 8
-        green = H * 16 * 2
-        gather = n * (3 * bx + 3 * bp + 3 * bp + 3 * bp) + G * 8
     else:
-        bx = bp = 4
+        bx = bp = b = 4
         dep = n * 3 * bx + G * 4
-        green = H * 8 * 2
-        gather = n * (3 * bx + 3 * bp + 3 * bp + 3 * bp) + G * 4
+    cplx = H * 2 * b
+    gather = n * (3 * bx + 3 * bp + 3 * bp + 3 * bp) + G * b
     kick = n * (3 * bx + 3 * bp + 3 * bp + 3 * bx + 3 * bp + 8)
     kick += sort_fraction * n * 2 * (3 * bx + 3 * bp + 4 + 8)
     kick += (1.0 - sort_fraction) * n * (4 + 4 + 4)   # cell order: key, rank in; order out
-    return {"sort": kick, "deposit": dep, "green": green, "gather": gather}
+    return {"sort": kick, "deposit": dep, "fft_forward": G * b + cplx + 2 * cplx,
+            "green": 2 * cplx, "fft_inverse": 2 * cplx + cplx + G * b, "gather": gather}
+
+
+# DRAM bytes (read + write) per launch of the single-kernel phases on the c3
+# workload, from the ncu --set full capture of the half-size c3 workload (c3h:
+# 1/8 of the particles and mesh cells, profiles/step_kernels_c3h.md) times 8;
+# each kernel's traffic scales with the particles and cells it processes.
+TRAFFIC_C3 = {
+    ("fp32", "deposit"): 8 * (273 + 484) * 1e6,
+    ("fp32", "green"): 8 * (554 + 499) * 1e6,
+    ("fp32", "gather"): 8 * (942 + 383) * 1e6,
+    ("fp64", "deposit"): 8 * (1466 + 996) * 1e6,
+    ("fp64", "green"): 8 * (1091 + 1034) * 1e6,
+    ("fp64", "gather"): 8 * (1885 + 789) * 1e6,
+}
 
 
 def run_reference(args, world, rank):
@@ -292,8 +308,9 @@ def main():
                                               "fft_inverse", "gather")}
     launches = int(timing["launches"])
 
-    # -- roofline: every phase of ours at its algorithmic bytes; the dominant one
-    #    (largest average duration) is the headline kernel --------------------
+    # -- roofline: every phase of ours at its algorithmic bytes over its CUDA-event
+    #    time; the headline kernel is the longest of the phases that are one
+    #    kernel each (deposit, the x pass with the Green's multiply, gather) ---
     hbm, peak_kind = peaks()
     pb = phase_bytes(args.form, n, N, sort_fraction=0.25)
     table = {}
@@ -302,10 +319,17 @@ def main():
             ach = b / (phases[k] * 1e-3) / 1e9
             table[k] = {"avg_ms": phases[k], "algorithmic_bytes": b, "achieved_GBs": ach,
                         "frac": ach / hbm}
-    dom = max(table, key=lambda k: table[k]["avg_ms"])
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": table[dom]["achieved_GBs"],
-                "peak": hbm, "unit": "GB/s", "frac": table[dom]["frac"], "traffic": None,
-                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": table[dom]["algorithmic_bytes"],
+    single = [k for k in ("deposit", "green", "gather") if k in table]
+    dom = max(single, key=lambda k: table[k]["avg_ms"])
+    kernel_name = {"deposit": "deposit", "green": "x pass + Green's multiply",
+                   "gather": "gather + K2"}[dom]
+    traffic = TRAFFIC_C3.get((args.form, dom)) if args.config == "c3" else None
+    roofline = {"bound": "hbm", "kernel": kernel_name, "phase": dom,
+                "achieved": table[dom]["achieved_GBs"], "peak": hbm, "unit": "GB/s",
+                "frac": table[dom]["frac"], "traffic": traffic,
+                "traffic_source": "ncu capture of the half-size c3 workload x 8" if traffic else None,
+                "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": table[dom]["algorithmic_bytes"],
                 "phases": table}
     step_bytes = algorithmic_bytes(args.form, n, N)
     step_roofline = {"algorithmic_bytes_per_step": step_bytes,
