@@ -109,30 +109,70 @@ __global__ void k_deposit(uint32_t n, const double* __restrict__ x, const double
                 atomicAdd(&mesh[cidx(gx[u], gy[v], gz[w], N)], m * wx[u] * wy[v] * wz[w]);
 }
 
-// Three-component CIC scatter (transpose of the interpolation).
+// Three-component CIC scatter (transpose of the interpolation). Particles
+// stay in lattice order, so consecutive lanes usually hold z-neighbours in the
+// same (x, y) cell column: when lane l+1's lower z cells are lane l's upper z
+// cells, lane l hands its upper-z weights to lane l+1, which adds them to its
+// own before the atomics (half the atomics for a matched pair; the sum is
+// the same up to the order of additions, which atomics leave open anyway).
 template <typename R>
 __global__ void k_scatter3(uint32_t n, const double* __restrict__ x, const double* __restrict__ y,
                            const double* __restrict__ z, const R* __restrict__ v0,
                            const R* __restrict__ v1, const R* __restrict__ v2, Axis a,
                            R* __restrict__ u0, R* __restrict__ u1, R* __restrict__ u2) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    Corner c;
-    if (!corner_of(x[i], y[i], z[i], a, c)) return;
+    const int lane = threadIdx.x & 31;
     const int N = a.N;
-    const R wx[2] = {R(1) - R(c.fx), R(c.fx)}, wy[2] = {R(1) - R(c.fy), R(c.fy)},
-            wz[2] = {R(1) - R(c.fz), R(c.fz)};
-    const int gx[2] = {c.ix, up(c.ix, N)}, gy[2] = {c.iy, up(c.iy, N)}, gz[2] = {c.iz, up(c.iz, N)};
-    const R a0 = v0[i], a1 = v1[i], a2 = v2[i];
+    Corner c{};
+    const bool ok = i < n && corner_of(x[i], y[i], z[i], a, c);
+    // contributions lo[u][v][d] (z cell iz) and hi[u][v][d] (z cell iz + 1)
+    R lo[2][2][3], hi[2][2][3];
+    int gx[2] = {0, 0}, gy[2] = {0, 0}, gz[2] = {0, 0};
+    if (ok) {
+        const R wx[2] = {R(1) - R(c.fx), R(c.fx)}, wy[2] = {R(1) - R(c.fy), R(c.fy)},
+                wz[2] = {R(1) - R(c.fz), R(c.fz)};
+        gx[0] = c.ix; gx[1] = up(c.ix, N);
+        gy[0] = c.iy; gy[1] = up(c.iy, N);
+        gz[0] = c.iz; gz[1] = up(c.iz, N);
+        const R av[3] = {v0[i], v1[i], v2[i]};
+        for (int u = 0; u < 2; ++u)
+            for (int v = 0; v < 2; ++v)
+                for (int d = 0; d < 3; ++d) {
+                    lo[u][v][d] = wx[u] * wy[v] * wz[0] * av[d];
+                    hi[u][v][d] = wx[u] * wy[v] * wz[1] * av[d];
+                }
+    } else {
+        for (int u = 0; u < 2; ++u)
+            for (int v = 0; v < 2; ++v)
+                for (int d = 0; d < 3; ++d) lo[u][v][d] = hi[u][v][d] = R(0);
+    }
+    // the cell column and upper z cell of the lane below
+    const int col = ok ? c.ix * N + c.iy : -1;
+    const int col_below = __shfl_up_sync(0xffffffffu, col, 1);
+    const int ztop_below = __shfl_up_sync(0xffffffffu, gz[1], 1);
+    const bool take = lane > 0 && ok && col_below == col && ztop_below == gz[0];
     for (int u = 0; u < 2; ++u)
         for (int v = 0; v < 2; ++v)
-            for (int w = 0; w < 2; ++w) {
-                const size_t k = cidx(gx[u], gy[v], gz[w], N);
-                const R W = wx[u] * wy[v] * wz[w];
-                atomicAdd(&u0[k], W * a0);
-                atomicAdd(&u1[k], W * a1);
-                atomicAdd(&u2[k], W * a2);
+            for (int d = 0; d < 3; ++d) {
+                const R h = __shfl_up_sync(0xffffffffu, hi[u][v][d], 1);
+                if (take) lo[u][v][d] += h;
             }
+    // whether the lane above took this lane's upper weights
+    const bool given = __shfl_down_sync(0xffffffffu, take ? 1 : 0, 1) != 0 && lane < 31;
+    if (!ok) return;
+    for (int u = 0; u < 2; ++u)
+        for (int v = 0; v < 2; ++v) {
+            const size_t k0 = cidx(gx[u], gy[v], gz[0], N);
+            atomicAdd(&u0[k0], lo[u][v][0]);
+            atomicAdd(&u1[k0], lo[u][v][1]);
+            atomicAdd(&u2[k0], lo[u][v][2]);
+            if (!given) {
+                const size_t k1 = cidx(gx[u], gy[v], gz[1], N);
+                atomicAdd(&u0[k1], hi[u][v][0]);
+                atomicAdd(&u1[k1], hi[u][v][1]);
+                atomicAdd(&u2[k1], hi[u][v][2]);
+            }
+        }
 }
 
 // s = sum_d (u_d[c+e_d] - u_d[c-e_d]) / (2 dx)
@@ -189,6 +229,75 @@ __device__ __forceinline__ void corner_forces(const R* __restrict__ phi, const C
                 g[u][v][w][1] = -(phi[cidx(xs[X], ys[Y + 1], zs[Z], N)] - phi[cidx(xs[X], ys[Y - 1], zs[Z], N)]) * inv_two_dx;
                 g[u][v][w][2] = -(phi[cidx(xs[X], ys[Y], zs[Z + 1], N)] - phi[cidx(xs[X], ys[Y], zs[Z - 1], N)]) * inv_two_dx;
             }
+}
+
+// CIC-interpolated centred-gradient force at one position; false (nothing
+// written) where the cell assignment fails.
+template <typename R>
+__device__ __forceinline__ bool force_at(double px, double py, double pz, const R* __restrict__ phi,
+                                         const Axis& a, R inv_two_dx, R& s0, R& s1, R& s2) {
+    Corner c;
+    if (!corner_of(px, py, pz, a, c)) return false;
+    R g[2][2][2][3];
+    corner_forces(phi, c, a.N, inv_two_dx, g);
+    const R wx[2] = {R(1) - R(c.fx), R(c.fx)}, wy[2] = {R(1) - R(c.fy), R(c.fy)},
+            wz[2] = {R(1) - R(c.fz), R(c.fz)};
+    s0 = s1 = s2 = 0;
+    for (int u = 0; u < 2; ++u)
+        for (int v = 0; v < 2; ++v)
+            for (int w = 0; w < 2; ++w) {
+                const R W = wx[u] * wy[v] * wz[w];
+                s0 += W * g[u][v][w][0];
+                s1 += W * g[u][v][w][1];
+                s2 += W * g[u][v][w][2];
+            }
+    return true;
+}
+
+// One step of the reverse leapfrog between re-solves: x = wrap(x - D p_half),
+// a = F(x) from the potential the forward pass kept for that state,
+// p = p_half - K1 a (the inverse of kick K1 + drift D).
+template <typename R>
+__global__ void k_unstep(uint32_t n, double* __restrict__ x0, double* __restrict__ x1,
+                         double* __restrict__ x2, R* __restrict__ p0, R* __restrict__ p1,
+                         R* __restrict__ p2, double D, double L, const R* __restrict__ phi, Axis a,
+                         R inv_two_dx, R K1, R* __restrict__ ax, R* __restrict__ ay,
+                         R* __restrict__ az) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const R q0 = p0[i], q1 = p1[i], q2 = p2[i];
+    const double nx = wrap_f64(x0[i] + D * static_cast<double>(q0), L);
+    const double ny = wrap_f64(x1[i] + D * static_cast<double>(q1), L);
+    const double nz = wrap_f64(x2[i] + D * static_cast<double>(q2), L);
+    x0[i] = nx;
+    x1[i] = ny;
+    x2[i] = nz;
+    R s0, s1, s2;
+    if (!force_at(nx, ny, nz, phi, a, inv_two_dx, s0, s1, s2)) return;
+    ax[i] = s0;
+    ay[i] = s1;
+    az[i] = s2;
+    p0[i] = q0 + K1 * s0;
+    p1[i] = q1 + K1 * s1;
+    p2[i] = q2 + K1 * s2;
+}
+
+// lp += D lx (the drift's transpose) and p += K a (a kick), one pass.
+template <typename R>
+__global__ void k_axpy3_kick(uint32_t n, double D, const double* __restrict__ x0,
+                             const double* __restrict__ x1, const double* __restrict__ x2,
+                             double* __restrict__ y0, double* __restrict__ y1,
+                             double* __restrict__ y2, R* __restrict__ p0, R* __restrict__ p1,
+                             R* __restrict__ p2, const R* __restrict__ a0,
+                             const R* __restrict__ a1, const R* __restrict__ a2, R K) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    y0[i] += D * x0[i];
+    y1[i] += D * x1[i];
+    y2[i] += D * x2[i];
+    p0[i] += K * a0[i];
+    p1[i] += K * a1[i];
+    p2[i] += K * a2[i];
 }
 
 template <typename R>
@@ -389,7 +498,8 @@ public:
         cufftSetStream(r2c_, s_);
         cufftSetStream(c2r_, s_);
         mesh_ = dmalloc<R>(cells_, owned_);
-        phi_ = dmalloc<R>(cells_, owned_);
+        phi_own_ = dmalloc<R>(cells_, owned_);
+        phi_ = phi_own_;
         modes_ = dmalloc<C>(half_, owned_);
         status_ = dmalloc<unsigned int>(1, owned_);
         ACK(cudaMemsetAsync(status_, 0, sizeof(unsigned int), s_));
@@ -408,8 +518,10 @@ public:
         for (void* p : owned_) cudaFree(p);
     }
 
-    // acc = F(x), phi_ = potential at x.
-    void force() {
+    // acc = F(x); phi_ = potential at x, written to `keep` when given (the
+    // forward pass's copy of it), else to the engine's own mesh.
+    void force(R* keep = nullptr) {
+        phi_ = keep ? keep : phi_own_;
         ACK(cudaMemsetAsync(mesh_, 0, sizeof(R) * cells_, s_));
         k_deposit<R><<<nb(n_), kT, 0, s_>>>(n_, x_[0], x_[1], x_[2], static_cast<R>(cfg_.particle_mass),
                                             axis_, mesh_, status_);
@@ -417,6 +529,13 @@ public:
         k_force<R><<<nb(n_), kT, 0, s_>>>(n_, x_[0], x_[1], x_[2], phi_, axis_, inv_two_dx_, acc_[0],
                                           acc_[1], acc_[2]);
         ++solves_;
+    }
+
+    // acc = F(x) from a potential the forward pass kept for this state.
+    void force_from(R* kept) {
+        phi_ = kept;
+        k_force<R><<<nb(n_), kT, 0, s_>>>(n_, x_[0], x_[1], x_[2], phi_, axis_, inv_two_dx_, acc_[0],
+                                          acc_[1], acc_[2]);
     }
 
     void apply_green(R* in, R* out) {
@@ -510,6 +629,20 @@ public:
             }
             psi = dmalloc<R>(cells_, tmp);
         }
+        // The potential of every forward state (S + 1 meshes) is kept when
+        // device memory allows: the reverse pass then re-derives each state's
+        // force by one gather instead of a deposit and a Green's-function
+        // solve. Particle states stay checkpointed every k steps either way.
+        std::vector<R*> kept;
+        if (want_grad) {
+            size_t free_b = 0, total_b = 0;
+            const size_t need = (S + 1) * cells_ * sizeof(R);
+            if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && need + (size_t(1) << 30) < free_b / 2) {
+                R* block = dmalloc<R>((S + 1) * cells_, tmp);
+                for (uint64_t j = 0; j <= S; ++j) kept.push_back(block + j * cells_);
+            }
+        }
+        auto keep_of = [&](uint64_t j) { return kept.empty() ? nullptr : kept[j]; };
         double* d_loss = dmalloc<double>(1, tmp);
         double* d_delta = delta_out ? dmalloc<double>(cells_, tmp) : nullptr;
         double* d_target = nullptr;
@@ -521,12 +654,12 @@ public:
         // Timed: the KDK forward from the 1LPT state, the loss, and the reverse
         // KDK pass (the 1LPT map and its adjoint, one FFT set each, are setup).
         cudaEventRecord(e0, s_);
-        force();
+        force(keep_of(0));
         save(0);
         for (uint64_t j = 0; j < S; ++j) {
             kick(cfg_.K1[j]);
             drift(cfg_.D[j]);
-            force();
+            force(keep_of(j + 1));
             kick(cfg_.K2[j]);
             if ((j + 1) % k == 0 && j + 1 < S) save((j + 1) / k);
         }
@@ -555,16 +688,23 @@ public:
             for (uint64_t jj = S; jj-- > 0;) {
                 const double coef = cfg_.K2[jj] + (jj + 1 < S ? cfg_.K1[jj + 1] : 0.0);
                 vjp(coef, lx, lp, v, u, psi);  // at x_{jj+1} with phi_{jj+1}
-                k_axpy3<<<nb(n_), kT, 0, s_>>>(n_, cfg_.D[jj], lx[0], lx[1], lx[2], lp[0], lp[1], lp[2]);
-                // reconstruct state jj
-                kick(-cfg_.K2[jj]);  // p' = p_{jj+1} - K2 a_{jj+1}
+                // lp += D lx; reconstruct state jj: p' = p_{jj+1} - K2 a_{jj+1}
+                k_axpy3_kick<R><<<nb(n_), kT, 0, s_>>>(n_, cfg_.D[jj], lx[0], lx[1], lx[2], lp[0],
+                                                       lp[1], lp[2], p_[0], p_[1], p_[2], acc_[0],
+                                                       acc_[1], acc_[2], static_cast<R>(-cfg_.K2[jj]));
                 if (jj % k == 0) {
                     restore(jj / k);
-                    force();
-                } else {
+                    if (kept.empty()) force(); else force_from(kept[jj]);
+                } else if (kept.empty()) {
                     drift(-cfg_.D[jj]);
                     force();
                     kick(-cfg_.K1[jj]);
+                } else {
+                    phi_ = kept[jj];
+                    k_unstep<R><<<nb(n_), kT, 0, s_>>>(n_, x_[0], x_[1], x_[2], p_[0], p_[1], p_[2],
+                                                       -cfg_.D[jj], cfg_.box_size, phi_, axis_,
+                                                       inv_two_dx_, static_cast<R>(-cfg_.K1[jj]),
+                                                       acc_[0], acc_[1], acc_[2]);
                 }
             }
             vjp(cfg_.K1[0], lx, lp, v, u, psi);  // at x_0
@@ -612,6 +752,7 @@ private:
     cufftHandle r2c_ = 0, c2r_ = 0;
     bool plans_ = false;
     R* mesh_ = nullptr;
+    R* phi_own_ = nullptr;
     R* phi_ = nullptr;
     C* modes_ = nullptr;
     unsigned int* status_ = nullptr;

@@ -9,7 +9,10 @@
  * -> CIC density contrast delta = M / Mbar - 1 on the same mesh ->
  * L = 1/2 sum_cells (delta - target)^2.
  * Reverse pass: reverse leapfrog (the KDK step run backwards reconstructs the
- * trajectory) with position / momentum checkpoints every ckpt_every steps,
+ * trajectory) with position / momentum checkpoints every ckpt_every steps;
+ * when device memory allows, the forward pass also keeps the potential mesh
+ * of every state (n_steps + 1 meshes), so the reverse pass re-derives each
+ * state's force by a gather instead of a deposit and a Green's-function solve;
  * hand-written adjoints of the gather (CIC scatter of the force cotangent),
  * of the deposit (gather with the CIC weight derivative), of the centred
  * gradient (centred divergence), of the Green's function (self-adjoint) and of

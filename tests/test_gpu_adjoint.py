@@ -116,4 +116,5 @@ def test_adjoint_cost_ratio_c4():
     ratio = (t["forward_ms"] + t["reverse_ms"]) / t["forward_ms"]
     print(f"c4 (forward + adjoint) / forward = {ratio:.2f} "
           f"(forward {t['forward_ms']:.1f} ms, reverse {t['reverse_ms']:.1f} ms)")
-    assert ratio <= 4.0
+    # target <= 3 (measured 2.83 on B200); the bound leaves room for timing noise
+    assert ratio <= 3.15
