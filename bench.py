@@ -111,6 +111,25 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def replica_seed(base_seed: int, rank: int) -> int:
+    """Noise seed of replica `rank`: each GPU evolves its own realisation."""
+    return base_seed + rank
+
+
+def max_over_ranks(value: float, device: str = "cuda") -> float:
+    """The slowest rank's device time (all ranks call it; one all-reduce)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, n_per_rank: int, steps: int, max_ms: float) -> float:
+    """Particle-steps/s of all replicas over the slowest rank's time."""
+    return world * n_per_rank * steps / (max_ms * 1e-3)
+
+
 def setup_dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -272,7 +291,7 @@ def main():
         reps = math.ceil(total_steps / K1.size)
         K1, D, K2 = np.tile(K1, reps), np.tile(D, reps), np.tile(K2, reps)
     m_p = ic.particle_mass(L, n_side)
-    noise = ic.white_noise(n_side, c["seed"] + rank)
+    noise = ic.white_noise(n_side, replica_seed(c["seed"], rank))
 
     def measure(form):
         """Device-resident K-step throughput of one arithmetic form."""
@@ -293,16 +312,12 @@ def main():
         timing = solver.last_timing()
         dev_ms = timing["total"]
         if world > 1:
-            import torch
-            import torch.distributed as dist
-            t = torch.tensor([dev_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dev_ms = float(t.item())
+            dev_ms = max_over_ranks(dev_ms)
         return solver, ics, timing, dev_ms, wall, clocks.summary()
 
     solver, ics, timing, dev_ms, wall, clock_summary = measure(args.form)
     ms_per_step = dev_ms / args.steps
-    value = world * n * args.steps / (dev_ms * 1e-3)
+    value = whole_job_rate(world, n, args.steps, dev_ms)
     solves = max(1.0, timing["solves"])
     phases = {k: timing[k] / solves for k in ("sort", "deposit", "fft_forward", "green",
                                               "fft_inverse", "gather")}
@@ -354,9 +369,12 @@ def main():
             e2e_solver.kdk_step(K1[s], D[s], K2[s])
         e2e_solver.download(out=result)
         e2e_secs = time.perf_counter() - t0
+        if world > 1:
+            e2e_secs = max_over_ranks(e2e_secs * 1e3) * 1e-3
         h2d = 6 * 8 * n + 24 * args.steps
         d2h = 6 * 8 * n + 8 * args.steps
-        e2e = {"value": world * n * args.steps / e2e_secs, "unit": "particle-steps/s",
+        e2e = {"value": whole_job_rate(world, n, args.steps, e2e_secs * 1e3),
+               "unit": "particle-steps/s",
                "h2d_bytes_per_step": h2d / args.steps,
                "d2h_bytes_per_step": d2h / args.steps,
                "note": "pinned host buffers: upload of the IC positions and momenta, K "
@@ -369,7 +387,7 @@ def main():
         other = "fp64" if args.form == "fp32" else "fp32"
         s2, _, t2, dev2, _, _ = measure(other)
         s2.close()
-        v2 = world * n * args.steps / (dev2 * 1e-3)
+        v2 = whole_job_rate(world, n, args.steps, dev2)
         compare = {"form": other, "value": v2, "ms_per_step": dev2 / args.steps,
                    "ratio_fp32_over_fp64": (value / v2) if args.form == "fp32" else (v2 / value)}
 
