@@ -612,6 +612,8 @@ struct State {
     float2* modes = nullptr;
     size_t modes_elems = 0;   // 8-byte slots of `modes` (host staging between solves)
     unsigned int* d_flag = nullptr;  // input validation flag of upload
+    cudaStream_t copy_stream = nullptr;  // download: device->host copies beside the kernels
+    cudaEvent_t staged[2] = {}, copied[2] = {};
     float2* phi_k = nullptr;
     float* lap = nullptr;
     float* win = nullptr;
@@ -743,6 +745,11 @@ int create(State** out, double L, int N, int method, int deconvolve, double r_s,
     CK(dalloc(&st->modes, modes_n));
     st->modes_elems = modes_n;
     CK(dalloc(&st->d_flag, 1));
+    CK(cudaStreamCreateWithFlags(&st->copy_stream, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+        CK(cudaEventCreateWithFlags(&st->staged[b], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&st->copied[b], cudaEventDisableTiming));
+    }
     if (method == HYOWON_TREEPM_LONG_RANGE) CK(dalloc(&st->phi_k, half));
     CK(dalloc(&st->lap, N));
     CK(dalloc(&st->win, N));
@@ -806,6 +813,11 @@ void destroy(State* st) {
     cudaFree(st->d_plan);
     cudaFree(st->d_qsum);
     cudaFree(st->d_flag);
+    for (int b = 0; b < 2; ++b) {
+        if (st->staged[b]) cudaEventDestroy(st->staged[b]);
+        if (st->copied[b]) cudaEventDestroy(st->copied[b]);
+    }
+    if (st->copy_stream) cudaStreamDestroy(st->copy_stream);
     free_particles(st);
     cudaFree(st->sort.count);
     cudaFree(st->sort.offset);
@@ -1121,37 +1133,56 @@ int download(State* st, cudaStream_t s, double* x, double* y, double* z, double*
              double* pz, double* ax, double* ay, double* az) {
     const uint32_t n = st->n;
     // Widened components are scattered back to the original particle order in
-    // a staging array of n doubles: the half-spectrum buffer when it is large
-    // enough (it holds nothing live between force solves; the potential mesh
-    // is left intact), else a temporary allocation.
-    double* stage = nullptr;
+    // staging arrays of n doubles: two in the half-spectrum buffer when it
+    // holds 2n slots (it holds nothing live between force solves; the
+    // potential mesh is left intact), so that the scatter of one component on
+    // the handle's stream overlaps the device-to-host copy of the previous one
+    // on the copy stream; else one (in the buffer, or a temporary allocation).
+    double* stage[2] = {};
+    int nstage = 1;
     bool owned = false;
-    if (st->modes_elems >= n) {
-        stage = reinterpret_cast<double*>(st->modes);
+    if (st->modes_elems >= 2ull * n) {
+        stage[0] = reinterpret_cast<double*>(st->modes);
+        stage[1] = stage[0] + n;
+        nstage = 2;
+    } else if (st->modes_elems >= n) {
+        stage[0] = reinterpret_cast<double*>(st->modes);
     } else {
-        CK(dalloc(&stage, n));
+        CK(dalloc(&stage[0], n));
         owned = true;
     }
     double* outs[9] = {x, y, z, px, py, pz, ax, ay, az};
     const double pos_scale = st->L / kTwo32;
     int rc = HYOWON_OK;
+    int j = 0;
     for (int a = 0; a < 9 && rc == HYOWON_OK; ++a) {
         if (!outs[a]) continue;
+        const int b = j % nstage;
+        if (j >= nstage && cudaStreamWaitEvent(s, st->copied[b], 0) != cudaSuccess) {
+            rc = fail(st, HYOWON_ECUDA, "download: stream wait failed");
+            break;
+        }
         ++st->launches;
         if (a < 3)
             k_unpermute_widen<uint32_t><<<blocks_for(n), kThreads, 0, s>>>(n, st->id[st->ic],
-                                                                         st->pos[st->pc][a], pos_scale, stage);
+                                                                         st->pos[st->pc][a], pos_scale, stage[b]);
         else if (a < 6)
             k_unpermute_widen<float><<<blocks_for(n), kThreads, 0, s>>>(n, st->id[st->ic],
-                                                                      st->mom[st->mc][a - 3], 1.0, stage);
+                                                                      st->mom[st->mc][a - 3], 1.0, stage[b]);
         else
             k_unpermute_widen<float><<<blocks_for(n), kThreads, 0, s>>>(n, st->id[st->ic],
-                                                                      st->acc[a - 6], 1.0, stage);
-        if (cudaMemcpyAsync(outs[a], stage, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess
-            || cudaStreamSynchronize(s) != cudaSuccess)
+                                                                      st->acc[a - 6], 1.0, stage[b]);
+        if (cudaEventRecord(st->staged[b], s) != cudaSuccess
+            || cudaStreamWaitEvent(st->copy_stream, st->staged[b], 0) != cudaSuccess
+            || cudaMemcpyAsync(outs[a], stage[b], sizeof(double) * n, cudaMemcpyDeviceToHost,
+                               st->copy_stream) != cudaSuccess
+            || cudaEventRecord(st->copied[b], st->copy_stream) != cudaSuccess)
             rc = fail(st, HYOWON_ECUDA, "download copy failed");
+        ++j;
     }
-    if (owned) cudaFree(stage);
+    if (cudaStreamSynchronize(st->copy_stream) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+        rc = rc ? rc : fail(st, HYOWON_ECUDA, "download copy failed");
+    if (owned) cudaFree(stage[0]);
     return rc;
 }
 

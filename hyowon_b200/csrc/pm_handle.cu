@@ -65,6 +65,8 @@ struct hyowon_pm_s {
     double field_scale = 0.0;  // (1/dx^3) * (1/N^3)
 
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // download: device->host copies beside the kernels
+    cudaEvent_t staged[2] = {}, copied[2] = {};
     cufftHandle plan_r2c = 0;
     cufftHandle plan_c2r = 0;
     bool plans = false;
@@ -600,8 +602,14 @@ int hyowon_pm_create(double box_size, uint64_t mesh_size, int method, int deconv
         hyowon_pm_destroy(h);
         return code;
     };
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess
+        || cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(HYOWON_ECUDA);
+    for (int b = 0; b < 2; ++b) {
+        if (cudaEventCreateWithFlags(&h->staged[b], cudaEventDisableTiming) != cudaSuccess
+            || cudaEventCreateWithFlags(&h->copied[b], cudaEventDisableTiming) != cudaSuccess)
+            return bail(HYOWON_ECUDA);
+    }
     if (cudaMallocHost(reinterpret_cast<void**>(&h->h_status), sizeof(unsigned int)) != cudaSuccess
         || cudaMallocHost(reinterpret_cast<void**>(&h->h_maxdrift), sizeof(unsigned long long)) != cudaSuccess
         || dalloc(&h->d_status, 1) != cudaSuccess || dalloc(&h->d_maxdrift, 1) != cudaSuccess
@@ -726,6 +734,11 @@ int hyowon_pm_destroy(hyowon_pm_t h) {
     for (auto& e : h->call_ev) {
         if (e) cudaEventDestroy(e);
     }
+    for (int b = 0; b < 2; ++b) {
+        if (h->staged[b]) cudaEventDestroy(h->staged[b]);
+        if (h->copied[b]) cudaEventDestroy(h->copied[b]);
+    }
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return HYOWON_OK;
@@ -904,19 +917,31 @@ int hyowon_pm_download(hyowon_pm_t h, double* x, double* y, double* z, double* p
         return status_or_cuda(h, rc);
     }
     const uint32_t n = h->n;
-    // The spare position buffer is dead between calls: use it as staging.
-    double* stage = h->pos[1 - h->pc][0];
+    // The spare position buffers are dead between calls: two of them stage
+    // the reordered components, so that the reorder of one component on the
+    // handle's stream overlaps the device-to-host copy of the previous one on
+    // the copy stream.
+    double* stage[2] = {h->pos[1 - h->pc][0], h->pos[1 - h->pc][1]};
     double* outs[9] = {x, y, z, px, py, pz, ax, ay, az};
     const double* srcs[9] = {h->pos[h->pc][0], h->pos[h->pc][1], h->pos[h->pc][2],
                              h->mom[h->mc][0], h->mom[h->mc][1], h->mom[h->mc][2],
                              h->acc[0], h->acc[1], h->acc[2]};
+    int j = 0;
     for (int a = 0; a < 9; ++a) {
         if (!outs[a]) continue;
+        const int b = j & 1;
+        if (j >= 2) CK(cudaStreamWaitEvent(h->stream, h->copied[b], 0));
         ++h->launches;
-        launch_unpermute_f64(n, h->id[h->ic], srcs[a], stage, h->stream);
-        CK(cudaMemcpyAsync(outs[a], stage, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
+        launch_unpermute_f64(n, h->id[h->ic], srcs[a], stage[b], h->stream);
+        CK(cudaEventRecord(h->staged[b], h->stream));
+        CK(cudaStreamWaitEvent(h->copy_stream, h->staged[b], 0));
+        CK(cudaMemcpyAsync(outs[a], stage[b], sizeof(double) * n, cudaMemcpyDeviceToHost,
+                           h->copy_stream));
+        CK(cudaEventRecord(h->copied[b], h->copy_stream));
+        ++j;
     }
+    CK(cudaStreamSynchronize(h->copy_stream));
+    CK(cudaStreamSynchronize(h->stream));
     return HYOWON_OK;
 }
 
