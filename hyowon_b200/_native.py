@@ -68,6 +68,15 @@ class PkBin(ctypes.Structure):
                 ("shot_noise_reference", c_double), ("mode_count", c_u64)]
 
 
+class ICParams(ctypes.Structure):
+    """hyowon_ic_params_t (include/hyowon_ic.h)."""
+    _fields_ = [("particles_per_dimension", c_u64), ("mesh_per_dimension", c_u64),
+                ("box_size", c_double), ("seed", c_u64), ("max_mode_per_axis", ctypes.c_int64),
+                ("amplitude_mode", c_int), ("phase_pairing", c_int), ("lpt_order", c_int),
+                ("momentum_factor_1", c_double), ("position_factor_2", c_double),
+                ("momentum_factor_2", c_double)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "hyowon_pm_create": (c_int, [c_double, c_u64, c_int, c_int, c_double, c_int,
@@ -111,6 +120,14 @@ _SIGS = {
     "hyowon_schedule": (c_int, [c_double, c_double, c_double, c_double, c_double, c_u64,
                                 P_double, P_u64]),
     "hyowon_growth": (c_int, [c_double, c_double, c_u64, P_double, P_double, P_double]),
+    "hyowon_growth2": (c_int, [c_double, c_double, c_u64] + [P_double] * 5),
+    "hyowon_ic_resolve": (c_int, [ctypes.POINTER(ICParams), P_u64, P_u64]),
+    "hyowon_ic_mode_amplitudes": (c_int, [c_u64, c_double, c_u64, P_double, P_double]),
+    "hyowon_ic_field": (c_int, [ctypes.POINTER(ICParams), c_u64, P_double, P_double]),
+    "hyowon_ic_generate": (c_int, [ctypes.POINTER(ICParams), c_u64, P_double] + [P_double] * 6),
+    "hyowon_pm_generate_ics": (c_int, [c_void_p, ctypes.POINTER(ICParams), c_u64, P_double,
+                                       c_double]),
+    "hyowon_ic_last_error": (ctypes.c_char_p, []),
 }
 
 

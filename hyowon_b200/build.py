@@ -39,6 +39,7 @@ UNITS = [
     ("pm_noalloc.cu", ["--fmad=false"]),
     ("pm_diag.cu", ["--fmad=false"]),
     ("pm_pk.cu", ["--fmad=false"]),
+    ("pm_ic.cu", ["--fmad=false"]),
     ("cosmology.cpp", []),
 ]
 

@@ -355,4 +355,85 @@ int hyowon_growth(double om, double ol, uint64_t n, const double* a, double* D1,
     return kOk;
 }
 
+// Second-order growth (include/cosmo_nbody/cosmology/cosmology_model.hpp:50-53,
+// src/cosmology/cosmology_model.cpp:194-320): y = [D1, dD1/dx, D2, dD2/dx] in
+// x = ln a obeys y0' = y1, y1' = -(2 - 3/2 Om(a)) y1 + 3/2 Om(a) y0,
+// y2' = y3, y3' = -(2 - 3/2 Om(a)) y3 + 3/2 Om(a) (y2 - y0^2), started in the
+// matter era at a_s = (eps Om / OL)^(1/3) from the EdS growing modes
+// (a, a, -3/7 a^2, -6/7 a^2) and integrated by classical RK4 with steps
+// <= eps^(1/5) / 2 in ln a (the reference's balanced step, refined once).
+// Normalised by D1(1) and D1(1)^2; f2 = y3 / y2. D1 and f1 come from
+// hyowon_growth's integral solution.
+int hyowon_growth2(double om, double ol, uint64_t n, const double* a, double* D1, double* f1,
+                   double* D2, double* f2) {
+    if (!valid_cosmology(om, ol) || (n && (!a || !D1 || !f1 || !D2 || !f2))) return kInvalid;
+    for (uint64_t i = 0; i < n; ++i)
+        if (!std::isfinite(a[i]) || a[i] <= 0.0 || a[i] > 1.0) return kInvalid;
+    if (int rc = hyowon_growth(om, ol, n, a, D1, f1)) return rc;
+    if (ol == 0.0) {
+        for (uint64_t i = 0; i < n; ++i) {
+            D2[i] = -3.0 / 7.0 * a[i] * a[i];
+            f2[i] = 2.0;
+        }
+        return kOk;
+    }
+    const double eps = std::numeric_limits<double>::epsilon();
+    const double a_s = std::fmin(std::cbrt(eps * om / ol), 1.0);
+    const double x0 = std::log(a_s);
+    const double h_max = 0.5 * std::pow(eps, 0.2);
+    auto om_a = [&](double x) {
+        const double a3 = std::exp(3.0 * x);
+        return om / (om + ol * a3);
+    };
+    auto rhs = [&](double x, const double* y, double* d) {
+        const double m = om_a(x);
+        const double drag = 2.0 - 1.5 * m;
+        d[0] = y[1];
+        d[1] = -drag * y[1] + 1.5 * m * y[0];
+        d[2] = y[3];
+        d[3] = -drag * y[3] + 1.5 * m * y[2] - 1.5 * m * y[0] * y[0];
+    };
+    // state at ln a = x1
+    auto integrate = [&](double x1, double* y) {
+        y[0] = a_s;
+        y[1] = a_s;
+        y[2] = -(3.0 / 7.0) * a_s * a_s;
+        y[3] = -(6.0 / 7.0) * a_s * a_s;
+        if (!(x1 > x0)) return;
+        const uint64_t steps = static_cast<uint64_t>(std::ceil((x1 - x0) / h_max));
+        const double h = (x1 - x0) / static_cast<double>(steps);
+        double k1[4], k2[4], k3[4], k4[4], t[4];
+        for (uint64_t s = 0; s < steps; ++s) {
+            const double x = x0 + static_cast<double>(s) * h;
+            rhs(x, y, k1);
+            for (int j = 0; j < 4; ++j) t[j] = y[j] + 0.5 * h * k1[j];
+            rhs(x + 0.5 * h, t, k2);
+            for (int j = 0; j < 4; ++j) t[j] = y[j] + 0.5 * h * k2[j];
+            rhs(x + 0.5 * h, t, k3);
+            for (int j = 0; j < 4; ++j) t[j] = y[j] + h * k3[j];
+            rhs(x + h, t, k4);
+            for (int j = 0; j < 4; ++j) y[j] += (h / 6.0) * (k1[j] + 2.0 * k2[j] + 2.0 * k3[j] + k4[j]);
+        }
+    };
+    double y1[4];
+    integrate(0.0, y1);
+    const double d1_today = y1[0];
+    if (!std::isfinite(d1_today) || d1_today <= 0.0) return kOverflow;
+    for (uint64_t i = 0; i < n; ++i) {
+        double y[4];
+        const double x = std::log(a[i]);
+        if (x <= x0) {
+            const double r = a[i] / a_s;
+            D2[i] = -(3.0 / 7.0) * a_s * a_s * r * r / (d1_today * d1_today);
+            f2[i] = 2.0;
+            continue;
+        }
+        integrate(x, y);
+        D2[i] = y[2] / (d1_today * d1_today);
+        f2[i] = y[3] / y[2];
+        if (!std::isfinite(D2[i]) || !std::isfinite(f2[i]) || D2[i] >= 0.0) return kOverflow;
+    }
+    return kOk;
+}
+
 }  // extern "C"

@@ -27,6 +27,7 @@
 #include "pm_fp32.h"
 #include "pm_poisson.h"
 #include "pm_kernels.h"
+#include "pm_ic.h"
 #include "pm_lpt.h"
 #include "pm_pk.h"
 
@@ -902,6 +903,75 @@ int hyowon_pm_lpt_ics(hyowon_pm_t h, uint64_t n_side, const double* noise, uint6
     }
     cudaFree(d_noise);
     cudaFree(tab);
+    if (rc == HYOWON_OK) h->has_state = true;
+    return rc;
+}
+
+int hyowon_pm_generate_ics(hyowon_pm_t h, const hyowon_ic_params_t* p, uint64_t n_power,
+                           const double* power, double uniform_mass) {
+    if (!h) return HYOWON_EINVAL;
+    hyowon::ic::Params r;
+    const char* err = nullptr;
+    int rc = hyowon::ic::resolve(p, &r, &err);
+    if (rc) return fail(h, rc, err);
+    if (!std::isfinite(uniform_mass) || uniform_mass <= 0.0)
+        return fail(h, HYOWON_EINVAL, "uniform mass must be finite and positive");
+    const uint64_t n64 = static_cast<uint64_t>(r.N) * r.N * r.N;
+    if (n64 > 0xFFFFFFF0ull) return fail(h, HYOWON_EINVAL, "particle count exceeds 2^32-16");
+    const uint32_t n = static_cast<uint32_t>(n64);
+    double2* d_amp = nullptr;
+    if ((rc = hyowon::ic::upload_amplitudes(r, n_power, power, &d_amp, &err))) return fail(h, rc, err);
+    h->has_state = h->acc_valid = h->sorted = false;
+    double* tmp_pos[3] = {};
+    double* tmp_mom[3] = {};
+    if (h->precision == HYOWON_FP64) {
+        rc = ensure_capacity(h, n, false);
+        if (rc == HYOWON_OK) rc = ensure_sort_buckets(h, n);
+        for (int a = 0; a < 3; ++a) {
+            tmp_pos[a] = h->pos[0][a];
+            tmp_mom[a] = h->mom[0][a];
+        }
+    } else {
+        for (int a = 0; a < 3 && rc == HYOWON_OK; ++a) {
+            if (dalloc(&tmp_pos[a], n) != cudaSuccess || dalloc(&tmp_mom[a], n) != cudaSuccess)
+                rc = fail(h, HYOWON_ENOMEM, "IC staging allocation failed");
+        }
+    }
+    if (rc == HYOWON_OK) {
+        cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream);
+        const int grc = hyowon::ic::generate_device(r, d_amp, tmp_pos, tmp_mom, h->d_status,
+                                                    h->stream, &err);
+        if (grc) rc = fail(h, grc, err);
+    }
+    unsigned int st = 0;
+    if (rc == HYOWON_OK) rc = read_status(h, &st);
+    if (rc == HYOWON_OK && st) {
+        const int src = hyowon::ic::status_code(st, &err);
+        cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream);
+        rc = fail(h, src, err);
+    }
+    h->n = n;
+    h->uniform_mass = uniform_mass;
+    h->has_masses = false;
+    set_input_mass(h, uniform_mass * static_cast<double>(n), n);
+    if (rc == HYOWON_OK) {
+        if (h->precision == HYOWON_FP64) {
+            h->pc = h->mc = h->ic = 0;
+            ++h->launches;
+            launch_iota_u32(n, h->id[0], h->stream);
+            if (cudaStreamSynchronize(h->stream) != cudaSuccess) rc = fail(h, HYOWON_ECUDA, "iota failed");
+        } else {
+            rc = status_or_cuda(h, fp32::upload_device(h->f32, n, tmp_pos, tmp_mom, uniform_mass,
+                                                       h->input_mass, h->mass_tol, h->stream));
+        }
+    }
+    if (h->precision != HYOWON_FP64) {
+        for (int a = 0; a < 3; ++a) {
+            cudaFree(tmp_pos[a]);
+            cudaFree(tmp_mom[a]);
+        }
+    }
+    cudaFree(d_amp);
     if (rc == HYOWON_OK) h->has_state = true;
     return rc;
 }

@@ -1,0 +1,684 @@
+// pm_ic.cu -- HYOWON's generated initial conditions on the device.
+//
+// Field (RandomField::generate, src/ic/random_field.cpp:70-330): one thread
+// per half-spectrum mode. The mode's integer numbers (mx, my, mz) outside the
+// Cartesian support |m_i| <= K (or m = 0) give 0. On the kz = 0 and Nyquist
+// planes the half spectrum stores each conjugate pair once: the member whose
+// conjugate index (M-i, M-j) is smaller (i first, then j) is drawn with the
+// conjugate's counter and its imaginary part negated; self-conjugate modes are
+// real. The draw is Philox4x32-10 (src/ic/philox_rng.cpp:43-62) on the
+// counter (mx, my, mz, stream) and key (seed low, seed high), mapped to two
+// 53-bit open uniforms and a Box-Muller pair (:27-36,85-96). The amplitudes
+// sqrt(var_s), sqrt(var_s/2) of s = |m|^2 come from a host table formed as
+// the reference forms them, so the only difference from the reference's field
+// is the device log / sin / cos of Box-Muller (a few ulp).
+//
+// LPT (LPTDisplacement::apply_to_arrays, src/ic/lpt_displacement.cpp:150-520):
+// per axis a, psi_k = (-Im d, Re d) k_a/k^2 (k_a = 0 on axis a's Nyquist
+// plane), cuFFT Z2D, times 1/M^3, sampled at node (i, j, k) M/N and applied
+// as x = wrap(x + x_f psi), p = p + p_f psi. 2LPT: the seven fields
+// H_xx, H_yy, H_zz, H_xy, H_xz, H_yz (k_a k_b / k^2, mixed terms 0 on either
+// Nyquist plane) and tr H (d with k = 0 removed) are transformed one at a time
+// and folded into the source S = -1/2 H_aa^2 ... - H_ab^2 ... + 1/2 (tr H)^2 in
+// the reference's order; D2Z of S, the Cartesian band limit
+// (src/ic/particle_lattice_bandlimit.cpp:42-80) fused into
+// psi2_k = (Im S, -Re S) k_a/k^2. Wavenumbers are (2 pi m)/L
+// (include/cosmo_nbody/mesh/mesh_geometry.hpp:112-115).
+//
+// Compiled with --fmad=false: every product and sum is rounded as the
+// reference's -ffp-contract=off build rounds it, so the spectral multipliers,
+// the source and the particle update are the reference's expressions; only the
+// FFT's rounding differs.
+//
+// HBM traffic per mode / cell is a few words in each kernel; the O(M^3 log M)
+// transforms (cuFFT, FP64) dominate: 1LPT = 3 Z2D, 2LPT = 3 + 7 + 3 Z2D + 1
+// D2Z on the IC mesh.
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <cufft.h>
+
+#include "pm_common.cuh"
+#include "pm_ic.h"
+
+namespace hyowon {
+namespace ic {
+
+namespace {
+
+constexpr double kTwoPi = 6.283185307179586;  // 2.0 * std::numbers::pi, exact doubling
+
+// ---------------------------------------------------------------- Philox ----
+
+struct Draw {
+    double u1, u2;
+};
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+    constexpr uint32_t kM0 = 0xD2511F53u, kM1 = 0xCD9E8D57u;
+    constexpr uint32_t kW0 = 0x9E3779B9u, kW1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(kM0, c.x), lo0 = kM0 * c.x;
+        const uint32_t hi1 = __umulhi(kM1, c.z), lo1 = kM1 * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        if (r != 9) {
+            k0 += kW0;
+            k1 += kW1;
+        }
+    }
+    return c;
+}
+
+__device__ __forceinline__ double open_uniform(uint32_t hi, uint32_t lo) {
+    const uint64_t bits = (static_cast<uint64_t>(hi) << 21) | (static_cast<uint64_t>(lo) >> 11);
+    if (bits == 0) return 0x1.0p-54;
+    return static_cast<double>(bits) * 0x1.0p-53;
+}
+
+__device__ __forceinline__ Draw mode_uniforms(uint64_t seed, int32_t mx, int32_t my, int32_t mz,
+                                              uint32_t stream) {
+    const uint4 w = philox4x32_10(
+        make_uint4(static_cast<uint32_t>(mx), static_cast<uint32_t>(my),
+                   static_cast<uint32_t>(mz), stream),
+        static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
+    return {open_uniform(w.x, w.y), open_uniform(w.z, w.w)};
+}
+
+__device__ __forceinline__ int mode_number(int i, int n) { return i <= n / 2 ? i : i - n; }
+
+__device__ __forceinline__ void half_index(uint64_t idx, int M, int& ix, int& iy, int& iz) {
+    const int hz = M / 2 + 1;
+    iz = static_cast<int>(idx % hz);
+    const uint64_t t = idx / hz;
+    iy = static_cast<int>(t % M);
+    ix = static_cast<int>(t / M);
+}
+
+// ----------------------------------------------------------------- field ----
+
+__global__ void k_field(int M, int K, uint64_t seed, int fixed, int negate,
+                        const double2* __restrict__ amp, double2* __restrict__ out,
+                        unsigned int* status) {
+    const uint64_t total = static_cast<uint64_t>(M) * M * (M / 2 + 1);
+    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    int i, j, k;
+    half_index(idx, M, i, j, k);
+    const int mx = mode_number(i, M), my = mode_number(j, M), mz = k;
+    if ((mx == 0 && my == 0 && mz == 0) || abs(mx) > K || abs(my) > K || mz > K) {
+        out[idx] = make_double2(0.0, 0.0);
+        return;
+    }
+    bool conjugate = false, self_conjugate = false;
+    int ci = i, cj = j;
+    if (k == 0 || ((M & 1) == 0 && k == M / 2)) {
+        const int ti = (M - i) % M, tj = (M - j) % M;
+        self_conjugate = ti == i && tj == j;
+        if (!self_conjugate && (ti < i || (ti == i && tj < j))) {
+            ci = ti;
+            cj = tj;
+            conjugate = true;
+        }
+    }
+    const int64_t s = static_cast<int64_t>(mx) * mx + static_cast<int64_t>(my) * my +
+                      static_cast<int64_t>(mz) * mz;
+    const double2 a = amp[s];
+    if (!(a.x > 0.0) || !(a.y > 0.0) || !isfinite(a.x) || !isfinite(a.y)) {
+        raise_status(status, IC_AMPLITUDE);
+        out[idx] = make_double2(0.0, 0.0);
+        return;
+    }
+    const Draw d = mode_uniforms(seed, mode_number(ci, M), mode_number(cj, M), mz, fixed ? 1u : 0u);
+    double re, im;
+    if (fixed) {
+        if (self_conjugate) {
+            re = d.u1 < 0.5 ? -a.x : a.x;
+            im = 0.0;
+        } else {
+            double sn, cs;
+            sincos(kTwoPi * d.u1, &sn, &cs);
+            im = a.x * sn;
+            if (conjugate) im = -im;
+            re = a.x * cs;
+        }
+    } else {
+        const double radius = sqrt(-2.0 * log(d.u1));
+        double sn, cs;
+        sincos(kTwoPi * d.u2, &sn, &cs);
+        const double n1 = radius * cs, n2 = radius * sn;
+        if (self_conjugate) {
+            re = a.x * n1;
+            im = 0.0;
+        } else {
+            re = a.y * n1;
+            im = a.y * n2;
+            if (conjugate) im = -im;
+        }
+    }
+    if (negate) {
+        re = -re;
+        im = -im;
+    }
+    out[idx] = make_double2(re, im);
+}
+
+// ------------------------------------------------------- spectral stages ----
+
+enum Stage : int { kPsi1 = 0, kHessian = 1, kTrace = 2, kPsi2 = 3 };
+
+// dst from src for one stage. Psi1 / Psi2: axis a; Hessian: axes (a, b);
+// Psi2 also applies the band limit |m_i| <= K to the source.
+__global__ void k_spectral(int M, double L, int stage, int a, int b, int K,
+                           const double2* __restrict__ src, double2* __restrict__ dst) {
+    const uint64_t total = static_cast<uint64_t>(M) * M * (M / 2 + 1);
+    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    int i, j, k;
+    half_index(idx, M, i, j, k);
+    const int m[3] = {mode_number(i, M), mode_number(j, M), mode_number(k, M)};
+    const bool even = (M & 1) == 0;
+    const bool nyq[3] = {even && i == M / 2, even && j == M / 2, even && k == M / 2};
+    double kc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) kc[d] = kTwoPi * static_cast<double>(m[d]) / L;
+    const double k2 = kc[0] * kc[0] + kc[1] * kc[1] + kc[2] * kc[2];
+    if (stage == kTrace) {
+        dst[idx] = idx == 0 ? make_double2(0.0, 0.0) : src[idx];
+        return;
+    }
+    if (k2 == 0.0) {
+        dst[idx] = make_double2(0.0, 0.0);
+        return;
+    }
+    double2 v = src[idx];
+    if (stage == kHessian) {
+        const double num = (a != b && (nyq[a] || nyq[b])) ? 0.0 : kc[a] * kc[b];
+        const double q = num / k2;
+        dst[idx] = make_double2(v.x * q, v.y * q);
+        return;
+    }
+    if (stage == kPsi2 && (abs(m[0]) > K || abs(m[1]) > K || abs(m[2]) > K)) v = make_double2(0.0, 0.0);
+    const double kd = nyq[a] ? 0.0 : kc[a];
+    const double f = kd / k2;
+    dst[idx] = stage == kPsi1 ? make_double2(-v.y * f, v.x * f) : make_double2(v.y * f, -v.x * f);
+}
+
+// ------------------------------------------------------------ real stages ----
+
+// Corner lattice (src/ic/initial_conditions.cpp:295-313).
+__global__ void k_lattice(int N, double dx, double* __restrict__ x, double* __restrict__ y,
+                          double* __restrict__ z, double* __restrict__ px,
+                          double* __restrict__ py, double* __restrict__ pz) {
+    const uint64_t total = static_cast<uint64_t>(N) * N * N;
+    const uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= total) return;
+    const int k = static_cast<int>(p % N);
+    const int j = static_cast<int>((p / N) % N);
+    const int i = static_cast<int>(p / (static_cast<uint64_t>(N) * N));
+    x[p] = static_cast<double>(i) * dx;
+    y[p] = static_cast<double>(j) * dx;
+    z[p] = static_cast<double>(k) * dx;
+    px[p] = 0.0;
+    py[p] = 0.0;
+    pz[p] = 0.0;
+}
+
+// apply_lpt_component_update (src/ic/lpt_displacement.cpp:101-128) at the
+// lattice node of each particle; a non-finite psi or candidate leaves the
+// particle unchanged and raises `flag`.
+__global__ void k_apply(int N, int M, const double* __restrict__ field, double norm, double xf,
+                        double pf, double L, double* __restrict__ pos, double* __restrict__ mom,
+                        unsigned int flag, unsigned int* status) {
+    const uint64_t total = static_cast<uint64_t>(N) * N * N;
+    const uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= total) return;
+    const uint64_t r = static_cast<uint64_t>(M / N);
+    const uint64_t k = p % N;
+    const uint64_t j = (p / N) % N;
+    const uint64_t i = p / (static_cast<uint64_t>(N) * N);
+    const double psi = field[((i * r) * M + j * r) * M + k * r] * norm;
+    const double disp = xf * psi;
+    const double dmom = pf * psi;
+    const double xc = pos[p] + disp;
+    const double mc = mom[p] + dmom;
+    const double w = wrap_f64(xc, L);
+    if (!isfinite(psi) || !isfinite(disp) || !isfinite(dmom) || !isfinite(xc) || !isfinite(mc) ||
+        !isfinite(w)) {
+        raise_status(status, flag);
+        return;
+    }
+    pos[p] = w;
+    mom[p] = mc;
+}
+
+// Folds one normalised field into the 2LPT source in the reference's order:
+// op 0: S = -(1/2 h h); 1: S -= 1/2 h h; 2: S -= h h; 3: S += 1/2 t t.
+__global__ void k_source(uint64_t n, const double* __restrict__ field, double norm, int op,
+                         double* __restrict__ src, unsigned int* status) {
+    const uint64_t c = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double h = field[c] * norm;
+    if (op < 3 && !isfinite(h)) raise_status(status, IC_HESSIAN);
+    double s;
+    if (op == 0) {
+        const double term = 0.5 * h * h;
+        s = -term;
+    } else if (op == 1) {
+        const double term = 0.5 * h * h;
+        s = src[c] - term;
+    } else if (op == 2) {
+        s = src[c] - h * h;
+    } else {
+        s = src[c] + 0.5 * h * h;
+        if (!isfinite(s)) raise_status(status, IC_SOURCE);
+    }
+    src[c] = s;
+}
+
+inline unsigned grid(uint64_t n) { return static_cast<unsigned>((n + 255) / 256); }
+
+// cuFFT plans on the IC mesh with one shared work area.
+struct Fft {
+    cufftHandle c2r = 0, r2c = 0;
+    bool has_c2r = false, has_r2c = false;
+    void* ws = nullptr;
+    ~Fft() {
+        if (has_c2r) cufftDestroy(c2r);
+        if (has_r2c) cufftDestroy(r2c);
+        cudaFree(ws);
+    }
+    int make(int M, bool forward, cudaStream_t s, const char** err) {
+        size_t w1 = 0, w2 = 0;
+        if (cufftCreate(&c2r) != CUFFT_SUCCESS) return *err = "cufftCreate failed", HYOWON_ECUDA;
+        has_c2r = true;
+        cufftSetAutoAllocation(c2r, 0);
+        if (cufftMakePlan3d(c2r, M, M, M, CUFFT_Z2D, &w1) != CUFFT_SUCCESS)
+            return *err = "cuFFT Z2D plan for the IC mesh failed", HYOWON_ECUDA;
+        if (forward) {
+            if (cufftCreate(&r2c) != CUFFT_SUCCESS) return *err = "cufftCreate failed", HYOWON_ECUDA;
+            has_r2c = true;
+            cufftSetAutoAllocation(r2c, 0);
+            if (cufftMakePlan3d(r2c, M, M, M, CUFFT_D2Z, &w2) != CUFFT_SUCCESS)
+                return *err = "cuFFT D2Z plan for the IC mesh failed", HYOWON_ECUDA;
+        }
+        size_t w = w1 > w2 ? w1 : w2;
+        if (w < 256) w = 256;
+        if (cudaMalloc(&ws, w) != cudaSuccess)
+            return *err = "cuFFT work area for the IC mesh could not be allocated", HYOWON_ENOMEM;
+        cufftSetWorkArea(c2r, ws);
+        cufftSetStream(c2r, s);
+        if (forward) {
+            cufftSetWorkArea(r2c, ws);
+            cufftSetStream(r2c, s);
+        }
+        return HYOWON_OK;
+    }
+};
+
+template <typename T>
+struct DeviceBuffer {
+    T* p = nullptr;
+    ~DeviceBuffer() { cudaFree(p); }
+    bool alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * n) == cudaSuccess; }
+};
+
+// ------------------------------------------------- scaled positive product --
+
+// Binary mantissa / exponent product in long double, one factor at a time, as
+// math::ScaledPositiveProduct consumes and materialises
+// (include/cosmo_nbody/math/scaled_positive_product.hpp:425-512).
+struct Scaled {
+    long double mant = 1.0L;
+    long long expo = 0;
+    void consume(double factor, bool divide) {
+        int fe = 0;
+        const long double fw = static_cast<long double>(std::frexp(factor, &fe));
+        if (divide) {
+            mant = mant / fw;
+            expo -= fe;
+        } else {
+            mant = mant * fw;
+            expo += fe;
+        }
+        int ne = 0;
+        mant = std::frexp(mant, &ne);
+        expo += ne;
+    }
+    // 0 on success, 1 underflow, 2 overflow.
+    static int materialize(long double m, long long e, double* out) {
+        if (e < INT_MIN || e > INT_MAX) return 2;
+        const long double wide = std::scalbn(m, static_cast<int>(e));
+        if (wide == 0.0L) return 1;
+        if (!std::isfinite(wide) || wide < 0.0L || wide > static_cast<long double>(DBL_MAX)) return 2;
+        const double r = static_cast<double>(wide);
+        if (!std::isfinite(r) || r <= 0.0) return 1;
+        *out = r;
+        return 0;
+    }
+    // sqrt(this * num / den) without materialising the square.
+    int sqrt_of_quotient(double num, double den, double* out) const {
+        Scaled t = *this;
+        t.consume(num, false);
+        t.consume(den, true);
+        long long q = t.expo / 2, rem = t.expo % 2;
+        if (rem < 0) {
+            rem += 2;
+            --q;
+        }
+        const long double root = std::sqrt(std::scalbn(t.mant, static_cast<int>(rem)));
+        if (!std::isfinite(root) || !(root > 0.0L)) return 2;
+        return materialize(root, q, out);
+    }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------ host ----
+
+int resolve(const hyowon_ic_params_t* in, Params* out, const char** err) {
+    if (!in || !out) return *err = "null IC parameters", HYOWON_EINVAL;
+    const uint64_t N = in->particles_per_dimension;
+    if (N == 0) return *err = "particles_per_dimension must be positive", HYOWON_EINVAL;
+    if (N > 1625) return *err = "Configured particle population N^3 exceeds the uint32 count range", HYOWON_EOVERFLOW;
+    if (!std::isfinite(in->box_size) || !(in->box_size > 0.0))
+        return *err = "Box size must be finite and positive", HYOWON_EINVAL;
+    if (in->max_mode_per_axis >= 0 &&
+        (in->max_mode_per_axis == 0 || static_cast<uint64_t>(in->max_mode_per_axis) > (N - 1) / 2))
+        return *err = "ic.max_mode_per_axis must be positive and satisfy 2*K < particles_per_dimension",
+               HYOWON_EINVAL;
+    const uint64_t K = in->max_mode_per_axis >= 0 ? static_cast<uint64_t>(in->max_mode_per_axis)
+                                                  : (N - 1) / 2;
+    if (K == 0)
+        return *err = "Generated IC particle lattice must admit at least one nonzero Fourier mode",
+               HYOWON_EINVAL;
+    if (in->lpt_order != 1 && in->lpt_order != 2)
+        return *err = "ic.lpt_order must be 1 or 2", HYOWON_EINVAL;
+    // projected_2lpt_source_mesh_is_alias_free (particle_lattice_bandlimit.hpp:56-61)
+    auto alias_free = [](uint64_t m, uint64_t k) { return m != 0 && k <= (m - 1) / 3; };
+    uint64_t M = in->mesh_per_dimension;
+    if (M == 0) M = (in->lpt_order == 2 && !alias_free(N, K)) ? 2 * N : N;
+    if (M > static_cast<uint64_t>(INT_MAX))
+        return *err = "IC mesh dimension must fit the int-based FFT and mesh APIs", HYOWON_EOVERFLOW;
+    if (M % N != 0)
+        return *err = "Generated IC mesh must be an integer multiple of particles_per_dimension",
+               HYOWON_EINVAL;
+    if (in->lpt_order == 2 && !alias_free(M, K))
+        return *err = "Generated projected 2LPT IC mesh must satisfy M > 3*K", HYOWON_EINVAL;
+    if (in->amplitude_mode != HYOWON_IC_GAUSSIAN && in->amplitude_mode != HYOWON_IC_FIXED)
+        return *err = "ic.amplitude_mode must be 'gaussian' or 'fixed'", HYOWON_EINVAL;
+    if (in->phase_pairing < HYOWON_IC_INDEPENDENT || in->phase_pairing > HYOWON_IC_PAIR_B)
+        return *err = "ic.phase_pairing must be 'independent', 'pair_a', or 'pair_b'", HYOWON_EINVAL;
+    if (!std::isfinite(in->momentum_factor_1) ||
+        (in->lpt_order == 2 &&
+         (!std::isfinite(in->position_factor_2) || !std::isfinite(in->momentum_factor_2))))
+        return *err = "Invalid start-scaled LPT normalization", HYOWON_ERUNTIME;
+    out->N = static_cast<int>(N);
+    out->M = static_cast<int>(M);
+    out->L = in->box_size;
+    out->seed = in->seed;
+    out->K = static_cast<int>(K);
+    out->fixed = in->amplitude_mode == HYOWON_IC_FIXED;
+    out->negate = in->phase_pairing == HYOWON_IC_PAIR_B;
+    out->order = in->lpt_order;
+    out->p1 = in->momentum_factor_1;
+    out->x2 = in->position_factor_2;
+    out->p2 = in->momentum_factor_2;
+    return HYOWON_OK;
+}
+
+int mode_amplitudes(uint64_t M, double L, uint64_t n, const double* power, double* amp,
+                    const char** err) {
+    if (M == 0 || !std::isfinite(L) || !(L > 0.0) || (n && (!power || !amp)))
+        return *err = "mode amplitudes need M > 0, a finite positive box and the tables",
+               HYOWON_EINVAL;
+    Scaled norm;
+    const double nr = static_cast<double>(M);
+    for (int r = 0; r < 6; ++r) norm.consume(nr, false);
+    for (int r = 0; r < 3; ++r) norm.consume(L, true);
+    for (uint64_t s = 0; s < n; ++s) {
+        amp[2 * s] = amp[2 * s + 1] = 0.0;
+        if (s == 0) continue;
+        const double p = power[s];
+        if (!std::isfinite(p) || !(p > 0.0))
+            return *err = "RandomField power spectrum returned invalid P(k)", HYOWON_ERUNTIME;
+        Scaled t = norm;
+        t.consume(p, false);
+        double var = 0.0;
+        const bool have = Scaled::materialize(t.mant, t.expo, &var) == 0;
+        double a1 = 0.0, a2 = 0.0;
+        int bad = 0;
+        if (have) {
+            a1 = std::sqrt(var);
+            const double reduced = var / 2.0;
+            if (reduced > 0.0) a2 = std::sqrt(reduced);
+            else bad |= norm.sqrt_of_quotient(p, 2.0, &a2);
+        } else {
+            bad |= norm.sqrt_of_quotient(p, 1.0, &a1);
+            bad |= norm.sqrt_of_quotient(p, 2.0, &a2);
+        }
+        if (bad || !std::isfinite(a1) || !std::isfinite(a2))
+            return *err = "RandomField mode amplitude is not representable as finite core::Real",
+                   HYOWON_EOVERFLOW;
+        amp[2 * s] = a1;
+        amp[2 * s + 1] = a2;
+    }
+    return HYOWON_OK;
+}
+
+int upload_amplitudes(const Params& p, uint64_t n_power, const double* power, double2** d_amp,
+                      const char** err) {
+    const uint64_t need = 3ull * p.K * p.K + 1;
+    if (!power || n_power < need)
+        return *err = "power must hold P(k_s) for s = 0 .. 3K^2", HYOWON_EINVAL;
+    double* amp = static_cast<double*>(std::malloc(sizeof(double) * 2 * need));
+    if (!amp) return *err = "host amplitude table could not be allocated", HYOWON_ENOMEM;
+    int rc = mode_amplitudes(static_cast<uint64_t>(p.M), p.L, need, power, amp, err);
+    if (rc == HYOWON_OK) {
+        if (cudaMalloc(d_amp, sizeof(double2) * need) != cudaSuccess) {
+            *err = "device amplitude table could not be allocated";
+            rc = HYOWON_ENOMEM;
+        } else if (cudaMemcpy(*d_amp, amp, sizeof(double2) * need, cudaMemcpyHostToDevice) !=
+                   cudaSuccess) {
+            cudaFree(*d_amp);
+            *d_amp = nullptr;
+            *err = "amplitude table upload failed";
+            rc = HYOWON_ECUDA;
+        }
+    }
+    std::free(amp);
+    return rc;
+}
+
+int status_code(unsigned int st, const char** err) {
+    if (!st) return HYOWON_OK;
+    if (st & IC_AMPLITUDE) return *err = "RandomField power spectrum returned invalid P(k)", HYOWON_ERUNTIME;
+    if (st & IC_PSI1) return *err = "1LPT particle update is non-finite or unrepresentable", HYOWON_ERUNTIME;
+    if (st & IC_HESSIAN) return *err = "2LPT first-order Hessian is non-finite", HYOWON_ERUNTIME;
+    if (st & IC_SOURCE) return *err = "2LPT quadratic source is non-finite", HYOWON_EOVERFLOW;
+    return *err = "2LPT particle update is non-finite or unrepresentable", HYOWON_ERUNTIME;
+}
+
+// ---------------------------------------------------------------- device ----
+
+int field_device(const Params& p, const double2* d_amp, double2* d_modes, unsigned int* d_status,
+                 cudaStream_t s, const char** err) {
+    const uint64_t half = static_cast<uint64_t>(p.M) * p.M * (p.M / 2 + 1);
+    k_field<<<grid(half), 256, 0, s>>>(p.M, p.K, p.seed, p.fixed, p.negate, d_amp, d_modes,
+                                       d_status);
+    if (cudaGetLastError() != cudaSuccess) return *err = "IC field launch failed", HYOWON_ECUDA;
+    return HYOWON_OK;
+}
+
+int generate_device(const Params& p, const double2* d_amp, double* const d_pos[3],
+                    double* const d_mom[3], unsigned int* d_status, cudaStream_t s,
+                    const char** err) {
+    const int M = p.M;
+    const uint64_t half = static_cast<uint64_t>(M) * M * (M / 2 + 1);
+    const uint64_t cells = static_cast<uint64_t>(M) * M * M;
+    const uint64_t n = static_cast<uint64_t>(p.N) * p.N * p.N;
+    const double norm = 1.0 / (static_cast<double>(M) * M * M);
+    DeviceBuffer<double2> delta, work;
+    DeviceBuffer<double> field, source;
+    if (!delta.alloc(half) || !work.alloc(half) || !field.alloc(cells) ||
+        (p.order == 2 && !source.alloc(cells)))
+        return *err = "IC mesh work arrays could not be allocated", HYOWON_ENOMEM;
+    Fft fft;
+    int rc = fft.make(M, p.order == 2, s, err);
+    if (rc) return rc;
+    auto c2r = [&](double2* in) {
+        return cufftExecZ2D(fft.c2r, reinterpret_cast<cufftDoubleComplex*>(in), field.p) ==
+               CUFFT_SUCCESS;
+    };
+    k_lattice<<<grid(n), 256, 0, s>>>(p.N, p.L / static_cast<double>(p.N), d_pos[0], d_pos[1],
+                                      d_pos[2], d_mom[0], d_mom[1], d_mom[2]);
+    if ((rc = field_device(p, d_amp, delta.p, d_status, s, err))) return rc;
+    for (int a = 0; a < 3; ++a) {
+        k_spectral<<<grid(half), 256, 0, s>>>(M, p.L, kPsi1, a, a, p.K, delta.p, work.p);
+        if (!c2r(work.p)) return *err = "IC c2r failed", HYOWON_ECUDA;
+        k_apply<<<grid(n), 256, 0, s>>>(p.N, M, field.p, norm, 1.0, p.p1, p.L, d_pos[a], d_mom[a],
+                                        IC_PSI1, d_status);
+    }
+    if (p.order == 2) {
+        static const int pairs[7][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}, {-1, -1}};
+        for (int t = 0; t < 7; ++t) {
+            const bool trace = t == 6;
+            k_spectral<<<grid(half), 256, 0, s>>>(M, p.L, trace ? kTrace : kHessian,
+                                                  trace ? 0 : pairs[t][0], trace ? 0 : pairs[t][1],
+                                                  p.K, delta.p, work.p);
+            if (!c2r(work.p)) return *err = "IC c2r failed", HYOWON_ECUDA;
+            const int op = trace ? 3 : (t == 0 ? 0 : (t < 3 ? 1 : 2));
+            k_source<<<grid(cells), 256, 0, s>>>(cells, field.p, norm, op, source.p, d_status);
+        }
+        if (cufftExecD2Z(fft.r2c, source.p, reinterpret_cast<cufftDoubleComplex*>(work.p)) !=
+            CUFFT_SUCCESS)
+            return *err = "IC r2c of the 2LPT source failed", HYOWON_ECUDA;
+        for (int a = 0; a < 3; ++a) {
+            k_spectral<<<grid(half), 256, 0, s>>>(M, p.L, kPsi2, a, a, p.K, work.p, delta.p);
+            if (!c2r(delta.p)) return *err = "IC c2r failed", HYOWON_ECUDA;
+            k_apply<<<grid(n), 256, 0, s>>>(p.N, M, field.p, norm, p.x2, p.p2, p.L, d_pos[a],
+                                            d_mom[a], IC_PSI2, d_status);
+        }
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) return *err = "IC kernels failed", HYOWON_ECUDA;
+    return HYOWON_OK;
+}
+
+}  // namespace ic
+}  // namespace hyowon
+
+// ------------------------------------------------------------------ C ABI ---
+
+namespace {
+thread_local char g_ic_err[256] = "";
+
+int ic_fail(int rc, const char* msg) {
+    std::strncpy(g_ic_err, msg ? msg : "IC generation failed", sizeof(g_ic_err) - 1);
+    g_ic_err[sizeof(g_ic_err) - 1] = '\0';
+    return rc;
+}
+
+// Device state of one standalone call.
+struct Call {
+    cudaStream_t s = nullptr;
+    unsigned int* d_status = nullptr;
+    double2* d_amp = nullptr;
+    ~Call() {
+        if (s) cudaStreamDestroy(s);
+        cudaFree(d_status);
+        cudaFree(d_amp);
+    }
+    int open(const hyowon::ic::Params& p, uint64_t n_power, const double* power,
+             const char** err) {
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaMalloc(&d_status, sizeof(unsigned int)) != cudaSuccess ||
+            cudaMemset(d_status, 0, sizeof(unsigned int)) != cudaSuccess)
+            return *err = "CUDA stream / status allocation failed", HYOWON_ECUDA;
+        return hyowon::ic::upload_amplitudes(p, n_power, power, &d_amp, err);
+    }
+    int finish(const char** err) {
+        unsigned int st = 0;
+        if (cudaStreamSynchronize(s) != cudaSuccess ||
+            cudaMemcpy(&st, d_status, sizeof(st), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return *err = "IC kernels failed", HYOWON_ECUDA;
+        return hyowon::ic::status_code(st, err);
+    }
+};
+}  // namespace
+
+extern "C" {
+
+const char* hyowon_ic_last_error(void) { return g_ic_err; }
+
+int hyowon_ic_resolve(const hyowon_ic_params_t* p, uint64_t* mesh, uint64_t* max_mode) {
+    hyowon::ic::Params r;
+    const char* err = nullptr;
+    const int rc = hyowon::ic::resolve(p, &r, &err);
+    if (rc) return ic_fail(rc, err);
+    if (mesh) *mesh = static_cast<uint64_t>(r.M);
+    if (max_mode) *max_mode = static_cast<uint64_t>(r.K);
+    return HYOWON_OK;
+}
+
+int hyowon_ic_mode_amplitudes(uint64_t mesh, double box_size, uint64_t n, const double* power,
+                              double* amp) {
+    const char* err = nullptr;
+    const int rc = hyowon::ic::mode_amplitudes(mesh, box_size, n, power, amp, &err);
+    return rc ? ic_fail(rc, err) : HYOWON_OK;
+}
+
+int hyowon_ic_field(const hyowon_ic_params_t* p, uint64_t n_power, const double* power,
+                    double* modes) {
+    hyowon::ic::Params r;
+    const char* err = nullptr;
+    int rc = hyowon::ic::resolve(p, &r, &err);
+    if (rc) return ic_fail(rc, err);
+    if (!modes) return ic_fail(HYOWON_EINVAL, "modes must not be NULL");
+    Call c;
+    if ((rc = c.open(r, n_power, power, &err))) return ic_fail(rc, err);
+    const uint64_t half = static_cast<uint64_t>(r.M) * r.M * (r.M / 2 + 1);
+    double2* d_modes = nullptr;
+    if (cudaMalloc(&d_modes, sizeof(double2) * half) != cudaSuccess)
+        return ic_fail(HYOWON_ENOMEM, "IC field could not be allocated");
+    rc = hyowon::ic::field_device(r, c.d_amp, d_modes, c.d_status, c.s, &err);
+    if (!rc) rc = c.finish(&err);
+    if (!rc && cudaMemcpy(modes, d_modes, sizeof(double2) * half, cudaMemcpyDeviceToHost) !=
+                   cudaSuccess) {
+        rc = HYOWON_ECUDA;
+        err = "IC field download failed";
+    }
+    cudaFree(d_modes);
+    return rc ? ic_fail(rc, err) : HYOWON_OK;
+}
+
+int hyowon_ic_generate(const hyowon_ic_params_t* p, uint64_t n_power, const double* power,
+                       double* x, double* y, double* z, double* px, double* py, double* pz) {
+    hyowon::ic::Params r;
+    const char* err = nullptr;
+    int rc = hyowon::ic::resolve(p, &r, &err);
+    if (rc) return ic_fail(rc, err);
+    double* host[6] = {x, y, z, px, py, pz};
+    for (double* h : host)
+        if (!h) return ic_fail(HYOWON_EINVAL, "particle arrays must not be NULL");
+    Call c;
+    if ((rc = c.open(r, n_power, power, &err))) return ic_fail(rc, err);
+    const uint64_t n = static_cast<uint64_t>(r.N) * r.N * r.N;
+    double* d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * 6 * n) != cudaSuccess)
+        return ic_fail(HYOWON_ENOMEM, "particle arrays could not be allocated on the device");
+    double* const pos[3] = {d, d + n, d + 2 * n};
+    double* const mom[3] = {d + 3 * n, d + 4 * n, d + 5 * n};
+    rc = hyowon::ic::generate_device(r, c.d_amp, pos, mom, c.d_status, c.s, &err);
+    if (!rc) rc = c.finish(&err);
+    for (int a = 0; a < 6 && !rc; ++a)
+        if (cudaMemcpy(host[a], d + a * n, sizeof(double) * n, cudaMemcpyDeviceToHost) !=
+            cudaSuccess) {
+            rc = HYOWON_ECUDA;
+            err = "particle download failed";
+        }
+    cudaFree(d);
+    return rc ? ic_fail(rc, err) : HYOWON_OK;
+}
+
+}  // extern "C"

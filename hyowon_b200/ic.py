@@ -183,3 +183,144 @@ def config_schedule(name: str):
     c = CONFIGS[name]
     a_start = 1.0 / (1.0 + c["z_start"])
     return a_start, math.log(1.0 / a_start) / c["steps"]
+
+
+# --------------------------------------------------------------------------
+# Generated initial conditions (include/hyowon_ic.h): HYOWON's own generator,
+# the Philox per-mode Fourier field and 1LPT / projected 2LPT, on the device.
+# --------------------------------------------------------------------------
+_AMPLITUDE = {"gaussian": 0, "fixed": 1}
+_PAIRING = {"independent": 0, "pair_a": 1, "pair_b": 2}
+
+
+class ICParams:
+    """The ic.* coordinates of SimulationParameters in generate mode
+    (include/cosmo_nbody/config/simulation_parameters.hpp:59-82) plus the
+    start-epoch LPT factors (src/ic/lpt_displacement.cpp:197-222)."""
+
+    def __init__(self, particles_per_dimension: int, box_size: float, seed: int,
+                 a_start: float, lpt_order: int = 1, mesh_per_dimension: int = 0,
+                 max_mode_per_axis: int = None, amplitude_mode: str = "gaussian",
+                 phase_pairing: str = "independent", model: CosmologyModel = None,
+                 factors=None):
+        if amplitude_mode not in _AMPLITUDE:
+            raise ValueError("ic.amplitude_mode must be 'gaussian' or 'fixed'")
+        if phase_pairing not in _PAIRING:
+            raise ValueError("ic.phase_pairing must be 'independent', 'pair_a', or 'pair_b'")
+        self.particles_per_dimension = int(particles_per_dimension)
+        self.box_size = float(box_size)
+        self.seed = int(seed)
+        self.a_start = float(a_start)
+        self.lpt_order = int(lpt_order)
+        self.mesh_per_dimension = int(mesh_per_dimension)
+        self.max_mode_per_axis = max_mode_per_axis
+        self.amplitude_mode = amplitude_mode
+        self.phase_pairing = phase_pairing
+        self.factors = tuple(factors) if factors is not None else lpt_factors(a_start, model)
+
+    def to_c(self):
+        from . import _native as nat
+        p1, x2, p2 = self.factors
+        return nat.ICParams(self.particles_per_dimension, self.mesh_per_dimension, self.box_size,
+                            self.seed, -1 if self.max_mode_per_axis is None
+                            else int(self.max_mode_per_axis), _AMPLITUDE[self.amplitude_mode],
+                            _PAIRING[self.phase_pairing], self.lpt_order, p1, x2, p2)
+
+    def resolve(self):
+        """(M, K): the IC mesh and Cartesian support (hyowon_ic_resolve)."""
+        import ctypes
+        from . import _native as nat
+        c = self.to_c()
+        M, K = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        _ic_check(nat.lib().hyowon_ic_resolve(ctypes.byref(c), ctypes.byref(M), ctypes.byref(K)),
+                  "resolve")
+        return int(M.value), int(K.value)
+
+
+def _ic_check(rc, where):
+    from . import _native as nat
+    if rc != nat.OK:
+        msg = nat.lib().hyowon_ic_last_error().decode(errors="replace")
+        raise nat._EXC.get(rc, RuntimeError)(f"{where}: {msg}")
+
+
+def lpt_factors(a_start: float, model: CosmologyModel = None):
+    """(a^2 H f1, D2/D1^2, a^2 H f2 D2/D1^2) at a_start, formed as
+    apply_to_arrays forms them (src/ic/lpt_displacement.cpp:197-222)."""
+    model = model or CosmologyModel()
+    D1, f1, D2, f2 = (float(v[0]) for v in model.growth2(a_start))
+    H = float(model.H(a_start)[0])
+    p1 = a_start * a_start * H * f1
+    x2 = D2 / (D1 * D1)
+    p2 = a_start * a_start * H * f2 * x2
+    return p1, x2, p2
+
+
+def represented_wavenumbers(box_size: float, max_mode: int):
+    """k_s = double(sqrt((long double) s)) * (2 pi / L) for s = 0 .. 3K^2
+    (include/cosmo_nbody/ic/particle_lattice_bandlimit.hpp:27-37)."""
+    s = np.arange(3 * max_mode * max_mode + 1, dtype=np.longdouble)
+    return np.sqrt(s).astype(np.float64) * (2.0 * math.pi / box_size)
+
+
+def start_spectrum(a_start: float, spectrum: "LinearSpectrum" = None,
+                   model: CosmologyModel = None, table_a: float = 1.0) -> "LinearSpectrum":
+    """LinearPowerSpectrum(config): the table rescaled by (D1(a_start) /
+    D1(table_a))^2 before the log-log spline (src/ic/linear_power_spectrum.cpp:451-488)."""
+    spectrum = spectrum or LinearSpectrum()
+    model = model or CosmologyModel()
+    D1 = model.growth(np.array([a_start, table_a]))[0]
+    scale = (float(D1[0]) / float(D1[1])) ** 2.0
+    return LinearSpectrum(spectrum.k, spectrum.P * scale)
+
+
+def power_table(params: ICParams, spectrum: "LinearSpectrum"):
+    """P at the represented wavenumbers of every |m|^2 in the support (the
+    `power` argument of include/hyowon_ic.h); spectrum at the start epoch."""
+    _, K = params.resolve()
+    k = represented_wavenumbers(params.box_size, K)
+    out = np.zeros_like(k)
+    out[1:] = spectrum(k[1:])
+    return out
+
+
+def mode_amplitudes(mesh: int, box_size: float, power):
+    """{sqrt(var_s), sqrt(var_s/2)} per s (hyowon_ic_mode_amplitudes; host only)."""
+    from . import _native as nat
+    power = np.ascontiguousarray(power, dtype=np.float64)
+    amp = np.zeros((power.size, 2))
+    _ic_check(nat.lib().hyowon_ic_mode_amplitudes(mesh, box_size, power.size, nat.dptr(power),
+                                                  nat.dptr(amp)), "mode_amplitudes")
+    return amp
+
+
+class RandomField:
+    """RandomField::generate (src/ic/random_field.cpp:70-330) on the device."""
+
+    @staticmethod
+    def generate(params: ICParams, power) -> np.ndarray:
+        import ctypes
+        from . import _native as nat
+        M, _ = params.resolve()
+        power = np.ascontiguousarray(power, dtype=np.float64)
+        out = np.zeros((M, M, M // 2 + 1), dtype=np.complex128)
+        c = params.to_c()
+        _ic_check(nat.lib().hyowon_ic_field(ctypes.byref(c), power.size, nat.dptr(power),
+                                            out.ctypes.data_as(nat.P_double)), "RandomField")
+        return out
+
+
+def generate_ics(params: ICParams, power) -> dict:
+    """The generate branch of InitialConditions on the device
+    (hyowon_ic_generate): {x, y, z, px, py, pz} in particle order."""
+    import ctypes
+    from . import _native as nat
+    n = params.particles_per_dimension ** 3
+    st = {k: np.zeros(n) for k in ("x", "y", "z", "px", "py", "pz")}
+    power = np.ascontiguousarray(power, dtype=np.float64)
+    c = params.to_c()
+    _ic_check(nat.lib().hyowon_ic_generate(ctypes.byref(c), power.size, nat.dptr(power),
+                                           *[nat.dptr(st[k]) for k in
+                                             ("x", "y", "z", "px", "py", "pz")]),
+              "generate_ics")
+    return st

@@ -207,6 +207,16 @@ class PMSolver:
                                             nat.dptr(K2), nat.dptr(md)), "run")
         return md
 
+    def generate_ics(self, params, power, uniform_mass: float):
+        """Generated initial conditions straight into the device state
+        (hyowon_pm_generate_ics): params is an ic.ICParams, power the table
+        of ic.power_table."""
+        c = params.to_c()
+        power = _f64(power)
+        self._check(nat.lib().hyowon_pm_generate_ics(self._h, ctypes.byref(c), power.size,
+                                                     nat.dptr(power), float(uniform_mass)),
+                    "generate_ics")
+
     def potential(self):
         N = self.geom.n_mesh
         phi = np.empty(N ** 3)
@@ -298,6 +308,15 @@ class CosmologyModel:
                                      nat.dptr(D1), nat.dptr(f1))
         nat.raise_for(rc, None, "CosmologyModel.growth")
         return D1, f1
+
+    def growth2(self, a):
+        """(D1, f1, D2, f2) at a (0 < a <= 1); D2 < 0 normalised by D1(1)^2."""
+        a = np.atleast_1d(_f64(a))
+        out = [np.empty_like(a) for _ in range(4)]
+        rc = nat.lib().hyowon_growth2(self.omega_m, self.omega_lambda, a.size, nat.dptr(a),
+                                      *[nat.dptr(o) for o in out])
+        nat.raise_for(rc, None, "CosmologyModel.growth2")
+        return tuple(out)
 
 
 class DriftKickIntegrator:

@@ -44,6 +44,14 @@ int hyowon_schedule(double omega_m, double omega_l, double a_start, double a_fin
 int hyowon_growth(double omega_m, double omega_l, uint64_t n, const double* a, double* D1,
                   double* f1);
 
+/* Second-order growth D2(a) (normalised by D1(1)^2, negative) and
+ * f2 = dln|D2|/dlna of flat matter + Lambda together with D1, f1
+ * (include/cosmo_nbody/cosmology/cosmology_model.hpp:50-53): RK4 in ln a of
+ * the growth ODE from the matter era. 0 < a <= 1. The 2LPT factors of
+ * hyowon_ic_params_t are D2/D1^2 and a^2 H f2 D2/D1^2. */
+int hyowon_growth2(double omega_m, double omega_l, uint64_t n, const double* a, double* D1,
+                   double* f1, double* D2, double* f2);
+
 #ifdef __cplusplus
 }
 #endif

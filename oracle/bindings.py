@@ -309,6 +309,14 @@ class Reference:
         self._check(rc, "ref_growth")
         return D1, f1
 
+    def growth2(self, a, omega_m=0.3, omega_l=0.7):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        out = [np.zeros_like(a) for _ in range(4)]
+        rc = self.lib.ref_growth2(_c_double(omega_m), _c_double(omega_l), _c_u64(a.size), _dp(a),
+                                  *[_dp(o) for o in out])
+        self._check(rc, "ref_growth2")
+        return tuple(out)
+
     def kdk_run(self, L, N, state, a_start, a_final, delta_ln_a, steps, uniform_mass,
                 deconvolve=False, omega_m=0.3, omega_l=0.7):
         """Runs `steps` KDK steps in place on state (x..pz); fills ax..az.
@@ -324,3 +332,68 @@ class Reference:
             _dp(s["ay"]), _dp(s["az"]), _dp(md), ctypes.byref(sec))
         self._check(rc, "ref_kdk_run")
         return md[:steps], sec.value
+
+    def philox(self, counters, keys):
+        """Philox4x32-10 blocks: counters (n, 4) u32, keys (n, 2) u32 -> (n, 4) u32."""
+        c = np.ascontiguousarray(counters, dtype=np.uint32).reshape(-1, 4)
+        k = np.ascontiguousarray(keys, dtype=np.uint32).reshape(-1, 2)
+        out = np.zeros_like(c)
+        rc = self.lib.ref_philox(_c_u64(c.shape[0]), _ip(c, ctypes.c_uint32),
+                                 _ip(k, ctypes.c_uint32), _ip(out, ctypes.c_uint32))
+        self._check(rc, "ref_philox")
+        return out
+
+    def mode_draws(self, seed, stream, modes):
+        """(u1, u2, n1, n2) per integer mode counter (n, 3) under seed/stream."""
+        m = np.ascontiguousarray(modes, dtype=np.int32).reshape(-1, 3)
+        out = np.zeros((m.shape[0], 4))
+        rc = self.lib.ref_mode_draws(_c_u64(seed), ctypes.c_uint32(stream), _c_u64(m.shape[0]),
+                                     _ip(m, ctypes.c_int32), _dp(out))
+        self._check(rc, "ref_mode_draws")
+        return out
+
+    def generate_ics(self, L, N, pk_path, z_pk, z_start, seed, lpt_order=1, mesh=0,
+                     amplitude_fixed=False, pairing=0, max_mode=-1, particles=True):
+        """RandomField::generate + LPTDisplacement::apply_to_arrays on the
+        corner lattice. Returns a dict: M, K, D1, D2, f1, f2, H, a_start,
+        modes (M, M, M//2+1) complex, power[s], amp (s, 2) and, when
+        `particles`, x..pz."""
+        meta = np.zeros(8)
+        args = (_c_double(L), _c_u64(N), _c_u64(0), _c_u64(seed), _c_int(int(amplitude_fixed)),
+                _c_int(pairing), _c_int(lpt_order), ctypes.c_int64(max_mode),
+                _c_double(z_start), pk_path.encode(), _c_double(z_pk), _dp(meta))
+        # first call: IC mesh and support only
+        self.lib.ref_generate_ics.argtypes = None
+        rc = self.lib.ref_generate_ics(*args[:2], _c_u64(mesh), *args[3:], None, None, None,
+                                       None, None, None, None, None, None)
+        self._check(rc, "ref_generate_ics")
+        M, K = int(meta[0]), int(meta[1])
+        modes = np.zeros((M, M, M // 2 + 1), dtype=np.complex128)
+        power = np.zeros(3 * K * K + 1)
+        amp = np.zeros((3 * K * K + 1, 2))
+        n = N ** 3
+        st = {k: np.zeros(n) for k in ("x", "y", "z", "px", "py", "pz")} if particles else None
+        pp = [_dp(st[k]) for k in ("x", "y", "z", "px", "py", "pz")] if particles else [None] * 6
+        rc = self.lib.ref_generate_ics(*args[:2], _c_u64(mesh), *args[3:],
+                                       modes.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       _dp(power), _dp(amp), *pp)
+        self._check(rc, "ref_generate_ics")
+        out = dict(M=M, K=K, D1=meta[2], D2=meta[3], f1=meta[4], f2=meta[5], H=meta[6],
+                   a_start=meta[7], modes=modes, power=power, amp=amp)
+        if particles:
+            out.update(st)
+        return out
+
+
+# The semantic header LinearPowerSpectrum requires
+# (src/ic/linear_power_spectrum.cpp:31-46,184-229), for the flat LCDM
+# cosmology of the harness (h 0.7, Om 0.3, Ob 0, OL 0.7, n_s 0.965, sigma8 0.8).
+def write_power_spectrum_file(path, k, P, redshift):
+    lines = ["# k_unit=h/Mpc", "# power_unit=(Mpc/h)^3", f"# redshift={redshift!r}",
+             "# species=cold_plus_baryon", "# gauge=synchronous",
+             "# fidelity=precision_boltzmann", "# normalization=sigma8_z0",
+             "# normalization_value=0.8", "# nonlinear=false", "# massive_neutrino_sum_eV=0",
+             "# h=0.7", "# omega_m=0.3", "# omega_b=0", "# omega_lambda=0.7", "# n_s=0.965"]
+    lines += [f"{float(a)!r} {float(b)!r}" for a, b in zip(k, P)]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")

@@ -20,6 +20,12 @@
 #include "cosmo_nbody/gravity/octree.hpp"
 #include "cosmo_nbody/gravity/tree_walk.hpp"
 #include "cosmo_nbody/gravity/pm_solver.hpp"
+#include "cosmo_nbody/ic/linear_power_spectrum.hpp"
+#include "cosmo_nbody/ic/lpt_displacement.hpp"
+#include "cosmo_nbody/ic/particle_lattice_bandlimit.hpp"
+#include "cosmo_nbody/ic/philox_rng.hpp"
+#include "cosmo_nbody/ic/random_field.hpp"
+#include "cosmo_nbody/math/scaled_positive_product.hpp"
 #include "cosmo_nbody/math/density_normalization.hpp"
 #include "cosmo_nbody/mesh/fft_backend.hpp"
 #include "cosmo_nbody/mesh/green_function.hpp"
@@ -33,7 +39,9 @@
 #include "cosmo_nbody/validation/force_balance_diagnostics.hpp"
 #include "mesh/cic_coordinate.hpp"
 
+#include <array>
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <optional>
@@ -352,6 +360,20 @@ int ref_growth(double omega_m, double omega_l, std::uint64_t n, const double* a,
     });
 }
 
+// Second-order growth D2(a), f2(a) with D1, f1 (cosmology_model.hpp:47-53).
+int ref_growth2(double omega_m, double omega_l, std::uint64_t n, const double* a, double* D1,
+                double* f1, double* D2, double* f2) {
+    return guarded([&] {
+        cosmology::CosmologyModel model(flat_lcdm(omega_m, omega_l));
+        for (std::uint64_t i = 0; i < n; ++i) {
+            D1[i] = model.D1(a[i]);
+            f1[i] = model.f1(a[i]);
+            D2[i] = model.D2(a[i]);
+            f2[i] = model.f2(a[i]);
+        }
+    });
+}
+
 // The production KDK loop: TimeStepper + LeapfrogIntegrator with a PMSolver
 // force callback (src/runtime/simulation_runner.cpp:1009-1143,1348-1351).
 // Runs the first `steps_to_run` steps of the schedule on the state in
@@ -479,6 +501,149 @@ int ref_tree_short_forces(double L, std::uint64_t n_side, std::uint64_t n_mesh,
             ay[k] = a.y;
             az[k] = a.z;
         }
+    });
+}
+
+// Philox4x32-10 blocks (src/ic/philox_rng.cpp): out4[4i..] from counter
+// ctr4[4i..] and key key2[2i..].
+int ref_philox(std::uint64_t n, const std::uint32_t* ctr4, const std::uint32_t* key2,
+               std::uint32_t* out4) {
+    return guarded([&] {
+        for (std::uint64_t i = 0; i < n; ++i) {
+            const ic::rng::Counter4x32 c{ctr4[4 * i], ctr4[4 * i + 1], ctr4[4 * i + 2],
+                                         ctr4[4 * i + 3]};
+            const ic::rng::Key2x32 k{key2[2 * i], key2[2 * i + 1]};
+            const auto w = ic::rng::philox4x32_10(c, k);
+            for (int j = 0; j < 4; ++j) out4[4 * i + j] = w[j];
+        }
+    });
+}
+
+// rng::uniform_pair_open01 and rng::normal_pair for n mode counters
+// (kx, ky, kz) = modes3[3i..] under one seed and stream: out4[4i..] =
+// {u1, u2, n1, n2}.
+int ref_mode_draws(std::uint64_t seed, std::uint32_t stream, std::uint64_t n,
+                   const std::int32_t* modes3, double* out4) {
+    return guarded([&] {
+        for (std::uint64_t i = 0; i < n; ++i) {
+            const auto [u1, u2] = ic::rng::uniform_pair_open01(
+                seed, modes3[3 * i], modes3[3 * i + 1], modes3[3 * i + 2], stream);
+            const auto [g1, g2] = ic::rng::normal_pair(
+                seed, modes3[3 * i], modes3[3 * i + 1], modes3[3 * i + 2], stream);
+            out4[4 * i] = u1;
+            out4[4 * i + 1] = u2;
+            out4[4 * i + 2] = g1;
+            out4[4 * i + 3] = g2;
+        }
+    });
+}
+
+// Generated initial conditions through the reference's own classes, the
+// sequence of src/ic/initial_conditions.cpp:295-378: corner lattice,
+// LinearPowerSpectrum(config) read from pk_path (tabulated at z_pk, rescaled
+// by the growth to z_start), RandomField::generate on the IC mesh, then
+// LPTDisplacement::apply_to_arrays. Flat LCDM Om=0.3, OL=0.7, h=0.7,
+// sigma8=0.8, n_s=0.965.
+//   mesh_request: 0 = the reference's automatic IC mesh; max_mode < 0: default.
+//   amplitude_fixed: 0 gaussian, 1 fixed; pairing: 0 independent, 1 pair_a,
+//   2 pair_b.
+// Outputs (any may be null except meta): meta[0..7] = {M, K, D1, D2, f1, f2,
+// H, a_start}; modes (2*M*M*(M/2+1) doubles) the generated field before LPT;
+// power[s], s = 0..3K^2: pk.evaluate of the represented wavenumber
+// sqrt(s) k_f (0 at s = 0); amp[2s..] = {sqrt(var_s), sqrt(var_s/2)} with
+// var_s = M^6/L^3 P_s as the generator forms them; x..pz the N^3 particles.
+int ref_generate_ics(double L, std::uint64_t N, std::uint64_t mesh_request, std::uint64_t seed,
+                     int amplitude_fixed, int pairing, int lpt_order, std::int64_t max_mode,
+                     double z_start, const char* pk_path, double z_pk, double* meta,
+                     double* modes, double* power, double* amp, double* x, double* y,
+                     double* z, double* px, double* py, double* pz) {
+    return guarded([&] {
+        config::GravityParams g;
+        g.solver = "PM";
+        g.deconvolve_cic = core::ExplicitBoolean(false);
+        config::BoxParams b;
+        b.L = L;
+        b.N = N;
+        b.N_mesh = N;
+        config::TimeParams t;
+        t.z_start = z_start;
+        t.z_final = 0.0;
+        t.delta_ln_a = 0.1;
+        config::ICParams ic;
+        ic.mode = "generate";
+        ic.lpt_order = lpt_order;
+        ic.seed = seed;
+        ic.mesh_per_dimension = mesh_request;
+        if (max_mode >= 0) ic.max_mode_per_axis = static_cast<std::uint64_t>(max_mode);
+        ic.power_spectrum_file = pk_path;
+        ic.power_spectrum_redshift = z_pk;
+        ic.power_spectrum_fidelity = "precision_boltzmann";
+        ic.amplitude_mode = amplitude_fixed ? "fixed" : "gaussian";
+        ic.phase_pairing = pairing == 2 ? "pair_b" : (pairing == 1 ? "pair_a" : "independent");
+        config::OutputParams o;
+        config::SimulationParameters cfg(flat_lcdm(0.3, 0.7), b, g, t, ic, o);
+        const std::uint64_t M = cfg.ic_mesh_per_dimension();
+        const std::uint64_t K = cfg.ic_effective_max_mode_per_axis();
+        cosmology::CosmologyModel cosmo(cfg.get_cosmology());
+        const double a0 = 1.0 / (1.0 + z_start);
+        meta[0] = static_cast<double>(M);
+        meta[1] = static_cast<double>(K);
+        meta[2] = cosmo.D1(a0);
+        meta[3] = cosmo.D2(a0);
+        meta[4] = cosmo.f1(a0);
+        meta[5] = cosmo.f2(a0);
+        meta[6] = cosmo.H(a0);
+        meta[7] = a0;
+
+        ic::LinearPowerSpectrum pk(cfg);
+        if (power || amp) {
+            const double kf = 2.0 * std::numbers::pi / L;
+            const double nr = static_cast<double>(M);
+            const std::array<double, 6> num{nr, nr, nr, nr, nr, nr};
+            const std::array<double, 3> den{L, L, L};
+            const auto norm = math::ScaledPositiveProduct::from_quotient(num, den, "harness");
+            for (std::uint64_t s = 0; s <= 3 * K * K; ++s) {
+                double p = 0.0, a1 = 0.0, a2 = 0.0;
+                if (s > 0) {
+                    const double k = static_cast<double>(
+                        std::sqrt(static_cast<long double>(s))) * kf;
+                    p = pk.evaluate(k);
+                    const double var = norm.multiplied_by(p, "harness variance");
+                    a1 = std::sqrt(var);
+                    a2 = std::sqrt(var / 2.0);
+                }
+                if (power) power[s] = p;
+                if (amp) {
+                    amp[2 * s] = a1;
+                    amp[2 * s + 1] = a2;
+                }
+            }
+        }
+
+        const mesh::MeshGeometry geom(L, M);
+        mesh::ComplexField delta(geom.complex_size());
+        ic::RandomField::generate(cfg, pk, delta, M);
+        if (modes) std::memcpy(modes, delta.data(), sizeof(double) * 2 * geom.complex_size());
+        if (!x) return;
+        const std::uint64_t n = N * N * N;
+        std::vector<double> ax(n), ay(n), az(n), bx(n, 0.0), by(n, 0.0), bz(n, 0.0);
+        const double dx = L / static_cast<double>(N);
+        for (std::uint64_t i = 0; i < N; ++i)
+            for (std::uint64_t j = 0; j < N; ++j)
+                for (std::uint64_t k = 0; k < N; ++k) {
+                    const std::uint64_t p = (i * N + j) * N + k;
+                    ax[p] = static_cast<double>(i) * dx;
+                    ay[p] = static_cast<double>(j) * dx;
+                    az[p] = static_cast<double>(k) * dx;
+                }
+        mesh::FFTBackend fft(geom);
+        ic::LPTDisplacement::apply_to_arrays(cfg, cosmo, fft, delta, ax, ay, az, bx, by, bz);
+        std::memcpy(x, ax.data(), sizeof(double) * n);
+        std::memcpy(y, ay.data(), sizeof(double) * n);
+        std::memcpy(z, az.data(), sizeof(double) * n);
+        std::memcpy(px, bx.data(), sizeof(double) * n);
+        std::memcpy(py, by.data(), sizeof(double) * n);
+        std::memcpy(pz, bz.data(), sizeof(double) * n);
     });
 }
 

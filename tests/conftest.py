@@ -53,3 +53,8 @@ def c1_diag():
 @pytest.fixture(scope="session")
 def pk_golden():
     return load_golden("pk.npz")
+
+
+@pytest.fixture(scope="session")
+def ic_golden():
+    return load_golden("ic.npz")

@@ -28,7 +28,14 @@ Fixtures:
                       small_pm with explicit masses
 
     python tests/golden/make_golden.py --only diag    # c1_diag.npz alone
+  ic.npz              generated initial conditions of the reference
+                      (RandomField::generate + LPTDisplacement::apply_to_arrays
+                      on the corner lattice, IC_CASES: 1LPT / 2LPT, gaussian /
+                      fixed, pairings, explicit K and mesh), the P(k) table
+                      they read, Philox4x32-10 blocks and per-mode draws
+
     python tests/golden/make_golden.py --only pk      # pk.npz alone
+    python tests/golden/make_golden.py --only ic      # ic.npz alone
 """
 from __future__ import annotations
 
@@ -111,10 +118,51 @@ def pk_fixture(ref):
     np.savez_compressed(os.path.join(HERE, "pk.npz"), **out)
 
 
+# name, N, lpt_order, mesh request (0 = automatic), fixed amplitude, pairing
+# (0 independent, 1 pair_a, 2 pair_b), K (-1 = (N-1)/2), seed
+IC_CASES = [
+    ("n16_1lpt", 16, 1, 0, False, 0, -1, 11),
+    ("n16_2lpt", 16, 2, 0, False, 0, -1, 11),
+    ("n16_2lpt_fixed_pair_b", 16, 2, 0, True, 2, -1, 12345678901),
+    ("n12_2lpt_pair_a_k4", 12, 2, 0, False, 1, 4, 5),
+    ("n16_1lpt_m32_k5", 16, 1, 32, False, 0, 5, 3),
+]
+IC_BOX, IC_Z_START, IC_Z_PK = 100.0, 49.0, 0.0
+
+
+def ic_fixture(ref):
+    """ic.npz from the reference's RandomField / LPTDisplacement / Philox."""
+    import tempfile
+    from oracle.bindings import write_power_spectrum_file
+    k, P = ic.bbks_table()
+    out = dict(pk_k=k, pk_P=P, box=IC_BOX, z_start=IC_Z_START, z_pk=IC_Z_PK)
+    rng = np.random.default_rng(77)
+    ctr = rng.integers(0, 2 ** 32, (254, 4), dtype=np.uint64)
+    key = rng.integers(0, 2 ** 32, (254, 2), dtype=np.uint64)
+    ctr = np.concatenate([np.zeros((1, 4), np.uint64), np.full((1, 4), 2 ** 32 - 1, np.uint64), ctr])
+    key = np.concatenate([np.zeros((1, 2), np.uint64), np.full((1, 2), 2 ** 32 - 1, np.uint64), key])
+    out.update(philox_ctr=ctr.astype(np.uint32), philox_key=key.astype(np.uint32),
+               philox_out=ref.philox(ctr, key))
+    modes = rng.integers(-700, 701, (512, 3)).astype(np.int32)
+    out["draw_modes"] = modes
+    for seed, stream in ((0, 0), (11, 0), (12345678901, 1)):
+        out[f"draws_{seed}_{stream}"] = ref.mode_draws(seed, stream, modes)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "pk.txt")
+        write_power_spectrum_file(path, k, P, IC_Z_PK)
+        for name, N, order, mesh, fixed, pairing, K, seed in IC_CASES:
+            g = ref.generate_ics(IC_BOX, N, path, IC_Z_PK, IC_Z_START, seed, lpt_order=order,
+                                 mesh=mesh, amplitude_fixed=fixed, pairing=pairing, max_mode=K)
+            for f in ("M", "K", "D1", "D2", "f1", "f2", "H", "a_start", "modes", "power", "amp",
+                      "x", "y", "z", "px", "py", "pz"):
+                out[f"{name}__{f}"] = g[f]
+    np.savez_compressed(os.path.join(HERE, "ic.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
-    ap.add_argument("--only", choices=["diag", "pk"], default=None)
+    ap.add_argument("--only", choices=["diag", "pk", "ic"], default=None)
     args = ap.parse_args()
     build_reference(args.ref_root)
     ref = Reference()
@@ -123,6 +171,9 @@ def main():
         return
     if args.only == "pk":
         pk_fixture(ref)
+        return
+    if args.only == "ic":
+        ic_fixture(ref)
         return
 
     # -- schedules --------------------------------------------------------
@@ -213,6 +264,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "treepm_tree.npz"), **tree_out)
     diag_fixture(ref)
     pk_fixture(ref)
+    ic_fixture(ref)
     print(f"c1 reference evolution: {c['steps']} steps in {secs:.2f} s")
 
 
