@@ -9,6 +9,13 @@ inputs: no public dataset is involved.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp64|fp32]
                     [--config c1|c2|c3|c3h] [--impl ours|reference]
+    python bench.py --workload ic [--steps K] [--warmup W]
+
+`--workload ic` times HYOWON's generated initial conditions instead (the
+Philox Fourier field and 2LPT of the 512^3 lattice on the automatic 1024^3 IC
+mesh, L = 1000, z = 49): a "step" is one whole generation through
+hyowon_pm_generate_ics into device-resident state (work arrays and cuFFT
+plans included); `e2e` the same through hyowon_ic_generate into host arrays.
 
 Prints one JSON line (rank 0). `value` = particle-steps/s over the K timed steps
 with the state resident in HBM, timed with CUDA events on the library's stream
@@ -47,6 +54,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="step", choices=["step", "ic"])
     return ap.parse_args()
 
 
@@ -262,9 +270,98 @@ def cpu_baseline_sample(cfg_name):
                       f"{c['mesh']}^3 mesh) on all host threads"}
 
 
+IC_WORKLOAD = dict(n_side=512, box=1000.0, z_start=49.0, seed=7, lpt_order=2)
+IC_SAMPLE = dict(n_side=128, box=250.0)  # the CPU sample: same cell size, 1/64 of the volume
+
+
+def ic_params(n_side, box, seed, order=2):
+    from hyowon_b200 import ic
+    a0 = 1.0 / (1.0 + IC_WORKLOAD["z_start"])
+    p = ic.ICParams(n_side, box, seed, a0, lpt_order=order)
+    return p, ic.power_table(p, ic.start_spectrum(a0))
+
+
+def ic_cpu_baseline():
+    """The reference's RandomField + LPTDisplacement (oracle/_ref) on the host
+    cores for the 64^3 lattice, 2LPT, 128^3 IC mesh (same cell size)."""
+    try:
+        from hyowon_b200 import ic
+        from oracle.bindings import Reference, write_power_spectrum_file
+        ref = Reference()
+    except Exception as e:  # pragma: no cover
+        return {"value": None, "unit": "particles/s", "cores": os.cpu_count(),
+                "kind": "reference", "sample": f"unavailable: {e}"}
+    k, P = ic.bbks_table()
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "pk.txt")
+        write_power_spectrum_file(path, k, P, 0.0)
+        n = IC_SAMPLE["n_side"]
+        t0 = time.perf_counter()
+        ref.generate_ics(IC_SAMPLE["box"], n, path, 0.0, IC_WORKLOAD["z_start"],
+                         IC_WORKLOAD["seed"], lpt_order=2)
+        secs = time.perf_counter() - t0
+    return {"value": n ** 3 / secs, "unit": "particles/s", "cores": os.cpu_count(),
+            "kind": "reference",
+            "sample": f"one 2LPT generation of a {n}^3 lattice on the {2 * n}^3 IC mesh "
+                      f"(L = {IC_SAMPLE['box']}), all host threads, {secs:.2f} s"}
+
+
+def run_ic(args, rank):
+    """Generated-IC workload (see the module docstring)."""
+    if rank != 0:
+        return
+    import hyowon_b200 as hb
+    from hyowon_b200 import ic
+    w = IC_WORKLOAD
+    p, power = ic_params(w["n_side"], w["box"], w["seed"], w["lpt_order"])
+    M, K = p.resolve()
+    n = w["n_side"] ** 3
+    m_p = ic.particle_mass(w["box"], w["n_side"])
+    solver = hb.PMSolver(hb.MeshGeometry(w["box"], 1024), hb.PMForceMethod.pure_pm(False))
+    for _ in range(args.warmup):
+        solver.generate_ics(p, power, m_p)
+    with ClockSampler() as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            solver.generate_ics(p, power, m_p)
+        secs = time.perf_counter() - t0
+    solver.close()
+    ms = 1e3 * secs / args.steps
+    host = {k: np.empty(n) for k in ("x", "y", "z", "px", "py", "pz")}
+    # e2e: the standalone call into host arrays (device -> host copy inside)
+    ic.generate_ics(p, power)
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        host = ic.generate_ics(p, power)
+    e2e_s = (time.perf_counter() - t0) / max(1, args.steps // 2)
+    launches = 1 + 1 + 3 * 2 + (7 * 2 + 3 * 2 if w["lpt_order"] == 2 else 0)
+    line = {
+        "metric": "IC particles/s", "value": n / (ms * 1e-3), "unit": "particles/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"generated ICs: {w['n_side']}^3 lattice, {w['lpt_order']}LPT on "
+                               f"the {M}^3 IC mesh, K = {K}", "box": w["box"],
+                   "z_start": w["z_start"], "seed": w["seed"],
+                   "l2": "IC mesh fields (8.6 GB each) >> 126 MB L2",
+                   "timing": "wall clock around the synchronous call (device work, work-array "
+                             "allocation and cuFFT plans)"},
+        "cpu_baseline": None if args.no_cpu_baseline else ic_cpu_baseline(),
+        "e2e": {"value": n / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": 8 * power.size,
+                "d2h_bytes_per_step": 6 * 8 * n},
+        "gpu_launches": launches * args.steps,
+        "clocks": clk.summary(),
+        "check": {"x_range": [float(host["x"].min()), float(host["x"].max())]},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = setup_dist()
+    if args.workload == "ic":
+        run_ic(args, rank)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         return
