@@ -14,25 +14,28 @@
 // is the device log / sin / cos of Box-Muller (a few ulp).
 //
 // LPT (LPTDisplacement::apply_to_arrays, src/ic/lpt_displacement.cpp:150-520):
-// per axis a, psi_k = (-Im d, Re d) k_a/k^2 (k_a = 0 on axis a's Nyquist
-// plane), cuFFT Z2D, times 1/M^3, sampled at node (i, j, k) M/N and applied
-// as x = wrap(x + x_f psi), p = p + p_f psi. 2LPT: the seven fields
-// H_xx, H_yy, H_zz, H_xy, H_xz, H_yz (k_a k_b / k^2, mixed terms 0 on either
-// Nyquist plane) and tr H (d with k = 0 removed) are transformed one at a time
-// and folded into the source S = -1/2 H_aa^2 ... - H_ab^2 ... + 1/2 (tr H)^2 in
-// the reference's order; D2Z of S, the Cartesian band limit
-// (src/ic/particle_lattice_bandlimit.cpp:42-80) fused into
+// per axis a, psi_k = (-Im d, Re d) k_a/k^2, inverse transform times 1/M^3,
+// sampled at lattice node (i, j, k) M/N and applied as x = wrap(x + x_f psi),
+// p = p + p_f psi. The displacement spectra are zero outside the support
+// |m_i| <= K < N/2, so their lattice samples are the N^3 inverse transform of
+// the same modes (k_displacement): 8x less transform work than the M^3
+// inverse when M = 2N, same values up to rounding. 2LPT: the six Hessian
+// fields H_ab = c2r(d k_a k_b / k^2) (mixed terms 0 on either Nyquist plane)
+// are transformed one at a time and folded into
+// S = Hxx Hyy + (Hxx + Hyy) Hzz - Hxy^2 - Hxz^2 - Hyz^2, which is the
+// reference's -1/2 sum H_aa^2 - sum H_ab^2 + 1/2 (tr H)^2 (tr H = d) without
+// its trace transform; D2Z of S, band limit |m_i| <= K, then
 // psi2_k = (Im S, -Re S) k_a/k^2. Wavenumbers are (2 pi m)/L
 // (include/cosmo_nbody/mesh/mesh_geometry.hpp:112-115).
 //
-// Compiled with --fmad=false: every product and sum is rounded as the
-// reference's -ffp-contract=off build rounds it, so the spectral multipliers,
-// the source and the particle update are the reference's expressions; only the
-// FFT's rounding differs.
+// Compiled with --fmad=false: the spectral multipliers and the particle
+// update are the reference's expressions, rounded as its -ffp-contract=off
+// build rounds them; the transforms (cuFFT) and the source's summation order
+// round differently, at the level of the last bits.
 //
-// HBM traffic per mode / cell is a few words in each kernel; the O(M^3 log M)
-// transforms (cuFFT, FP64) dominate: 1LPT = 3 Z2D, 2LPT = 3 + 7 + 3 Z2D + 1
-// D2Z on the IC mesh.
+// HBM traffic per mode / cell is a few words in each kernel; the FP64
+// transforms dominate: 1LPT = 3 Z2D of N^3; 2LPT = 6 Z2D + 1 D2Z of M^3 and
+// 6 Z2D of N^3.
 #include <cfloat>
 #include <climits>
 #include <cmath>
@@ -166,43 +169,80 @@ __global__ void k_field(int M, int K, uint64_t seed, int fixed, int negate,
 
 // ------------------------------------------------------- spectral stages ----
 
-enum Stage : int { kPsi1 = 0, kHessian = 1, kTrace = 2, kPsi2 = 3 };
+// Half-spectrum coordinates of element idx with the index type I (32-bit
+// whenever the spectrum has fewer than 2^32 elements: cheaper division).
+template <typename I>
+__device__ __forceinline__ void half_coords(I idx, I M, I hz, int& i, int& j, int& k) {
+    k = static_cast<int>(idx % hz);
+    const I t = idx / hz;
+    j = static_cast<int>(t % M);
+    i = static_cast<int>(t / M);
+}
 
-// dst from src for one stage. Psi1 / Psi2: axis a; Hessian: axes (a, b);
-// Psi2 also applies the band limit |m_i| <= K to the source.
-__global__ void k_spectral(int M, double L, int stage, int a, int b, int K,
-                           const double2* __restrict__ src, double2* __restrict__ dst) {
-    const uint64_t total = static_cast<uint64_t>(M) * M * (M / 2 + 1);
-    const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+__device__ __forceinline__ double wavenumber(int m, double L) {
+    return kTwoPi * static_cast<double>(m) / L;
+}
+
+// Hessian (a, b) of the field: dst = src * (k_a k_b / k^2), the mixed terms 0
+// on either axis's Nyquist plane (include/cosmo_nbody/mesh/fourier_hessian.hpp).
+template <typename I>
+__global__ void k_hessian(int M, double L, int a, int b, const double2* __restrict__ src,
+                          double2* __restrict__ dst) {
+    const I total = static_cast<I>(M) * static_cast<I>(M) * static_cast<I>(M / 2 + 1);
+    const I idx = static_cast<I>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= total) return;
     int i, j, k;
-    half_index(idx, M, i, j, k);
-    const int m[3] = {mode_number(i, M), mode_number(j, M), mode_number(k, M)};
-    const bool even = (M & 1) == 0;
-    const bool nyq[3] = {even && i == M / 2, even && j == M / 2, even && k == M / 2};
-    double kc[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) kc[d] = kTwoPi * static_cast<double>(m[d]) / L;
-    const double k2 = kc[0] * kc[0] + kc[1] * kc[1] + kc[2] * kc[2];
-    if (stage == kTrace) {
-        dst[idx] = idx == 0 ? make_double2(0.0, 0.0) : src[idx];
-        return;
-    }
+    half_coords<I>(idx, static_cast<I>(M), static_cast<I>(M / 2 + 1), i, j, k);
+    const double kx = wavenumber(mode_number(i, M), L);
+    const double ky = wavenumber(mode_number(j, M), L);
+    const double kz = wavenumber(mode_number(k, M), L);
+    const double k2 = kx * kx + ky * ky + kz * kz;
     if (k2 == 0.0) {
         dst[idx] = make_double2(0.0, 0.0);
         return;
     }
-    double2 v = src[idx];
-    if (stage == kHessian) {
-        const double num = (a != b && (nyq[a] || nyq[b])) ? 0.0 : kc[a] * kc[b];
-        const double q = num / k2;
-        dst[idx] = make_double2(v.x * q, v.y * q);
+    const bool even = (M & 1) == 0;
+    const int ia = a == 0 ? i : (a == 1 ? j : k);
+    const int ib = b == 0 ? i : (b == 1 ? j : k);
+    const double ka = a == 0 ? kx : (a == 1 ? ky : kz);
+    const double kb = b == 0 ? kx : (b == 1 ? ky : kz);
+    const bool mixed_nyquist = a != b && even && (ia == M / 2 || ib == M / 2);
+    const double num = mixed_nyquist ? 0.0 : ka * kb;
+    const double q = num / k2;
+    const double2 v = src[idx];
+    dst[idx] = make_double2(v.x * q, v.y * q);
+}
+
+// Displacement spectrum of axis a on the particle lattice's own N^3 mesh.
+// The IC mesh field src (M^3 half spectrum) is zero outside the Cartesian
+// support |m_i| <= K < N/2, so every retained mode has one image on the
+// lattice mesh and the N^3 inverse transform of the restricted spectrum is
+// exactly the M^3 inverse sampled at the lattice nodes (i, j, k) M/N.
+// first: psi_k = (-Im d, Re d) k_a/k^2; second (2LPT, source S band-limited to
+// K): (Im S, -Re S) k_a/k^2. Nyquist planes of the IC mesh lie outside the
+// support (K < N/2 <= M/2), where k_a would be 0.
+template <typename I>
+__global__ void k_displacement(int N, int M, double L, int a, int K, bool second,
+                               const double2* __restrict__ src, double2* __restrict__ dst) {
+    const I total = static_cast<I>(N) * static_cast<I>(N) * static_cast<I>(N / 2 + 1);
+    const I idx = static_cast<I>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    int i, j, k;
+    half_coords<I>(idx, static_cast<I>(N), static_cast<I>(N / 2 + 1), i, j, k);
+    const int mx = mode_number(i, N), my = mode_number(j, N), mz = k;
+    if (abs(mx) > K || abs(my) > K || mz > K || (mx == 0 && my == 0 && mz == 0)) {
+        dst[idx] = make_double2(0.0, 0.0);
         return;
     }
-    if (stage == kPsi2 && (abs(m[0]) > K || abs(m[1]) > K || abs(m[2]) > K)) v = make_double2(0.0, 0.0);
-    const double kd = nyq[a] ? 0.0 : kc[a];
+    const uint64_t hz = static_cast<uint64_t>(M / 2 + 1);
+    const uint64_t at = (static_cast<uint64_t>(mx < 0 ? mx + M : mx) * M +
+                         static_cast<uint64_t>(my < 0 ? my + M : my)) * hz + static_cast<uint64_t>(mz);
+    const double kx = wavenumber(mx, L), ky = wavenumber(my, L), kz = wavenumber(mz, L);
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double kd = a == 0 ? kx : (a == 1 ? ky : kz);
     const double f = kd / k2;
-    dst[idx] = stage == kPsi1 ? make_double2(-v.y * f, v.x * f) : make_double2(v.y * f, -v.x * f);
+    const double2 v = src[at];
+    dst[idx] = second ? make_double2(v.y * f, -v.x * f) : make_double2(-v.y * f, v.x * f);
 }
 
 // ------------------------------------------------------------ real stages ----
@@ -225,20 +265,15 @@ __global__ void k_lattice(int N, double dx, double* __restrict__ x, double* __re
     pz[p] = 0.0;
 }
 
-// apply_lpt_component_update (src/ic/lpt_displacement.cpp:101-128) at the
-// lattice node of each particle; a non-finite psi or candidate leaves the
-// particle unchanged and raises `flag`.
-__global__ void k_apply(int N, int M, const double* __restrict__ field, double norm, double xf,
+// apply_lpt_component_update (src/ic/lpt_displacement.cpp:101-128): particle p
+// sits on lattice node p of the N^3 displacement field; a non-finite psi or
+// candidate leaves it unchanged and raises `flag`.
+__global__ void k_apply(uint64_t n, const double* __restrict__ field, double norm, double xf,
                         double pf, double L, double* __restrict__ pos, double* __restrict__ mom,
                         unsigned int flag, unsigned int* status) {
-    const uint64_t total = static_cast<uint64_t>(N) * N * N;
     const uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (p >= total) return;
-    const uint64_t r = static_cast<uint64_t>(M / N);
-    const uint64_t k = p % N;
-    const uint64_t j = (p / N) % N;
-    const uint64_t i = p / (static_cast<uint64_t>(N) * N);
-    const double psi = field[((i * r) * M + j * r) * M + k * r] * norm;
+    if (p >= n) return;
+    const double psi = field[p] * norm;
     const double disp = xf * psi;
     const double dmom = pf * psi;
     const double xc = pos[p] + disp;
@@ -253,27 +288,34 @@ __global__ void k_apply(int N, int M, const double* __restrict__ field, double n
     mom[p] = mc;
 }
 
-// Folds one normalised field into the 2LPT source in the reference's order:
-// op 0: S = -(1/2 h h); 1: S -= 1/2 h h; 2: S -= h h; 3: S += 1/2 t t.
+// The 2LPT source as the second invariant of the Hessian minus the mixed
+// squares, S = Hxx Hyy + (Hxx + Hyy) Hzz - Hxy^2 - Hxz^2 - Hyz^2: equal to the
+// reference's -1/2 sum H_aa^2 - sum H_ab^2 + 1/2 (tr H)^2 with tr H = sum H_aa
+// (its Hessian keeps k_a^2 on Nyquist planes), one transform fewer and no
+// cancellation between the trace and diagonal squares. One normalised field
+// h per launch: op 0 (xx): A = h; 1 (yy): S = A h, A += h; 2 (zz): S += A h;
+// 3 (mixed): S -= h h; the last launch checks S.
 __global__ void k_source(uint64_t n, const double* __restrict__ field, double norm, int op,
-                         double* __restrict__ src, unsigned int* status) {
+                         bool last, double* __restrict__ acc, double* __restrict__ src,
+                         unsigned int* status) {
     const uint64_t c = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (c >= n) return;
     const double h = field[c] * norm;
-    if (op < 3 && !isfinite(h)) raise_status(status, IC_HESSIAN);
+    if (!isfinite(h)) raise_status(status, IC_HESSIAN);
     double s;
     if (op == 0) {
-        const double term = 0.5 * h * h;
-        s = -term;
+        acc[c] = h;
+        return;
     } else if (op == 1) {
-        const double term = 0.5 * h * h;
-        s = src[c] - term;
+        const double a = acc[c];
+        s = a * h;
+        acc[c] = a + h;
     } else if (op == 2) {
-        s = src[c] - h * h;
+        s = src[c] + acc[c] * h;
     } else {
-        s = src[c] + 0.5 * h * h;
-        if (!isfinite(s)) raise_status(status, IC_SOURCE);
+        s = src[c] - h * h;
     }
+    if (last && !isfinite(s)) raise_status(status, IC_SOURCE);
     src[c] = s;
 }
 
@@ -514,52 +556,75 @@ int field_device(const Params& p, const double2* d_amp, double2* d_modes, unsign
 int generate_device(const Params& p, const double2* d_amp, double* const d_pos[3],
                     double* const d_mom[3], unsigned int* d_status, cudaStream_t s,
                     const char** err) {
-    const int M = p.M;
+    const int M = p.M, N = p.N;
     const uint64_t half = static_cast<uint64_t>(M) * M * (M / 2 + 1);
     const uint64_t cells = static_cast<uint64_t>(M) * M * M;
-    const uint64_t n = static_cast<uint64_t>(p.N) * p.N * p.N;
+    const uint64_t n = static_cast<uint64_t>(N) * N * N;
+    const uint64_t half_n = static_cast<uint64_t>(N) * N * (N / 2 + 1);
+    const bool folded = M != N;
     const double norm = 1.0 / (static_cast<double>(M) * M * M);
-    DeviceBuffer<double2> delta, work;
-    DeviceBuffer<double> field, source;
-    if (!delta.alloc(half) || !work.alloc(half) || !field.alloc(cells) ||
-        (p.order == 2 && !source.alloc(cells)))
+    const bool small_m = half < (1ull << 32), small_n = half_n < (1ull << 32);
+    // delta (M half spectrum) stays; work / field serve the Hessians (M) and,
+    // when M == N, the displacements; psi_n / field_n hold the folded N^3
+    // displacements otherwise. acc / source: the 2LPT source terms.
+    DeviceBuffer<double2> delta, work, psi_n;
+    DeviceBuffer<double> field, field_n, acc, source;
+    const bool second = p.order == 2;
+    if (!delta.alloc(half) || (second && (!work.alloc(half) || !field.alloc(cells))) ||
+        (second && (!acc.alloc(cells) || !source.alloc(cells))) ||
+        ((folded || !second) && (!psi_n.alloc(half_n) || !field_n.alloc(n))))
         return *err = "IC mesh work arrays could not be allocated", HYOWON_ENOMEM;
-    Fft fft;
-    int rc = fft.make(M, p.order == 2, s, err);
-    if (rc) return rc;
-    auto c2r = [&](double2* in) {
-        return cufftExecZ2D(fft.c2r, reinterpret_cast<cufftDoubleComplex*>(in), field.p) ==
-               CUFFT_SUCCESS;
+    // M == N with 2LPT: the displacements reuse the Hessian buffers
+    double2* const disp_k = psi_n.p ? psi_n.p : work.p;
+    double* const disp_r = field_n.p ? field_n.p : field.p;
+    Fft fft_m, fft_n;
+    int rc = 0;
+    if (second && (rc = fft_m.make(M, true, s, err))) return rc;
+    if ((folded || !second) && (rc = fft_n.make(N, false, s, err))) return rc;
+    const cufftHandle c2r_n = (folded || !second) ? fft_n.c2r : fft_m.c2r;
+
+    auto displacements = [&](const double2* src, bool second_order, double xf, double pf,
+                             unsigned int flag) -> int {
+        for (int a = 0; a < 3; ++a) {
+            if (small_n)
+                k_displacement<uint32_t><<<grid(half_n), 256, 0, s>>>(N, M, p.L, a, p.K,
+                                                                      second_order, src, disp_k);
+            else
+                k_displacement<uint64_t><<<grid(half_n), 256, 0, s>>>(N, M, p.L, a, p.K,
+                                                                      second_order, src, disp_k);
+            if (cufftExecZ2D(c2r_n, reinterpret_cast<cufftDoubleComplex*>(disp_k), disp_r) !=
+                CUFFT_SUCCESS)
+                return *err = "IC c2r failed", HYOWON_ECUDA;
+            k_apply<<<grid(n), 256, 0, s>>>(n, disp_r, norm, xf, pf, p.L, d_pos[a], d_mom[a],
+                                            flag, d_status);
+        }
+        return HYOWON_OK;
     };
-    k_lattice<<<grid(n), 256, 0, s>>>(p.N, p.L / static_cast<double>(p.N), d_pos[0], d_pos[1],
+
+    k_lattice<<<grid(n), 256, 0, s>>>(N, p.L / static_cast<double>(N), d_pos[0], d_pos[1],
                                       d_pos[2], d_mom[0], d_mom[1], d_mom[2]);
     if ((rc = field_device(p, d_amp, delta.p, d_status, s, err))) return rc;
-    for (int a = 0; a < 3; ++a) {
-        k_spectral<<<grid(half), 256, 0, s>>>(M, p.L, kPsi1, a, a, p.K, delta.p, work.p);
-        if (!c2r(work.p)) return *err = "IC c2r failed", HYOWON_ECUDA;
-        k_apply<<<grid(n), 256, 0, s>>>(p.N, M, field.p, norm, 1.0, p.p1, p.L, d_pos[a], d_mom[a],
-                                        IC_PSI1, d_status);
-    }
-    if (p.order == 2) {
-        static const int pairs[7][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}, {-1, -1}};
-        for (int t = 0; t < 7; ++t) {
-            const bool trace = t == 6;
-            k_spectral<<<grid(half), 256, 0, s>>>(M, p.L, trace ? kTrace : kHessian,
-                                                  trace ? 0 : pairs[t][0], trace ? 0 : pairs[t][1],
-                                                  p.K, delta.p, work.p);
-            if (!c2r(work.p)) return *err = "IC c2r failed", HYOWON_ECUDA;
-            const int op = trace ? 3 : (t == 0 ? 0 : (t < 3 ? 1 : 2));
-            k_source<<<grid(cells), 256, 0, s>>>(cells, field.p, norm, op, source.p, d_status);
+    if ((rc = displacements(delta.p, false, 1.0, p.p1, IC_PSI1))) return rc;
+    if (second) {
+        static const int pairs[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+        for (int t = 0; t < 6; ++t) {
+            if (small_m)
+                k_hessian<uint32_t><<<grid(half), 256, 0, s>>>(M, p.L, pairs[t][0], pairs[t][1],
+                                                               delta.p, work.p);
+            else
+                k_hessian<uint64_t><<<grid(half), 256, 0, s>>>(M, p.L, pairs[t][0], pairs[t][1],
+                                                               delta.p, work.p);
+            if (cufftExecZ2D(fft_m.c2r, reinterpret_cast<cufftDoubleComplex*>(work.p), field.p) !=
+                CUFFT_SUCCESS)
+                return *err = "IC c2r failed", HYOWON_ECUDA;
+            k_source<<<grid(cells), 256, 0, s>>>(cells, field.p, norm, t < 3 ? t : 3, t == 5,
+                                                 acc.p, source.p, d_status);
         }
-        if (cufftExecD2Z(fft.r2c, source.p, reinterpret_cast<cufftDoubleComplex*>(work.p)) !=
+        // S -> S_k in the delta buffer (delta is no longer needed)
+        if (cufftExecD2Z(fft_m.r2c, source.p, reinterpret_cast<cufftDoubleComplex*>(delta.p)) !=
             CUFFT_SUCCESS)
             return *err = "IC r2c of the 2LPT source failed", HYOWON_ECUDA;
-        for (int a = 0; a < 3; ++a) {
-            k_spectral<<<grid(half), 256, 0, s>>>(M, p.L, kPsi2, a, a, p.K, work.p, delta.p);
-            if (!c2r(delta.p)) return *err = "IC c2r failed", HYOWON_ECUDA;
-            k_apply<<<grid(n), 256, 0, s>>>(p.N, M, field.p, norm, p.x2, p.p2, p.L, d_pos[a],
-                                            d_mom[a], IC_PSI2, d_status);
-        }
+        if ((rc = displacements(delta.p, true, p.x2, p.p2, IC_PSI2))) return rc;
     }
     if (cudaStreamSynchronize(s) != cudaSuccess) return *err = "IC kernels failed", HYOWON_ECUDA;
     return HYOWON_OK;
