@@ -57,7 +57,8 @@ class Diagnostics(ctypes.Structure):
     _fields_ = [("potential_energy_comoving", c_double), ("kinetic_energy", c_double),
                 ("momentum", c_double * 3), ("mass_weighted_force", c_double * 3),
                 ("force_norm_sum", c_double), ("force_balance", c_double),
-                ("momentum_force_contraction", c_double)]
+                ("momentum_force_contraction", c_double),
+                ("directional_potential_energy_comoving", c_double)]
 
 
 class PkBin(ctypes.Structure):

@@ -32,6 +32,13 @@ struct PMForceDiagnostics {
     double potential_energy_comoving = 0.0;
 };
 
+// gravity::PMPostForceEnergyDiagnostics (include/cosmo_nbody/gravity/pm_solver.hpp:37-46),
+// the single-process fields.
+struct PMPostForceEnergyDiagnostics {
+    double potential_energy_comoving = 0.0;
+    double directional_potential_energy_comoving = 0.0;
+};
+
 enum class Method { PurePM = HYOWON_PURE_PM, TreePMLongRange = HYOWON_TREEPM_LONG_RANGE };
 enum class Precision { FP64 = HYOWON_FP64, FP32Fixed = HYOWON_FP32_FIXED };
 
@@ -109,6 +116,19 @@ public:
         hyowon_pm_diagnostics_t d{};
         check(hyowon_pm_diagnostics(h_, a, &d));
         return d;
+    }
+
+    // PMSolver::measure_post_force_energy_diagnostics_in_place
+    // (src/gravity/pm_post_force_energy_diagnostics.cpp:17-100) on the device
+    // state: the potential of the last force solve at the current positions,
+    // directional derivative along the current momenta. Pure PM only, as in
+    // the reference (std::logic_error otherwise).
+    PMPostForceEnergyDiagnostics measure_post_force_energy_diagnostics() const {
+        const hyowon_pm_diagnostics_t d = diagnostics(1.0);
+        if (d.directional_potential_energy_comoving != d.directional_potential_energy_comoving)
+            throw std::logic_error(
+                "PMSolver post-force energy diagnostic is defined only for pure PM");
+        return {d.potential_energy_comoving, d.directional_potential_energy_comoving};
     }
 
     // ParticleStore -> device. Momenta may be empty (zero).

@@ -10,6 +10,10 @@
 //                                      (force balance |F| / S,
 //                                       include/cosmo_nbody/validation/force_balance_diagnostics.hpp:19-27)
 //   C  = sum_i m_i p_i . a_i           (ConservationChecks::compute_momentum_force_contraction)
+//   D  = sum_i m_i p_i . grad_S phi(x_i) (the directional derivative of the CIC
+//                                       particle-position energy along the
+//                                       momenta; PMPostForceEnergyDiagnostics,
+//                                       src/gravity/pm_post_force_energy_diagnostics.cpp:17-100)
 // in binary64 for both arithmetic forms (the precision form widens its FP32
 // momenta, accelerations and potential and its fixed-point positions exactly).
 //
@@ -19,6 +23,13 @@
 // value = sum over the 8 corners (x, y, z offsets in that nesting) of
 // phi * ((wx * wy) * wz), then m * value. This unit is compiled with
 // --fmad=false so those products are not contracted.
+//
+// The gradient of D is the derivative of the CIC weights, one-sided per cell
+// (CICMassAssignment::interpolate_mass_weighted_directional_derivative,
+// src/mesh/mass_assignment_directional.cpp:133-166): g_x = sum over (y, z)
+// corners of (phi[x+1] - phi[x]) * w_y * w_z, likewise for y and z, times
+// 1 / dx; then m (p . g). The reference forms g in long double; here it is
+// binary64 (agreement to rounding of each term).
 //
 // The sums are deterministic run to run: a fixed grid of kBlocks blocks, each
 // thread accumulating a grid-stride subsequence with Neumaier compensation,
@@ -88,10 +99,29 @@ __device__ __forceinline__ void store_partial(const Acc (&acc)[kTerms], double* 
     }
 }
 
-// Per-particle terms shared by both forms; `value` is the CIC sum of phi.
+// One-sided CIC-weight gradient of the 8 corner values v[x][y][z] (weights
+// w*[0] = 1 - f, w*[1] = f), dotted with p, times 1/dx.
+__device__ __forceinline__ double directional(const double (&v)[2][2][2], const double (&wx)[2],
+                                              const double (&wy)[2], const double (&wz)[2],
+                                              double inv_dx, double px, double py, double pz) {
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            gx += (v[1][a][b] - v[0][a][b]) * wy[a] * wz[b];
+            gy += (v[a][1][b] - v[a][0][b]) * wx[a] * wz[b];
+            gz += (v[a][b][1] - v[a][b][0]) * wx[a] * wy[b];
+        }
+    }
+    return px * (gx * inv_dx) + py * (gy * inv_dx) + pz * (gz * inv_dx);
+}
+
+// Per-particle terms shared by both forms; `value` is the CIC sum of phi and
+// `dir` the directional derivative along p.
 __device__ __forceinline__ void particle_terms(Acc (&acc)[kTerms], double m, double value,
-                                               double px, double py, double pz, double ax,
-                                               double ay, double az) {
+                                               double dir, double px, double py, double pz,
+                                               double ax, double ay, double az) {
     add(acc[0], m * value);
     add(acc[1], 0.5 * m * (px * px + py * py + pz * pz));
     add(acc[2], m * px);
@@ -102,6 +132,7 @@ __device__ __forceinline__ void particle_terms(Acc (&acc)[kTerms], double m, dou
     add(acc[7], m * az);
     add(acc[8], m * sqrt(ax * ax + ay * ay + az * az));
     add(acc[9], m * (px * ax + py * ay + pz * az));
+    add(acc[10], m * dir);
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -112,7 +143,7 @@ k_diag_f64(InputsF64 in, double* __restrict__ partial, unsigned int* status) {
     const int N = in.axis.N;
     for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < in.n; i += kBlocks * kThreads) {
         const double m = in.mass ? in.mass[i] : in.uniform_mass;
-        double value = 0.0;
+        double value = 0.0, dir = 0.0;
         if (in.phi) {
             int b[3];
             double f[3];
@@ -128,6 +159,7 @@ k_diag_f64(InputsF64 in, double* __restrict__ partial, unsigned int* status) {
             const double wy[2] = {1.0 - f[1], f[1]};
             const double wz[2] = {1.0 - f[2], f[2]};
             bool lost = false;
+            double v[2][2][2];
 #pragma unroll
             for (int ox = 0; ox < 2; ++ox) {
                 const size_t gx = static_cast<size_t>(wrap_index(b[0] + ox, N));
@@ -138,6 +170,7 @@ k_diag_f64(InputsF64 in, double* __restrict__ partial, unsigned int* status) {
                     for (int oz = 0; oz < 2; ++oz) {
                         const size_t gz = static_cast<size_t>(wrap_index(b[2] + oz, N));
                         const double fv = in.phi[(gx * N + gy) * N + gz];
+                        v[ox][oy][oz] = fv;
                         const double xy = wx[ox] * wy[oy];
                         const double w = xy * wz[oz];
                         if (w == 0.0 && wx[ox] != 0.0 && wy[oy] != 0.0 && wz[oz] != 0.0 && fv != 0.0
@@ -151,8 +184,10 @@ k_diag_f64(InputsF64 in, double* __restrict__ partial, unsigned int* status) {
             }
             if (lost || (m != 0.0 && value != 0.0 && m * value == 0.0))
                 raise_status(status, ST_UNDERFLOW);
+            dir = directional(v, wx, wy, wz, 1.0 / in.axis.dx, in.px[i], in.py[i], in.pz[i]);
         }
-        particle_terms(acc, m, value, in.px[i], in.py[i], in.pz[i], in.ax[i], in.ay[i], in.az[i]);
+        particle_terms(acc, m, value, dir, in.px[i], in.py[i], in.pz[i], in.ax[i], in.ay[i],
+                       in.az[i]);
     }
     block_merge(acc);
     store_partial(acc, partial);
@@ -167,7 +202,9 @@ k_diag_f32(InputsF32 in, double* __restrict__ partial) {
     const double m = in.uniform_mass;
     constexpr double kInv32 = 1.0 / 4294967296.0;
     for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < in.n; i += kBlocks * kThreads) {
-        double value = 0.0;
+        double value = 0.0, dir = 0.0;
+        const double px = static_cast<double>(in.px[i]), py = static_cast<double>(in.py[i]),
+                     pz = static_cast<double>(in.pz[i]);
         if (in.phi) {
             // u * N = cell * 2^32 + fraction * 2^32 exactly in 64 bits
             const unsigned long long qx = static_cast<unsigned long long>(in.ux[i]) * N;
@@ -181,6 +218,7 @@ k_diag_f32(InputsF32 in, double* __restrict__ partial) {
             const double wx[2] = {1.0 - f[0], f[0]};
             const double wy[2] = {1.0 - f[1], f[1]};
             const double wz[2] = {1.0 - f[2], f[2]};
+            double v[2][2][2];
 #pragma unroll
             for (int ox = 0; ox < 2; ++ox) {
                 const size_t gx = b[0] + ox == N ? 0 : b[0] + ox;
@@ -191,12 +229,14 @@ k_diag_f32(InputsF32 in, double* __restrict__ partial) {
                     for (int oz = 0; oz < 2; ++oz) {
                         const size_t gz = b[2] + oz == N ? 0 : b[2] + oz;
                         const double fv = static_cast<double>(in.phi[(gx * N + gy) * N + gz]);
+                        v[ox][oy][oz] = fv;
                         value += fv * ((wx[ox] * wy[oy]) * wz[oz]);
                     }
                 }
             }
+            dir = directional(v, wx, wy, wz, in.inv_dx, px, py, pz);
         }
-        particle_terms(acc, m, value, in.px[i], in.py[i], in.pz[i], in.ax[i], in.ay[i], in.az[i]);
+        particle_terms(acc, m, value, dir, px, py, pz, in.ax[i], in.ay[i], in.az[i]);
     }
     block_merge(acc);
     store_partial(acc, partial);

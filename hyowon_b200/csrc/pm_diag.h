@@ -12,8 +12,8 @@ namespace hyowon {
 namespace diag {
 
 // Terms, in this order: sum m phi, sum 0.5 m |p|^2, sum m p (3), sum m a (3),
-// sum m |a|, sum m p.a.
-constexpr int kTerms = 10;
+// sum m |a|, sum m p.a, sum m p . grad_S phi (one-sided CIC-weight gradient).
+constexpr int kTerms = 11;
 constexpr int kBlocks = 1024;   // fixed, so the summation order is too
 constexpr int kThreads = 256;
 
@@ -38,6 +38,7 @@ struct InputsF32 {
     double uniform_mass;
     const float* phi;       // real-space potential N^3, or null
     int N;
+    double inv_dx;          // 1 / cell size
 };
 
 // Enqueue the pass and the final combination; the kTerms results land at

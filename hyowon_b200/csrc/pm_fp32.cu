@@ -1218,6 +1218,7 @@ int diagnostics(State* st, cudaStream_t s, bool with_potential, double* scratch,
     in.uniform_mass = st->uniform_mass;
     in.phi = with_potential ? st->rmesh : nullptr;
     in.N = st->N;
+    in.inv_dx = static_cast<double>(st->N) / st->L;
     const int k = diag::launch_f32(in, scratch, s);
     if (k < 0) return fail(st, HYOWON_ECUDA, "diagnostics launch failed");
     st->launches += k;

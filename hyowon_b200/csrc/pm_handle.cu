@@ -1224,8 +1224,11 @@ int hyowon_pm_diagnostics(hyowon_pm_t h, double a, hyowon_pm_diagnostics_t* out)
     const double net = std::sqrt(r[5] * r[5] + r[6] * r[6] + r[7] * r[7]);
     out->force_balance = r[8] > 0.0 ? net / r[8] : 0.0;
     out->momentum_force_contraction = r[9];
-    for (int t = 1; t < diag::kTerms; ++t)
+    out->directional_potential_energy_comoving = with_phi ? r[10] : nan;
+    for (int t = 1; t < 10; ++t)
         if (!std::isfinite(r[t])) return fail(h, HYOWON_EOVERFLOW, "diagnostic sum is non-finite");
+    if (with_phi && !std::isfinite(r[10]))
+        return fail(h, HYOWON_EOVERFLOW, "PMSolver post-force energy diagnostic is non-finite");
     if (with_phi && !std::isfinite(out->potential_energy_comoving))
         return fail(h, HYOWON_EOVERFLOW, "PMSolver potential-energy diagnostic is non-finite");
     if (with_phi && r[0] != 0.0 && out->potential_energy_comoving == 0.0)

@@ -244,7 +244,8 @@ class PMSolver:
         """Binary64 global sums of the state at the last force solve
         (hyowon_pm_diagnostics): potential_energy_comoving, kinetic_energy
         (sum 0.5 m p^2 / a^2), momentum, mass_weighted_force, force_norm_sum,
-        force_balance (|sum m a| / sum m |a|), momentum_force_contraction."""
+        force_balance (|sum m a| / sum m |a|), momentum_force_contraction,
+        directional_potential_energy_comoving (sum m p . grad_S phi)."""
         d = nat.Diagnostics()
         self._check(nat.lib().hyowon_pm_diagnostics(self._h, float(a), ctypes.byref(d)),
                     "diagnostics")
@@ -253,7 +254,9 @@ class PMSolver:
                 "momentum": np.array(d.momentum[:]),
                 "mass_weighted_force": np.array(d.mass_weighted_force[:]),
                 "force_norm_sum": d.force_norm_sum, "force_balance": d.force_balance,
-                "momentum_force_contraction": d.momentum_force_contraction}
+                "momentum_force_contraction": d.momentum_force_contraction,
+                "directional_potential_energy_comoving":
+                    d.directional_potential_energy_comoving}
 
     def power_spectrum(self, num_bins: int, max_k_fraction_nyquist: float = 1.0,
                        subtract_shot_noise: bool = False, interlaced: bool = False,

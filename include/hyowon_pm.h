@@ -185,6 +185,12 @@ int hyowon_pm_last_timing(hyowon_pm_t h, double* times);
  *   momentum_force_contraction  sum_i m_i p_i . a_i
  *       (ConservationChecks::compute_momentum_force_contraction,
  *       include/cosmo_nbody/validation/conservation_checks.hpp).
+ *   directional_potential_energy_comoving  sum_i m_i p_i . grad_S phi(x_i), the
+ *       derivative of the CIC particle-position energy along the momenta with
+ *       the one-sided CIC-weight gradient (PMPostForceEnergyDiagnostics of
+ *       PMSolver::measure_post_force_energy_diagnostics_in_place,
+ *       src/gravity/pm_post_force_energy_diagnostics.cpp:17-100,
+ *       src/mesh/mass_assignment_directional.cpp:12-194); NaN for TreePM.
  * a is the scale factor of the state (finite, > 0). HYOWON_ELOGIC when no
  * force solve is valid for the current positions; HYOWON_EOVERFLOW for a
  * non-finite sum; HYOWON_EUNDERFLOW when a non-zero CIC product is lost
@@ -197,6 +203,7 @@ typedef struct hyowon_pm_diagnostics {
     double force_norm_sum;
     double force_balance;
     double momentum_force_contraction;
+    double directional_potential_energy_comoving;
 } hyowon_pm_diagnostics_t;
 int hyowon_pm_diagnostics(hyowon_pm_t h, double a, hyowon_pm_diagnostics_t* out);
 

@@ -223,6 +223,20 @@ class Reference:
         self._check(rc, "ref_pm_forces_energy")
         return ax, ay, az, e.value
 
+    def post_force_energy(self, L, N, x, y, z, px, py, pz, masses=None, uniform_mass=1.0,
+                          deconvolve=False):
+        """PMSolver::measure_post_force_energy_diagnostics_in_place after a force
+        solve: (potential_energy_comoving, directional_potential_energy_comoving)."""
+        n = len(x)
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z, px, py, pz)]
+        m = None if masses is None else np.ascontiguousarray(masses, dtype=np.float64)
+        out = np.zeros(2)
+        rc = self.lib.ref_post_force_energy(
+            _c_double(L), _c_u64(N), _c_int(int(deconvolve)), _c_u64(n), _dp(a[0]), _dp(a[1]),
+            _dp(a[2]), _dp(m), _c_double(uniform_mass), _dp(a[3]), _dp(a[4]), _dp(a[5]), _dp(out))
+        self._check(rc, "ref_post_force_energy")
+        return float(out[0]), float(out[1])
+
     def power_spectrum(self, L, mesh, x, y, z, masses=None, uniform_mass=1.0, num_bins=16,
                        subtract_shot_noise=False, interlaced=False, max_k_fraction_nyquist=1.0):
         """MatterPowerSpectrum::compute_pk: dict of per-bin arrays."""

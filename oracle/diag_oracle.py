@@ -83,3 +83,42 @@ def force_balance(ax, ay, az, masses):
 def momentum_force_contraction(px, py, pz, ax, ay, az, masses):
     m = np.broadcast_to(np.asarray(masses, dtype=np.float64), np.shape(px))
     return math.fsum(m * (px * ax + py * ay + pz * az))
+
+
+def directional_potential_energy(L, N, phi, base, frac, masses, px, py, pz):
+    """sum_i m_i p_i . grad_S phi(x_i) with the one-sided CIC-weight gradient
+    (CICMassAssignment::interpolate_mass_weighted_directional_derivative,
+    src/mesh/mass_assignment_directional.cpp:133-180): per axis the sum over
+    the other two axes' corners of (phi[+1] - phi[0]) w w, in long double,
+    times 1 / dx (long double); the per-particle term m (p . g) rounded to
+    binary64 (PMSolver::measure_post_force_energy_diagnostics_in_place,
+    src/gravity/pm_post_force_energy_diagnostics.cpp:67-100)."""
+    ld = np.longdouble
+    phi = np.asarray(phi, dtype=np.float64).reshape(N, N, N)
+    g = [(base[d] % N, (base[d] + 1) % N) for d in range(3)]
+    v = np.empty((2, 2, 2, base.shape[1]), dtype=ld)
+    for ox in (0, 1):
+        for oy in (0, 1):
+            for oz in (0, 1):
+                v[ox, oy, oz] = phi[g[0][ox], g[1][oy], g[2][oz]].astype(ld)
+    w = [np.stack([(1.0 - frac[d]), frac[d]]).astype(ld) for d in range(3)]
+    gx = np.zeros(base.shape[1], dtype=ld)
+    gy = np.zeros_like(gx)
+    gz = np.zeros_like(gx)
+    for a in (0, 1):
+        for b in (0, 1):
+            gx = gx + (v[1, a, b] - v[0, a, b]) * w[1][a] * w[2][b]
+    for a in (0, 1):
+        for b in (0, 1):
+            gy = gy + (v[a, 1, b] - v[a, 0, b]) * w[0][a] * w[2][b]
+    for a in (0, 1):
+        for b in (0, 1):
+            gz = gz + (v[a, b, 1] - v[a, b, 0]) * w[0][a] * w[1][b]
+    inv = ld(1.0) / ld(L / N)
+    gx, gy, gz = gx * inv, gy * inv, gz * inv
+    m = np.broadcast_to(np.asarray(masses, dtype=np.float64), gx.shape).astype(ld)
+    d = (np.asarray(px, dtype=np.float64).astype(ld) * gx
+         + np.asarray(py, dtype=np.float64).astype(ld) * gy
+         + np.asarray(pz, dtype=np.float64).astype(ld) * gz)
+    terms = (m * d).astype(np.float64)
+    return math.fsum(terms), math.fsum(np.abs(terms))

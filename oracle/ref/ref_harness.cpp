@@ -37,6 +37,7 @@
 #include "cosmo_nbody/time/time_stepper.hpp"
 #include "cosmo_nbody/validation/conservation_checks.hpp"
 #include "cosmo_nbody/validation/force_balance_diagnostics.hpp"
+#include "cosmo_nbody/runtime/evolution_pm_solver_handle.hpp"
 #include "mesh/cic_coordinate.hpp"
 
 #include <array>
@@ -220,6 +221,34 @@ int ref_pm_forces_energy(double L, std::uint64_t N, int deconvolve, std::uint64_
             std::span<double>(ay, n), std::span<double>(az, n), true);
         if (!d.has_value()) throw std::logic_error("no PMForceDiagnostics returned");
         *energy = d->potential_energy_comoving;
+    });
+}
+
+// The runner's path (src/runtime/simulation_runner.cpp:1182): an
+// EvolutionPMSolverHandle force refresh, then
+// measure_post_force_energy_diagnostics -> PMSolver::
+// measure_post_force_energy_diagnostics_in_place
+// (src/gravity/pm_post_force_energy_diagnostics.cpp:17-100) with momenta
+// px..pz: out2 = {potential_energy_comoving, directional_potential_energy_comoving}.
+int ref_post_force_energy(double L, std::uint64_t N, int deconvolve, std::uint64_t n,
+                          const double* x, const double* y, const double* z,
+                          const double* masses, double uniform_mass, const double* px,
+                          const double* py, const double* pz, double* out2) {
+    return guarded([&] {
+        mesh::MeshGeometry geom(L, N);
+        runtime::EvolutionPMSolverHandle solver(std::make_unique<gravity::PMSolver>(
+            geom, mesh::PMForceMethod::pure_pm(deconvolve != 0), false,
+            config::MemoryPolicyParams{}));
+        std::vector<double> ax(n, 0.0), ay(n, 0.0), az(n, 0.0);
+        const std::span<const double> sx(x, n), sy(y, n), sz(z, n);
+        solver.compute_forces(sx, sy, sz, mass_span(masses, n),
+                              uniform_or_none(masses, uniform_mass), ax, ay, az, false);
+        const auto d = solver.measure_post_force_energy_diagnostics(
+            sx, sy, sz, mass_span(masses, n), uniform_or_none(masses, uniform_mass),
+            std::span<const double>(px, n), std::span<const double>(py, n),
+            std::span<const double>(pz, n));
+        out2[0] = d.potential_energy_comoving;
+        out2[1] = d.directional_potential_energy_comoving;
     });
 }
 

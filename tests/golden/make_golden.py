@@ -20,20 +20,22 @@ Fixtures:
                       steps of the reference integrator
   c1_diag.npz         global diagnostics of the reference at the c1 ICs and after
                       32 steps (PMForceDiagnostics potential energy, kinetic
-                      energy, force balance, momentum-force contraction) and the
-                      potential energy / force balance of small_pm with masses
+                      energy, force balance, momentum-force contraction, the
+                      post-force directional energy derivative) and the
+                      potential energy / force balance / directional derivative
+                      of small_pm with masses
 
   pk.npz              MatterPowerSpectrum::compute_pk of the c1 states (own mesh
                       64 and 32; raw, shot-noise-subtracted, interlaced) and of
                       small_pm with explicit masses
 
-    python tests/golden/make_golden.py --only diag    # c1_diag.npz alone
   ic.npz              generated initial conditions of the reference
                       (RandomField::generate + LPTDisplacement::apply_to_arrays
                       on the corner lattice, IC_CASES: 1LPT / 2LPT, gaussian /
                       fixed, pairings, explicit K and mesh), the P(k) table
                       they read, Philox4x32-10 blocks and per-mode draws
 
+    python tests/golden/make_golden.py --only diag    # c1_diag.npz alone
     python tests/golden/make_golden.py --only pk      # pk.npz alone
     python tests/golden/make_golden.py --only ic      # ic.npz alone
 """
@@ -79,11 +81,18 @@ def diag_fixture(ref):
         out.update({tag + "_a": a, tag + "_potential_energy": e, tag + "_kinetic_energy": K,
                     tag + "_momentum_force_contraction": C,
                     tag + "_force_balance": ref.force_balance(ax, ay, az, uniform_mass=m)})
+        pe, de = ref.post_force_energy(L, N, x, y, z, px, py, pz, uniform_mass=m)
+        out.update({tag + "_post_potential_energy": pe, tag + "_directional": de})
     sp = np.load(os.path.join(HERE, "small_pm.npz"))
     Ls, Ns = float(sp["L"]), int(sp["N"])
     ax, ay, az, e = ref.pm_forces_energy(Ls, Ns, sp["x"], sp["y"], sp["z"], masses=sp["masses"])
     out.update(small_masses_potential_energy=e,
                small_masses_force_balance=ref.force_balance(ax, ay, az, masses=sp["masses"]))
+    dr = np.random.default_rng(31)
+    spx, spy, spz = (dr.normal(0.0, 2.0, sp["x"].size) for _ in range(3))
+    _, de = ref.post_force_energy(Ls, Ns, sp["x"], sp["y"], sp["z"], spx, spy, spz,
+                                  masses=sp["masses"])
+    out.update(small_px=spx, small_py=spy, small_pz=spz, small_masses_directional=de)
     np.savez_compressed(os.path.join(HERE, "c1_diag.npz"), **out)
 
 

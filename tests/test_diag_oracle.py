@@ -49,3 +49,27 @@ def test_small_pm_masses_potential_energy(oracle, small_pm, c1_diag):
     phi, b, f = _phi(oracle, L, N, s["x"], s["y"], s["z"], masses=s["masses"])
     e = dg.potential_energy_comoving(L, N, phi, b, f, s["masses"])
     assert abs(e / float(c1_diag["small_masses_potential_energy"]) - 1) < 1e-13
+
+
+@pytest.mark.parametrize("tag", ["ic", "s32"])
+def test_directional_derivative_matches_reference(oracle, c1_kdk, c1_diag, tag):
+    """PMSolver::measure_post_force_energy_diagnostics_in_place: the one-sided
+    CIC-weight directional derivative along the momenta, within 1e-15 of
+    sum |term| (long-double per-particle terms as the reference forms them)."""
+    d, g = c1_kdk, c1_diag
+    L, N, m = float(d["box"]), int(d["mesh"]), float(d["particle_mass"])
+    x, y, z = d[tag + "_x"], d[tag + "_y"], d[tag + "_z"]
+    phi, b, f = _phi(oracle, L, N, x, y, z, uniform_mass=m)
+    v, scale = dg.directional_potential_energy(L, N, phi, b, f, m, d[tag + "_px"],
+                                               d[tag + "_py"], d[tag + "_pz"])
+    assert abs(v - float(g[tag + "_directional"])) <= 1e-15 * scale
+    assert float(g[tag + "_post_potential_energy"]) == float(g[tag + "_potential_energy"])
+
+
+def test_directional_derivative_masses(oracle, small_pm, c1_diag):
+    s_ = small_pm
+    L, N = float(s_["L"]), int(s_["N"])
+    phi, b, f = _phi(oracle, L, N, s_["x"], s_["y"], s_["z"], masses=s_["masses"])
+    v, scale = dg.directional_potential_energy(L, N, phi, b, f, s_["masses"], c1_diag["small_px"],
+                                               c1_diag["small_py"], c1_diag["small_pz"])
+    assert abs(v - float(c1_diag["small_masses_directional"])) <= 1e-15 * scale

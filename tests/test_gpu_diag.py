@@ -12,6 +12,9 @@ Tolerances:
   (binary64 sums of identical per-particle terms in another order);
 * after 32 c1 steps vs the reference: 1e-5 relative (positions differ by
   <= 1e-6 cell after 32 chaotic steps);
+* directional derivative sum m p . grad_S phi (sign-mixed): within 1e-12 of
+  the sum of its terms' magnitudes vs the reference and the oracle (1e-10 for
+  the precision form vs the oracle on its own state);
 * repeated calls: bit-identical (fixed reduction order).
 """
 import math
@@ -44,6 +47,8 @@ def oracle_of_state(oracle, L, N, st, phi, masses, a):
         "force_balance": dg.force_balance(st["ax"], st["ay"], st["az"], masses),
         "momentum_force_contraction": dg.momentum_force_contraction(
             st["px"], st["py"], st["pz"], st["ax"], st["ay"], st["az"], masses),
+        "directional": dg.directional_potential_energy(L, N, phi, b, f, masses, st["px"],
+                                                       st["py"], st["pz"]),
     }
 
 
@@ -57,6 +62,9 @@ def check_against(d, o, tol):
     assert np.max(np.abs(d["mass_weighted_force"] - o["mass_weighted_force"])) \
         <= 1e-12 * o["force_norm_sum"]
     assert abs(d["force_balance"] - o["force_balance"]) < 1e-12
+    # sign-mixed sum: bounded by the sum of the magnitudes of its terms
+    dv, scale = o["directional"]
+    assert abs(d["directional_potential_energy_comoving"] - dv) <= tol * scale
 
 
 def test_fp64_c1_ics_match_reference(oracle, c1_kdk, c1_diag):
@@ -76,6 +84,9 @@ def test_fp64_c1_ics_match_reference(oracle, c1_kdk, c1_diag):
     assert rel(r1["momentum_force_contraction"],
                float(g["ic_momentum_force_contraction"])) < 1e-12
     assert abs(r1["force_balance"] - float(g["ic_force_balance"])) < 1e-14
+    o = oracle_of_state(oracle, L, N, st, phi, m, a0)
+    assert abs(r1["directional_potential_energy_comoving"] - float(g["ic_directional"])) \
+        <= 1e-12 * o["directional"][1]
     for k in r1:
         assert np.array_equal(np.asarray(r1[k]), np.asarray(r2[k])), k
     check_against(r1, oracle_of_state(oracle, L, N, st, phi, m, a0), 1e-12)
@@ -103,7 +114,7 @@ def test_fp64_c1_after_32_steps(oracle, c1_kdk, c1_diag):
         assert rel(r[k], float(g[gk])) < 1e-5, (k, r[k], float(g[gk]))
 
 
-def test_fp64_explicit_masses_collect_potential_energy(small_pm, c1_diag):
+def test_fp64_explicit_masses_collect_potential_energy(oracle, small_pm, c1_diag):
     s_ = small_pm
     L, N = float(s_["L"]), int(s_["N"])
     n = s_["x"].size
@@ -117,6 +128,21 @@ def test_fp64_explicit_masses_collect_potential_energy(small_pm, c1_diag):
     assert rel(out["potential_energy_comoving"],
                float(c1_diag["small_masses_potential_energy"])) < 1e-12
     assert abs(r["force_balance"] - float(c1_diag["small_masses_force_balance"])) < 1e-14
+    # directional derivative along given momenta: upload them with the state
+    with hb.PMSolver(hb.MeshGeometry(L, N), hb.PMForceMethod.pure_pm(False)) as s:
+        s.upload(s_["x"], s_["y"], s_["z"], c1_diag["small_px"], c1_diag["small_py"],
+                 c1_diag["small_pz"], masses=s_["masses"])
+        s.solve_forces()
+        r = s.diagnostics(1.0)
+    _, phi = oracle.potential(L, N, s_["x"], s_["y"], s_["z"], masses=s_["masses"])
+    b = np.empty((3, n), dtype=np.int64)
+    f = np.empty((3, n))
+    for d, v in enumerate((s_["x"], s_["y"], s_["z"])):
+        b[d], f[d] = oracle.cic_coords(L, N, v)
+    _, scale = dg.directional_potential_energy(L, N, phi, b, f, s_["masses"], c1_diag["small_px"],
+                                               c1_diag["small_py"], c1_diag["small_pz"])
+    ref = float(c1_diag["small_masses_directional"])
+    assert abs(r["directional_potential_energy_comoving"] - ref) <= 1e-12 * scale
 
 
 def test_fp32_matches_oracle_on_its_state(oracle, c1_kdk):
@@ -157,4 +183,5 @@ def test_errors_and_treepm():
         s.solve_forces()
         r = s.diagnostics(1.0)
         assert math.isnan(r["potential_energy_comoving"])
+        assert math.isnan(r["directional_potential_energy_comoving"])
         assert math.isfinite(r["force_norm_sum"]) and r["force_norm_sum"] > 0
