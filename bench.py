@@ -334,7 +334,9 @@ def run_ic(args, rank):
     for _ in range(max(1, args.steps // 2)):
         host = ic.generate_ics(p, power)
     e2e_s = (time.perf_counter() - t0) / max(1, args.steps // 2)
-    launches = 1 + 1 + 3 * 2 + (7 * 2 + 3 * 2 if w["lpt_order"] == 2 else 0)
+    # lattice + field, 3 x (displacement + apply), 2LPT: 6 x (Hessian + source)
+    # and 3 x (displacement + apply); cuFFT's own kernels not counted
+    launches = 2 + 3 * 2 + (6 * 2 + 3 * 2 if w["lpt_order"] == 2 else 0)
     line = {
         "metric": "IC particles/s", "value": n / (ms * 1e-3), "unit": "particles/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,

@@ -219,7 +219,24 @@ __device__ __forceinline__ void store_cell(long long* out, long long q) { *out =
 // counted exactly once. Threads walk the concatenated segments
 // kDepositBatch particles at a time.
 constexpr int kDepositThreads = 256;
-constexpr int kDepositBatch = 4;
+#ifndef HYOWON_DEPOSIT_BATCH
+#define HYOWON_DEPOSIT_BATCH 4
+#endif
+constexpr int kDepositBatch = HYOWON_DEPOSIT_BATCH;
+
+// Adds w to a shared-memory int64 accumulator. HYOWON_DEPOSIT_RED selects the
+// reduction form (red.shared.add.u64: no value returned) over atomicAdd.
+#ifndef HYOWON_DEPOSIT_RED
+#define HYOWON_DEPOSIT_RED 0
+#endif
+__device__ __forceinline__ void shared_add_u64(unsigned long long* a, unsigned long long w) {
+#if HYOWON_DEPOSIT_RED
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(a));
+    asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(sa), "l"(w) : "memory");
+#else
+    atomicAdd(a, w);
+#endif
+}
 
 // Rows of a deposit tile: 8-byte accumulators, at most 64 KiB per tile.
 inline int deposit_rows(int N) {
@@ -236,9 +253,9 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
                 const FixedPlan* plan, OUT* __restrict__ out, unsigned long long* qsum,
                 const unsigned int* status) {
     extern __shared__ __align__(16) unsigned long long qtile[];
-    __shared__ uint32_t seg_p0[4];
-    __shared__ uint32_t seg_cum[5];
+    __shared__ uint32_t seg_p0[4], seg_len[4];
     __shared__ int seg_plane[4], seg_row_lo[4], seg_row_hi[4], seg_xr[4];
+    __shared__ int seg_n;
     if (*status & ST_BLOCKS_PUBLISH) return;
     const int tid = threadIdx.x;
     const int x0 = blockIdx.y;
@@ -249,7 +266,6 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
         // segments: (plane x0 then x0-1) x (row ranges); a wrapped halo row
         // N-1 is its own segment
         int ns = 0;
-        uint32_t cum = 0;
         for (int xr = 0; xr < 2; ++xr) {
             const int p = xr == 0 ? x0 : (x0 == 0 ? N - 1 : x0 - 1);
             int lo[2], hi[2], nr = 0;
@@ -265,24 +281,15 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
                 const uint32_t a = offset[c_lo >> shift];
                 const uint32_t b = offset[(c_hi >> shift) + 1];
                 seg_p0[ns] = a;
-                seg_cum[ns] = cum;
+                seg_len[ns] = b - a;
                 seg_plane[ns] = p;
                 seg_row_lo[ns] = lo[k];
                 seg_row_hi[ns] = hi[k];
                 seg_xr[ns] = xr;
-                cum += b - a;
                 ++ns;
             }
         }
-        for (int k = ns; k < 4; ++k) {
-            seg_p0[k] = 0;
-            seg_cum[k] = cum;
-            seg_plane[k] = -1;
-            seg_row_lo[k] = 1;
-            seg_row_hi[k] = 0;
-            seg_xr[k] = 0;
-        }
-        seg_cum[4] = cum;
+        seg_n = ns;
     }
     const int tcells = ty * N;
     {
@@ -291,62 +298,63 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
         if ((tcells & 1) && tid == 0) qtile[tcells - 1] = 0ull;
     }
     __syncthreads();
-    const uint32_t c1 = seg_cum[1], c2 = seg_cum[2], c3 = seg_cum[3];
-    const uint32_t total = seg_cum[4];
     const int B = plan->B;
-    const unsigned one = 1u << B;
-    for (uint32_t v0 = tid; v0 < total; v0 += kDepositBatch * kDepositThreads) {
-        uint32_t idx[kDepositBatch];
-        int sg[kDepositBatch];
+    const uint32_t one = 1u << B;
+    const int sh = 32 - B;
+    const uint32_t uN = static_cast<uint32_t>(N);
+    const int ns = seg_n;
+    // one segment at a time: its bounds, plane and rows are block-uniform
+    for (int g = 0; g < ns; ++g) {
+        const uint32_t p0 = seg_p0[g];
+        const uint32_t len = seg_len[g];
+        const uint32_t plane = static_cast<uint32_t>(seg_plane[g]);
+        const int row_lo = seg_row_lo[g], row_hi = seg_row_hi[g];
+        const bool own_plane = seg_xr[g] == 0;
+        for (uint32_t v0 = tid; v0 < len; v0 += kDepositBatch * kDepositThreads) {
+            uint32_t idx[kDepositBatch];
 #pragma unroll
-        for (int k = 0; k < kDepositBatch; ++k) {
-            const uint32_t v = v0 + k * kDepositThreads;
-            sg[k] = -1;
-            if (v < total) {
-                const int g = (v >= c1) + (v >= c2) + (v >= c3);
-                sg[k] = g;
-                const uint32_t q = seg_p0[g] + (v - seg_cum[g]);
-                idx[k] = order ? order[q] : q;
+            for (int k = 0; k < kDepositBatch; ++k) {
+                const uint32_t v = v0 + k * kDepositThreads;
+                idx[k] = v < len ? (order ? order[p0 + v] : p0 + v) : 0xffffffffu;
             }
-        }
-        uint32_t u[kDepositBatch][3];
+            uint32_t u[kDepositBatch][3];
 #pragma unroll
-        for (int k = 0; k < kDepositBatch; ++k) {
-            if (sg[k] >= 0) {
-                u[k][0] = ux[idx[k]];
-                u[k][1] = uy[idx[k]];
-                u[k][2] = uz[idx[k]];
+            for (int k = 0; k < kDepositBatch; ++k) {
+                if (idx[k] != 0xffffffffu) {
+                    u[k][0] = ux[idx[k]];
+                    u[k][1] = uy[idx[k]];
+                    u[k][2] = uz[idx[k]];
+                }
             }
-        }
 #pragma unroll
-        for (int k = 0; k < kDepositBatch; ++k) {
-            if (sg[k] < 0) continue;
-            const int g = sg[k];
-            uint32_t fx, fy, fz;
-            const uint32_t ix = cell_of(u[k][0], N, fx);
-            const uint32_t iy = cell_of(u[k][1], N, fy);
-            const uint32_t iz = cell_of(u[k][2], N, fz);
-            // keep the particle only in the segment of its own base cell
-            if (static_cast<int>(ix) != seg_plane[g] || static_cast<int>(iy) < seg_row_lo[g]
-                || static_cast<int>(iy) > seg_row_hi[g])
-                continue;
-            fx >>= (32 - B);
-            fy >>= (32 - B);
-            fz >>= (32 - B);
-            const unsigned long long wx = seg_xr[g] == 0 ? one - fx : fx;
-            const unsigned long long wy[2] = {one - fy, fy};
-            const unsigned long long wz[2] = {one - fz, fz};
-            const uint32_t gz[2] = {iz, iz + 1 == static_cast<uint32_t>(N) ? 0u : iz + 1};
+            for (int k = 0; k < kDepositBatch; ++k) {
+                if (idx[k] == 0xffffffffu) continue;
+                uint32_t fx, fy, fz;
+                const uint32_t ix = cell_of(u[k][0], N, fx);
+                const uint32_t iy = cell_of(u[k][1], N, fy);
+                const uint32_t iz = cell_of(u[k][2], N, fz);
+                // keep the particle only in the segment of its own base cell
+                if (ix != plane || static_cast<int>(iy) < row_lo || static_cast<int>(iy) > row_hi)
+                    continue;
+                fx >>= sh;
+                fy >>= sh;
+                fz >>= sh;
+                const uint32_t wx = own_plane ? one - fx : fx;
+                const uint32_t wz0 = one - fz, wz1 = fz;
+                const uint32_t gz1 = iz + 1 == uN ? 0u : iz + 1;
 #pragma unroll
-            for (int oy = 0; oy < 2; ++oy) {
-                const uint32_t ys = iy + oy == static_cast<uint32_t>(N) ? 0u : iy + oy;
-                const int ly = static_cast<int>(ys) - y0;
-                if (ly < 0 || ly >= ty) continue;
-                const unsigned long long wxy = wx * wy[oy];
-#pragma unroll
-                for (int oz = 0; oz < 2; ++oz) {
-                    const unsigned long long w = wxy * wz[oz];
-                    if (w) atomicAdd(&qtile[ly * N + gz[oz]], w);
+                for (int oy = 0; oy < 2; ++oy) {
+                    const uint32_t ys = iy + oy == uN ? 0u : iy + oy;
+                    const int ly = static_cast<int>(ys) - y0;
+                    if (ly < 0 || ly >= ty) continue;
+                    // (wx wy) wz: a 32x32 -> 64 product, then 64 x 32
+                    const unsigned long long wxy =
+                        static_cast<unsigned long long>(wx) * (oy ? fy : one - fy);
+                    unsigned long long* row = qtile + static_cast<uint32_t>(ly) * uN;
+                    const unsigned long long w0 = wxy * wz0;
+                    const unsigned long long w1 = wxy * wz1;
+                    if (w0) shared_add_u64(row + iz, w0);
+                    if (w1) shared_add_u64(row + gz1, w1);
                 }
             }
         }
