@@ -86,6 +86,7 @@ _SIGS = {
     "hyowon_pm_last_error": (ctypes.c_char_p, [c_void_p]),
     "hyowon_pm_upload": (c_int, [c_void_p, c_u64] + [P_double] * 7 + [c_double]),
     "hyowon_pm_download": (c_int, [c_void_p] + [P_double] * 9),
+    "hyowon_pm_snapshot_payload": (c_int, [c_void_p, c_double, P_double, P_double]),
     "hyowon_pm_lpt_ics": (c_int, [c_void_p, c_u64, P_double, c_u64, P_double, P_double,
                                   P_double, c_double, c_double]),
     "hyowon_pm_compute_forces": (c_int, [c_void_p] + [P_double] * 3),

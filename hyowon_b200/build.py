@@ -40,6 +40,7 @@ UNITS = [
     ("pm_diag.cu", ["--fmad=false"]),
     ("pm_pk.cu", ["--fmad=false"]),
     ("pm_ic.cu", ["--fmad=false"]),
+    ("pm_snapshot.cu", ["--fmad=false"]),
     ("cosmology.cpp", []),
 ]
 

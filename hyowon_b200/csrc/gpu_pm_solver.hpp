@@ -131,6 +131,14 @@ public:
         return {d.potential_energy_comoving, d.directional_potential_energy_comoving};
     }
 
+    // /PartType1 Coordinates and Velocities rows (n x 3, original particle
+    // order, velocities p / a) for the snapshot writer; either span may be
+    // empty. hyowon_pm_snapshot_payload.
+    void snapshot_payload(double a, std::span<double> coordinates, std::span<double> velocities) {
+        check(hyowon_pm_snapshot_payload(h_, a, coordinates.empty() ? nullptr : coordinates.data(),
+                                         velocities.empty() ? nullptr : velocities.data()));
+    }
+
     // ParticleStore -> device. Momenta may be empty (zero).
     void upload(std::span<const double> x, std::span<const double> y, std::span<const double> z,
                 std::span<const double> px, std::span<const double> py,

@@ -200,6 +200,13 @@ __global__ void k_plan(uint32_t n, uint64_t cells, const uint32_t* max_count, do
 
 __device__ __forceinline__ void store_cell(float* out, long long q) { *out = __ll2float_rn(q); }
 __device__ __forceinline__ void store_cell(long long* out, long long q) { *out = q; }
+// Two adjacent cells (8-byte aligned for float, 16-byte for int64).
+__device__ __forceinline__ void store_cell2(float* out, long long a, long long b) {
+    *reinterpret_cast<float2*>(out) = make_float2(__ll2float_rn(a), __ll2float_rn(b));
+}
+__device__ __forceinline__ void store_cell2(long long* out, long long a, long long b) {
+    *reinterpret_cast<longlong2*>(out) = make_longlong2(a, b);
+}
 
 // Owner-computes fixed-point deposit: one block per tile of TY mesh rows
 // (x0, y0 .. y0+TY-1, all z) accumulating int64 weights in shared memory
@@ -363,10 +370,22 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
     const long long mean = plan->mean_q;
     OUT* o = out + (static_cast<uint64_t>(x0) * N + y0) * N;
     unsigned long long local = 0;
-    for (int e = tid; e < tcells; e += kDepositThreads) {
-        const long long v = static_cast<long long>(qtile[e]) - mean;
-        store_cell(&o[e], v);
-        local += static_cast<unsigned long long>(v);
+    if ((tcells & 1) == 0 && (N & 1) == 0) {
+        // two cells per thread and iteration: the tile starts on an even cell
+        const ulonglong2* q2 = reinterpret_cast<const ulonglong2*>(qtile);
+        for (int e = tid; e < tcells / 2; e += kDepositThreads) {
+            const ulonglong2 q = q2[e];
+            const long long v0 = static_cast<long long>(q.x) - mean;
+            const long long v1 = static_cast<long long>(q.y) - mean;
+            store_cell2(&o[2 * e], v0, v1);
+            local += static_cast<unsigned long long>(v0) + static_cast<unsigned long long>(v1);
+        }
+    } else {
+        for (int e = tid; e < tcells; e += kDepositThreads) {
+            const long long v = static_cast<long long>(qtile[e]) - mean;
+            store_cell(&o[e], v);
+            local += static_cast<unsigned long long>(v);
+        }
     }
     if (qsum) block_sum_to(local, qsum);
 }
@@ -1192,6 +1211,17 @@ int download(State* st, cudaStream_t s, double* x, double* y, double* z, double*
         rc = rc ? rc : fail(st, HYOWON_ECUDA, "download copy failed");
     if (owned) cudaFree(stage[0]);
     return rc;
+}
+
+void snapshot_view(State* st, snapshot::Component pos[3], snapshot::Component mom[3],
+                   const uint32_t** id, double** stage, uint64_t* stage_doubles) {
+    for (int a = 0; a < 3; ++a) {
+        pos[a] = {st->pos[st->pc][a], snapshot::kFixedU32, st->L / kTwo32};
+        mom[a] = {st->mom[st->mc][a], snapshot::kF32, 1.0};
+    }
+    *id = st->id[st->ic];
+    *stage = reinterpret_cast<double*>(st->modes);
+    *stage_doubles = st->modes_elems;
 }
 
 __global__ void k_widen_positions(uint32_t n, const uint32_t* __restrict__ u, double scale,

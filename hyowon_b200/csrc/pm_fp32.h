@@ -14,6 +14,8 @@
 
 #include <cuda_runtime.h>
 
+#include "pm_snapshot.h"
+
 struct hyowon_pm_s;
 
 namespace hyowon {
@@ -57,6 +59,11 @@ int diagnostics(State* st, cudaStream_t s, bool with_potential, double* scratch,
 // the particle count, in the current storage order.
 int positions_f64(State* st, cudaStream_t s, double* x, double* y, double* z);
 int download_mass_mesh(State* st, cudaStream_t s, unsigned int* d_status, double* mesh);
+// The device state as snapshot components (positions as u32 fixed point,
+// momenta FP32), the slot -> particle index, and the staging area available
+// between force solves (the half-spectrum buffer, *stage_doubles doubles).
+void snapshot_view(State* st, snapshot::Component pos[3], snapshot::Component mom[3],
+                   const uint32_t** id, double** stage, uint64_t* stage_doubles);
 
 }  // namespace fp32
 }  // namespace hyowon

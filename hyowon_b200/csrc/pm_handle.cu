@@ -28,6 +28,7 @@
 #include "pm_poisson.h"
 #include "pm_kernels.h"
 #include "pm_ic.h"
+#include "pm_snapshot.h"
 #include "pm_lpt.h"
 #include "pm_pk.h"
 
@@ -1013,6 +1014,79 @@ int hyowon_pm_download(hyowon_pm_t h, double* x, double* y, double* z, double* p
     CK(cudaStreamSynchronize(h->copy_stream));
     CK(cudaStreamSynchronize(h->stream));
     return HYOWON_OK;
+}
+
+int hyowon_pm_snapshot_payload(hyowon_pm_t h, double a, double* coordinates,
+                               double* velocities) {
+    if (!h) return HYOWON_EINVAL;
+    if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
+    if (!std::isfinite(a) || a <= 0.0)
+        return fail(h, HYOWON_EINVAL, "Snapshot scale factor must be finite and positive");
+    const double inv_a = 1.0 / a;
+    if (!std::isfinite(inv_a) || inv_a <= 0.0)
+        return fail(h, HYOWON_EOVERFLOW, "Snapshot inverse scale factor is not finite and positive");
+    const uint32_t n = h->n;
+    snapshot::Component pos[3], mom[3];
+    const uint32_t* id = nullptr;
+    double* stage = nullptr;
+    uint64_t stage_doubles = 0;
+    if (h->precision == HYOWON_FP32_FIXED) {
+        fp32::snapshot_view(h->f32, pos, mom, &id, &stage, &stage_doubles);
+    } else {
+        for (int d = 0; d < 3; ++d) {
+            pos[d] = {h->pos[h->pc][d], snapshot::kF64, 1.0};
+            mom[d] = {h->mom[h->mc][d], snapshot::kF64, 1.0};
+        }
+        id = h->id[h->ic];
+        const size_t half = static_cast<size_t>(h->N) * h->N * (h->N / 2 + 1);
+        stage = reinterpret_cast<double*>(h->modes);   // dead between force solves
+        stage_doubles = 2ull * half;
+    }
+    double* outs[2] = {coordinates, velocities};
+    const int sets = (coordinates ? 1 : 0) + (velocities ? 1 : 0);
+    if (sets == 0) return HYOWON_OK;
+    // every requested dataset is staged and validated before any is copied
+    const uint64_t need = 3ull * n * sets;
+    double* owned = nullptr;
+    if (stage_doubles < need) {
+        CK(dalloc(&owned, need));
+        stage = owned;
+    }
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
+    int rc = HYOWON_OK;
+    int k = 0;
+    for (int set = 0; set < 2 && rc == HYOWON_OK; ++set) {
+        if (!outs[set]) continue;
+        ++h->launches;
+        if (snapshot::launch_rows(n, id, set == 0 ? pos : mom, set == 1, inv_a, h->L,
+                                  stage + 3ull * n * k, h->d_status, h->stream) < 0)
+            rc = fail(h, HYOWON_ECUDA, "snapshot staging launch failed");
+        ++k;
+    }
+    unsigned int st = 0;
+    if (rc == HYOWON_OK) rc = read_status(h, &st);
+    if (rc == HYOWON_OK && st) {
+        if (st & snapshot::kNonFinite)
+            rc = fail(h, HYOWON_EINVAL, "Snapshot particle phase-space fields must be finite");
+        else if (st & snapshot::kOutsideBox)
+            rc = fail(h, HYOWON_EINVAL,
+                      "Snapshot coordinates must lie in the periodic half-open interval [0,L)");
+        else
+            rc = fail(h, HYOWON_EOVERFLOW, "Snapshot momentum-to-velocity conversion overflowed");
+    }
+    k = 0;
+    for (int set = 0; set < 2 && rc == HYOWON_OK; ++set) {
+        if (!outs[set]) continue;
+        if (cudaMemcpyAsync(outs[set], stage + 3ull * n * k, sizeof(double) * 3ull * n,
+                            cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+            rc = fail(h, HYOWON_ECUDA, "snapshot copy failed");
+        ++k;
+    }
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess && rc == HYOWON_OK)
+        rc = fail(h, HYOWON_ECUDA, "snapshot copy failed");
+    cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream);
+    cudaFree(owned);
+    return rc;
 }
 
 int hyowon_pm_compute_forces(hyowon_pm_t h, double* ax, double* ay, double* az) {

@@ -190,6 +190,18 @@ class PMSolver:
         self._check(rc, "download")
         return out
 
+    def snapshot_payload(self, a: float, coordinates=True, velocities=True):
+        """The /PartType1 Coordinates and Velocities datasets as (n, 3) arrays
+        in the original particle order, velocities p / a
+        (hyowon_pm_snapshot_payload); validated on the device first."""
+        n = self.info()[0]
+        c = np.empty((n, 3)) if coordinates else None
+        v = np.empty((n, 3)) if velocities else None
+        self._check(nat.lib().hyowon_pm_snapshot_payload(
+            self._h, float(a), None if c is None else c.ctypes.data_as(nat.P_double),
+            None if v is None else v.ctypes.data_as(nat.P_double)), "snapshot_payload")
+        return c, v
+
     def solve_forces(self):
         """Force solve at the device positions (accelerations become valid)."""
         self._check(nat.lib().hyowon_pm_compute_forces(self._h, None, None, None), "solve_forces")

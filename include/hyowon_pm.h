@@ -98,6 +98,18 @@ int hyowon_pm_lpt_ics(hyowon_pm_t h, uint64_t n_side, const double* noise,
 int hyowon_pm_download(hyowon_pm_t h, double* x, double* y, double* z, double* px,
                        double* py, double* pz, double* ax, double* ay, double* az);
 
+/* Snapshot payload staging for the native HDF5 writer: the /PartType1
+ * Coordinates and Velocities datasets (include/cosmo_nbody/io/output_schema.hpp:132-135)
+ * as n x 3 row-major binary64 arrays in the caller's original particle order,
+ * Velocities = p * (1 / a) (peculiar km/s; write_vector_dataset_batched,
+ * src/io/snapshot_io_particle_helpers.inc:116-200). The payload is validated
+ * as require_finite_particle_payload (:48-104) does, on the device, before
+ * anything is written: HYOWON_EINVAL for a non-finite field or a coordinate
+ * outside [0, L), HYOWON_EOVERFLOW when p / a is not finite. Either pointer
+ * may be NULL. ParticleIDs stay the caller's (row i is upload index i). */
+int hyowon_pm_snapshot_payload(hyowon_pm_t h, double a, double* coordinates,
+                               double* velocities);
+
 /* PMSolver::compute_forces (src/gravity/pm_solver.cpp:494-567) on the device
  * state: solves the force at the current positions, stores it as the valid
  * acceleration field, and ADDS it to the host arrays ax/ay/az when they are
