@@ -245,9 +245,14 @@ __device__ __forceinline__ void shared_add_u64(unsigned long long* a, unsigned l
 #endif
 }
 
-// Rows of a deposit tile: 8-byte accumulators, at most 64 KiB per tile.
+// Rows of a deposit tile: 8-byte accumulators, at most HYOWON_DEPOSIT_TILE_CELLS
+// cells (32 KiB at 4096: 6 blocks per SM, which hides the particle loads
+// better than 64 KiB tiles despite more halo rows) per tile.
+#ifndef HYOWON_DEPOSIT_TILE_CELLS
+#define HYOWON_DEPOSIT_TILE_CELLS 4096
+#endif
 inline int deposit_rows(int N) {
-    int ty = 8192 / N;
+    int ty = HYOWON_DEPOSIT_TILE_CELLS / N;
     if (ty < 1) ty = 1;
     return ty > N ? N : ty;
 }
@@ -492,7 +497,10 @@ __global__ void k_interp_add(uint32_t n, const float* __restrict__ field,
 }
 
 // Centred-gradient CIC gather (FP32) fused with the K2 kick.
-__global__ void __launch_bounds__(kThreads)
+#ifndef HYOWON_GATHER_MINB
+#define HYOWON_GATHER_MINB 1
+#endif
+__global__ void __launch_bounds__(kThreads, HYOWON_GATHER_MINB)
 k_gather_kick(uint32_t n, const float* __restrict__ phi, const uint32_t* __restrict__ ux,
               const uint32_t* __restrict__ uy, const uint32_t* __restrict__ uz,
               const float* __restrict__ px, const float* __restrict__ py,
