@@ -2,6 +2,10 @@
 //   wrapper_main invalid             -> prints the exception type of a bad config
 //   wrapper_main forces IN OUT       -> IN: u64 n, u64 N, f64 L, f64 m, x[n], y[n], z[n]
 //                                       OUT: ax[n], ay[n], az[n] (added to zero)
+//   wrapper_main post IN OUT         -> IN: as forces, then px[n], py[n], pz[n]
+//                                       OUT: {potential energy, directional derivative}
+//                                       after upload + a zero KDK step, then the
+//                                       snapshot rows coordinates[3n], velocities[3n] at a = 0.5
 #include "gpu_pm_solver.hpp"
 
 #include <cstdio>
@@ -54,6 +58,37 @@ int main(int argc, char** argv) {
         out.write(reinterpret_cast<const char*>(az.data()), 8 * n);
         return out ? 0 : 4;
     }
-    std::cerr << "usage: wrapper_main invalid | forces IN OUT\n";
+    if (argc == 4 && std::string(argv[1]) == "post") {
+        std::ifstream in(argv[2], std::ios::binary);
+        std::uint64_t n = 0, N = 0;
+        double L = 0.0, m = 0.0;
+        in.read(reinterpret_cast<char*>(&n), 8);
+        in.read(reinterpret_cast<char*>(&N), 8);
+        in.read(reinterpret_cast<char*>(&L), 8);
+        in.read(reinterpret_cast<char*>(&m), 8);
+        std::vector<std::vector<double>> c(6, std::vector<double>(n));
+        for (auto& v : c) in.read(reinterpret_cast<char*>(v.data()), 8 * n);
+        if (!in) return 2;
+        std::vector<double> coords(3 * n), vel(3 * n);
+        double out2[2] = {};
+        try {
+            GpuPMSolver s(L, N);
+            s.upload(c[0], c[1], c[2], c[3], c[4], c[5], {}, m);
+            s.kdk_step(0.0, 0.0, 0.0);   // force at the uploaded positions, state unchanged
+            const auto d = s.measure_post_force_energy_diagnostics();
+            out2[0] = d.potential_energy_comoving;
+            out2[1] = d.directional_potential_energy_comoving;
+            s.snapshot_payload(0.5, coords, vel);
+        } catch (const std::exception& e) {
+            std::cerr << typeid(e).name() << ": " << e.what() << "\n";
+            return 3;
+        }
+        std::ofstream out(argv[3], std::ios::binary);
+        out.write(reinterpret_cast<const char*>(out2), 16);
+        out.write(reinterpret_cast<const char*>(coords.data()), 8 * 3 * n);
+        out.write(reinterpret_cast<const char*>(vel.data()), 8 * 3 * n);
+        return out ? 0 : 4;
+    }
+    std::cerr << "usage: wrapper_main invalid | forces IN OUT | post IN OUT\n";
     return 64;
 }

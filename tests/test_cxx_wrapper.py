@@ -54,3 +54,39 @@ def test_compute_forces_through_cxx_matches_oracle(wrapper_exe, oracle, tmp_path
     for g, r in zip(got, ref):
         # two solves were added to zeroed arrays
         assert np.max(np.abs(g - 2.0 * r)) <= 1e-12 * scale
+
+
+@pytest.mark.gpu
+def test_post_force_diagnostics_and_snapshot_through_cxx(wrapper_exe, oracle, tmp_path):
+    """GpuPMSolver::measure_post_force_energy_diagnostics and snapshot_payload
+    from C++: the oracle's values of the uploaded state."""
+    from oracle import diag_oracle as dg
+    rng = np.random.default_rng(12)
+    n, N, L, m = 20000, 32, 50.0, 0.7
+    x, y, z = (rng.uniform(0, L, n) for _ in range(3))
+    px, py, pz = (rng.normal(0, 30.0, n) for _ in range(3))
+    src = tmp_path / "in.bin"
+    dst = tmp_path / "out.bin"
+    with open(src, "wb") as f:
+        f.write(np.array([n, N], dtype=np.uint64).tobytes())
+        f.write(np.array([L, m], dtype=np.float64).tobytes())
+        for a in (x, y, z, px, py, pz):
+            f.write(a.tobytes())
+    out = subprocess.run([wrapper_exe, "post", str(src), str(dst)], capture_output=True,
+                         text=True)
+    assert out.returncode == 0, out.stderr
+    raw = np.fromfile(dst, dtype=np.float64)
+    pe, de = raw[0], raw[1]
+    coords = raw[2:2 + 3 * n].reshape(n, 3)
+    vel = raw[2 + 3 * n:].reshape(n, 3)
+    _, phi = oracle.potential(L, N, x, y, z, uniform_mass=m)
+    b = np.empty((3, n), dtype=np.int64)
+    f = np.empty((3, n))
+    for d, v in enumerate((x, y, z)):
+        b[d], f[d] = oracle.cic_coords(L, N, v)
+    e_ref = dg.potential_energy_comoving(L, N, phi, b, f, m)
+    d_ref, scale = dg.directional_potential_energy(L, N, phi, b, f, m, px, py, pz)
+    assert abs(pe / e_ref - 1.0) < 1e-12
+    assert abs(de - d_ref) <= 1e-12 * scale
+    assert np.array_equal(coords, np.stack([x, y, z], axis=1))
+    assert np.array_equal(vel, np.stack([px, py, pz], axis=1) * (1.0 / 0.5))
