@@ -56,6 +56,7 @@ struct Error {
 }  // namespace
 
 struct hyowon_pm_s {
+    hyowon::ic::Workspace* ic_ws = nullptr;  // generated-IC work arrays (hyowon_pm_generate_ics)
     double L = 0.0;
     int N = 0;
     int method = HYOWON_PURE_PM;
@@ -255,6 +256,15 @@ void set_input_mass(hyowon_pm_t h, double total, uint32_t n) {
     const long double nu = (32.0L * n + 1.0L) * eps;
     const long double gamma = nu / (1.0L - nu);
     h->mass_tol = static_cast<double>((gamma + 64.0L * eps) * total * (1.0L + 4.0L * gamma));
+}
+
+// The generated-IC work arrays are kept between hyowon_pm_generate_ics calls
+// and given back before anything else that needs device memory runs.
+void release_ic_workspace(hyowon_pm_t h) {
+    if (h && h->ic_ws) {
+        hyowon::ic::workspace_destroy(h->ic_ws);
+        h->ic_ws = nullptr;
+    }
 }
 
 int read_status(hyowon_pm_t h, unsigned int* st) {
@@ -708,6 +718,7 @@ int hyowon_pm_create(double box_size, uint64_t mesh_size, int method, int deconv
 int hyowon_pm_destroy(hyowon_pm_t h) {
     if (!h) return HYOWON_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    hyowon::ic::workspace_destroy(h->ic_ws);
     if (h->f32) fp32::destroy(h->f32);
     if (h->plans) {
         cufftDestroy(h->plan_r2c);
@@ -754,6 +765,7 @@ const char* hyowon_pm_last_error(hyowon_pm_t h) {
 int hyowon_pm_upload(hyowon_pm_t h, uint64_t n64, const double* x, const double* y, const double* z,
                      const double* px, const double* py, const double* pz, const double* masses,
                      double uniform_mass) {
+    release_ic_workspace(h);
     if (!h) return HYOWON_EINVAL;
     if (n64 == 0 || n64 > 0xFFFFFFF0ull) return fail(h, HYOWON_EINVAL, "particle count must be in [1, 2^32-16]");
     if (!x || !y || !z) return fail(h, HYOWON_EINVAL, "position arrays must be non-null");
@@ -833,6 +845,7 @@ int hyowon_pm_upload(hyowon_pm_t h, uint64_t n64, const double* x, const double*
 int hyowon_pm_lpt_ics(hyowon_pm_t h, uint64_t n_side, const double* noise, uint64_t n_nodes,
                       const double* ln_k, const double* ln_p, const double* ln_p_y2,
                       double momentum_factor, double uniform_mass) {
+    release_ic_workspace(h);
     if (!h) return HYOWON_EINVAL;
     if (n_side < 2 || n_side > 2048 || !noise || n_nodes < 2 || !ln_k || !ln_p || !ln_p_y2)
         return fail(h, HYOWON_EINVAL, "LPT requires n_side in [2,2048], noise and a spline table");
@@ -940,8 +953,9 @@ int hyowon_pm_generate_ics(hyowon_pm_t h, const hyowon_ic_params_t* p, uint64_t 
     }
     if (rc == HYOWON_OK) {
         cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream);
+        if (!h->ic_ws) h->ic_ws = hyowon::ic::workspace_create();
         const int grc = hyowon::ic::generate_device(r, d_amp, tmp_pos, tmp_mom, h->d_status,
-                                                    h->stream, &err);
+                                                    h->stream, &err, h->ic_ws);
         if (grc) rc = fail(h, grc, err);
     }
     unsigned int st = 0;
@@ -1090,6 +1104,7 @@ int hyowon_pm_snapshot_payload(hyowon_pm_t h, double a, double* coordinates,
 }
 
 int hyowon_pm_compute_forces(hyowon_pm_t h, double* ax, double* ay, double* az) {
+    release_ic_workspace(h);
     if (!h) return HYOWON_EINVAL;
     if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
     int rc;
@@ -1127,12 +1142,14 @@ int hyowon_pm_compute_forces(hyowon_pm_t h, double* ax, double* ay, double* az) 
 int hyowon_pm_forces_host(hyowon_pm_t h, uint64_t n, const double* x, const double* y,
                           const double* z, const double* masses, double uniform_mass, double* ax,
                           double* ay, double* az) {
+    release_ic_workspace(h);
     int rc = hyowon_pm_upload(h, n, x, y, z, nullptr, nullptr, nullptr, masses, uniform_mass);
     if (rc) return rc;
     return hyowon_pm_compute_forces(h, ax, ay, az);
 }
 
 int hyowon_pm_kdk_step(hyowon_pm_t h, double K1, double D, double K2, double* max_drift) {
+    release_ic_workspace(h);
     if (!h) return HYOWON_EINVAL;
     CallTimer timer(h);
     return kdk_step_impl(h, K1, D, K2, max_drift);
@@ -1140,6 +1157,7 @@ int hyowon_pm_kdk_step(hyowon_pm_t h, double K1, double D, double K2, double* ma
 
 int hyowon_pm_run(hyowon_pm_t h, uint64_t n_steps, const double* K1, const double* D,
                   const double* K2, double* max_drift) {
+    release_ic_workspace(h);
     if (!h) return HYOWON_EINVAL;
     if (n_steps > 0 && (!K1 || !D || !K2)) return fail(h, HYOWON_EINVAL, "factor arrays must be non-null");
     CallTimer timer(h);
@@ -1174,6 +1192,7 @@ int hyowon_pm_download_potential(hyowon_pm_t h, double* phi) {
 }
 
 int hyowon_pm_download_mass_mesh(hyowon_pm_t h, double* mesh) {
+    release_ic_workspace(h);
     if (!h || !mesh) return HYOWON_EINVAL;
     if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
     if (!h->sorted) {
@@ -1313,6 +1332,7 @@ int hyowon_pm_diagnostics(hyowon_pm_t h, double a, hyowon_pm_diagnostics_t* out)
 int hyowon_pm_power_spectrum(hyowon_pm_t h, uint64_t mesh_size, int num_bins,
                              double max_k_fraction_nyquist, int subtract_shot_noise,
                              int interlaced, hyowon_pk_bin_t* bins) {
+    release_ic_workspace(h);
     if (!h || !bins) return HYOWON_EINVAL;
     if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
     const uint64_t N = mesh_size ? mesh_size : static_cast<uint64_t>(h->N);

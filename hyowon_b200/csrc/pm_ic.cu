@@ -34,16 +34,21 @@
 // round differently, at the level of the last bits.
 //
 // HBM traffic per mode / cell is a few words in each kernel; the FP64
-// transforms dominate: 1LPT = 3 Z2D of N^3; 2LPT = 6 Z2D + 1 D2Z of M^3 and
-// 6 Z2D of N^3.
+// transforms dominate: 1LPT = 3 Z2D of N^3; 2LPT = 6 inverse transforms and 1
+// D2Z of M^3 and 6 Z2D of N^3. On power-of-two IC meshes the six Hessian
+// transforms run through the potential solve's own passes (generate_fused):
+// the symbol is applied inside the x pass and the source accumulation inside
+// the z pass, so no separate multiply or accumulate sweep touches HBM.
 #include <cfloat>
 #include <climits>
 #include <cmath>
 #include <cstring>
 #include <cufft.h>
+#include <new>
 
 #include "pm_common.cuh"
 #include "pm_ic.h"
+#include "pm_poisson.h"
 
 namespace hyowon {
 namespace ic {
@@ -101,17 +106,28 @@ __device__ __forceinline__ void half_index(uint64_t idx, int M, int& ix, int& iy
 
 // ----------------------------------------------------------------- field ----
 
+// Element (i, j, k) of an M^3 half spectrum: row-major ((i M + j)(M/2+1) + k)
+// when cc == 0, else the chunked layout of the five-pass transform
+// ((k / cc) M^2 cc + (i M + j) cc + k % cc).
+__device__ __forceinline__ uint64_t spectrum_at(int i, int j, int k, int M, int cc) {
+    if (cc == 0)
+        return (static_cast<uint64_t>(i) * M + j) * static_cast<uint64_t>(M / 2 + 1) + k;
+    return static_cast<uint64_t>(k / cc) * static_cast<uint64_t>(M) * M * cc +
+           (static_cast<uint64_t>(i) * M + j) * cc + k % cc;
+}
+
 __global__ void k_field(int M, int K, uint64_t seed, int fixed, int negate,
-                        const double2* __restrict__ amp, double2* __restrict__ out,
+                        const double2* __restrict__ amp, double2* __restrict__ out_modes, int cc,
                         unsigned int* status) {
     const uint64_t total = static_cast<uint64_t>(M) * M * (M / 2 + 1);
     const uint64_t idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= total) return;
     int i, j, k;
     half_index(idx, M, i, j, k);
+    double2* const out = out_modes + spectrum_at(i, j, k, M, cc);
     const int mx = mode_number(i, M), my = mode_number(j, M), mz = k;
     if ((mx == 0 && my == 0 && mz == 0) || abs(mx) > K || abs(my) > K || mz > K) {
-        out[idx] = make_double2(0.0, 0.0);
+        *out = make_double2(0.0, 0.0);
         return;
     }
     bool conjugate = false, self_conjugate = false;
@@ -130,7 +146,7 @@ __global__ void k_field(int M, int K, uint64_t seed, int fixed, int negate,
     const double2 a = amp[s];
     if (!(a.x > 0.0) || !(a.y > 0.0) || !isfinite(a.x) || !isfinite(a.y)) {
         raise_status(status, IC_AMPLITUDE);
-        out[idx] = make_double2(0.0, 0.0);
+        *out = make_double2(0.0, 0.0);
         return;
     }
     const Draw d = mode_uniforms(seed, mode_number(ci, M), mode_number(cj, M), mz, fixed ? 1u : 0u);
@@ -164,7 +180,7 @@ __global__ void k_field(int M, int K, uint64_t seed, int fixed, int negate,
         re = -re;
         im = -im;
     }
-    out[idx] = make_double2(re, im);
+    *out = make_double2(re, im);
 }
 
 // ------------------------------------------------------- spectral stages ----
@@ -223,7 +239,7 @@ __global__ void k_hessian(int M, double L, int a, int b, const double2* __restri
 // support (K < N/2 <= M/2), where k_a would be 0.
 template <typename I>
 __global__ void k_displacement(int N, int M, double L, int a, int K, bool second,
-                               const double2* __restrict__ src, double2* __restrict__ dst) {
+                               const double2* __restrict__ src, int cc, double2* __restrict__ dst) {
     const I total = static_cast<I>(N) * static_cast<I>(N) * static_cast<I>(N / 2 + 1);
     const I idx = static_cast<I>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (idx >= total) return;
@@ -234,9 +250,7 @@ __global__ void k_displacement(int N, int M, double L, int a, int K, bool second
         dst[idx] = make_double2(0.0, 0.0);
         return;
     }
-    const uint64_t hz = static_cast<uint64_t>(M / 2 + 1);
-    const uint64_t at = (static_cast<uint64_t>(mx < 0 ? mx + M : mx) * M +
-                         static_cast<uint64_t>(my < 0 ? my + M : my)) * hz + static_cast<uint64_t>(mz);
+    const uint64_t at = spectrum_at(mx < 0 ? mx + M : mx, my < 0 ? my + M : my, mz, M, cc);
     const double kx = wavenumber(mx, L), ky = wavenumber(my, L), kz = wavenumber(mz, L);
     const double k2 = kx * kx + ky * ky + kz * kz;
     const double kd = a == 0 ? kx : (a == 1 ? ky : kz);
@@ -326,18 +340,24 @@ struct Fft {
     cufftHandle c2r = 0, r2c = 0;
     bool has_c2r = false, has_r2c = false;
     void* ws = nullptr;
-    ~Fft() {
+    ~Fft() { reset(); }
+    void reset() {
         if (has_c2r) cufftDestroy(c2r);
         if (has_r2c) cufftDestroy(r2c);
         cudaFree(ws);
+        has_c2r = has_r2c = false;
+        ws = nullptr;
     }
-    int make(int M, bool forward, cudaStream_t s, const char** err) {
+    int make(int M, bool forward, cudaStream_t s, const char** err, bool inverse = true) {
+        reset();
         size_t w1 = 0, w2 = 0;
-        if (cufftCreate(&c2r) != CUFFT_SUCCESS) return *err = "cufftCreate failed", HYOWON_ECUDA;
-        has_c2r = true;
-        cufftSetAutoAllocation(c2r, 0);
-        if (cufftMakePlan3d(c2r, M, M, M, CUFFT_Z2D, &w1) != CUFFT_SUCCESS)
-            return *err = "cuFFT Z2D plan for the IC mesh failed", HYOWON_ECUDA;
+        if (inverse) {
+            if (cufftCreate(&c2r) != CUFFT_SUCCESS) return *err = "cufftCreate failed", HYOWON_ECUDA;
+            has_c2r = true;
+            cufftSetAutoAllocation(c2r, 0);
+            if (cufftMakePlan3d(c2r, M, M, M, CUFFT_Z2D, &w1) != CUFFT_SUCCESS)
+                return *err = "cuFFT Z2D plan for the IC mesh failed", HYOWON_ECUDA;
+        }
         if (forward) {
             if (cufftCreate(&r2c) != CUFFT_SUCCESS) return *err = "cufftCreate failed", HYOWON_ECUDA;
             has_r2c = true;
@@ -349,8 +369,10 @@ struct Fft {
         if (w < 256) w = 256;
         if (cudaMalloc(&ws, w) != cudaSuccess)
             return *err = "cuFFT work area for the IC mesh could not be allocated", HYOWON_ENOMEM;
-        cufftSetWorkArea(c2r, ws);
-        cufftSetStream(c2r, s);
+        if (inverse) {
+            cufftSetWorkArea(c2r, ws);
+            cufftSetStream(c2r, s);
+        }
         if (forward) {
             cufftSetWorkArea(r2c, ws);
             cufftSetStream(r2c, s);
@@ -363,7 +385,11 @@ template <typename T>
 struct DeviceBuffer {
     T* p = nullptr;
     ~DeviceBuffer() { cudaFree(p); }
-    bool alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * n) == cudaSuccess; }
+    bool alloc(size_t n) {
+        cudaFree(p);
+        p = nullptr;
+        return cudaMalloc(&p, sizeof(T) * n) == cudaSuccess;
+    }
 };
 
 // ------------------------------------------------- scaled positive product --
@@ -545,17 +571,157 @@ int status_code(unsigned int st, const char** err) {
 // ---------------------------------------------------------------- device ----
 
 int field_device(const Params& p, const double2* d_amp, double2* d_modes, unsigned int* d_status,
-                 cudaStream_t s, const char** err) {
+                 cudaStream_t s, const char** err, int cc) {
     const uint64_t half = static_cast<uint64_t>(p.M) * p.M * (p.M / 2 + 1);
-    k_field<<<grid(half), 256, 0, s>>>(p.M, p.K, p.seed, p.fixed, p.negate, d_amp, d_modes,
+    k_field<<<grid(half), 256, 0, s>>>(p.M, p.K, p.seed, p.fixed, p.negate, d_amp, d_modes, cc,
                                        d_status);
     if (cudaGetLastError() != cudaSuccess) return *err = "IC field launch failed", HYOWON_ECUDA;
     return HYOWON_OK;
 }
 
+namespace {
+struct PlanOwner {
+    poisson::Plan* p = nullptr;
+    ~PlanOwner() { poisson::destroy_plan(p); }
+    void reset() {
+        poisson::destroy_plan(p);
+        p = nullptr;
+    }
+};
+}  // namespace
+
+// Work arrays and plans of generate_fused for one (N, M, L).
+struct Workspace {
+    int N = 0, M = 0;
+    double L = 0.0;
+    bool ready = false;
+    DeviceBuffer<double2> delta, work, psi_n, tw;
+    DeviceBuffer<double> acc, source, field_n, ktab;
+    PlanOwner pd, pw;
+    Fft fft_m, fft_n;
+
+    int prepare(const Params& p, cudaStream_t s, const char** err) {
+        if (ready && N == p.N && M == p.M && L == p.L) {
+            // the cuFFT plans follow the caller's stream
+            cufftSetStream(fft_m.r2c, s);
+            cufftSetStream(fft_n.c2r, s);
+            return HYOWON_OK;
+        }
+        ready = false;
+        N = p.N;
+        M = p.M;
+        L = p.L;
+        const uint64_t cells = static_cast<uint64_t>(M) * M * M;
+        const uint64_t n = static_cast<uint64_t>(N) * N * N;
+        const uint64_t half_n = static_cast<uint64_t>(N) * N * (N / 2 + 1);
+        const size_t chunked = poisson::modes_elements_f64(M);
+        if (!delta.alloc(chunked) || !work.alloc(chunked) || !acc.alloc(cells) ||
+            !source.alloc(cells) || !psi_n.alloc(half_n) || !field_n.alloc(n) || !tw.alloc(M) ||
+            !ktab.alloc(M))
+            return *err = "IC mesh work arrays could not be allocated", HYOWON_ENOMEM;
+        // twiddles exp(-2 pi i m / M) and wavenumbers (2 pi m) / L (the device
+        // expression: two IEEE roundings, as on the host)
+        double* h = static_cast<double*>(std::malloc(sizeof(double) * 3 * M));
+        if (!h) return *err = "host twiddle table could not be allocated", HYOWON_ENOMEM;
+        poisson::twiddles(M, h);
+        for (int i = 0; i < M; ++i) {
+            const int m = i <= M / 2 ? i : i - M;
+            h[2 * M + i] = kTwoPi * static_cast<double>(m) / p.L;
+        }
+        const bool ok =
+            cudaMemcpy(tw.p, h, sizeof(double2) * M, cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(ktab.p, h + 2 * M, sizeof(double) * M, cudaMemcpyHostToDevice) == cudaSuccess;
+        std::free(h);
+        if (!ok) return *err = "twiddle upload failed", HYOWON_ECUDA;
+        pd.reset();
+        pw.reset();
+        if (!(pd.p = poisson::create_plan(M, false, delta.p, err)) ||
+            !(pw.p = poisson::create_plan(M, false, work.p, err)))
+            return HYOWON_ECUDA;
+        int rc = fft_m.make(M, true, s, err, false);   // D2Z of the source only
+        if (!rc) rc = fft_n.make(N, false, s, err);
+        if (rc) return rc;
+        ready = true;
+        return HYOWON_OK;
+    }
+};
+
+Workspace* workspace_create() { return new (std::nothrow) Workspace(); }
+void workspace_destroy(Workspace* w) { delete w; }
+
+namespace {
+// 2LPT on a power-of-two IC mesh with the five-pass transform machinery: the
+// field in its chunked layout, each Hessian as three passes (symbol and
+// inverse x, inverse y, c2r along z folding into the source), the D2Z of the
+// source and the N^3 displacement transforms by cuFFT. The arithmetic is the
+// generator's; the transforms round differently from cuFFT's. Four M^3
+// fields (spectrum, work spectrum, two source accumulators) instead of five.
+int generate_fused(const Params& p, const double2* d_amp, double* const d_pos[3],
+                   double* const d_mom[3], unsigned int* d_status, cudaStream_t s,
+                   const char** err, Workspace& w) {
+    const int M = p.M, N = p.N;
+    const uint64_t n = static_cast<uint64_t>(N) * N * N;
+    const uint64_t half_n = static_cast<uint64_t>(N) * N * (N / 2 + 1);
+    const int cc = poisson::chunk_columns_f64(M);
+    const double norm = 1.0 / (static_cast<double>(M) * M * M);
+    int rc = w.prepare(p, s, err);
+    if (rc) return rc;
+    const bool small_n = half_n < (1ull << 32);
+    auto displacements = [&](const double2* src, int src_cc, bool second_order, double xf,
+                             double pf, unsigned int flag) -> int {
+        for (int a = 0; a < 3; ++a) {
+            if (small_n)
+                k_displacement<uint32_t><<<grid(half_n), 256, 0, s>>>(N, M, p.L, a, p.K,
+                                                                      second_order, src, src_cc,
+                                                                      w.psi_n.p);
+            else
+                k_displacement<uint64_t><<<grid(half_n), 256, 0, s>>>(N, M, p.L, a, p.K,
+                                                                      second_order, src, src_cc,
+                                                                      w.psi_n.p);
+            if (cufftExecZ2D(w.fft_n.c2r, reinterpret_cast<cufftDoubleComplex*>(w.psi_n.p),
+                             w.field_n.p) != CUFFT_SUCCESS)
+                return *err = "IC c2r failed", HYOWON_ECUDA;
+            k_apply<<<grid(n), 256, 0, s>>>(n, w.field_n.p, norm, xf, pf, p.L, d_pos[a],
+                                            d_mom[a], flag, d_status);
+        }
+        return HYOWON_OK;
+    };
+    k_lattice<<<grid(n), 256, 0, s>>>(N, p.L / static_cast<double>(N), d_pos[0], d_pos[1],
+                                      d_pos[2], d_mom[0], d_mom[1], d_mom[2]);
+    if ((rc = field_device(p, d_amp, w.delta.p, d_status, s, err, cc))) return rc;
+    if ((rc = displacements(w.delta.p, cc, false, 1.0, p.p1, IC_PSI1))) return rc;
+    static const int pairs[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    for (int t = 0; t < 6; ++t) {
+        const poisson::HessianF64 h{w.ktab.p, pairs[t][0], pairs[t][1]};
+        const poisson::SourceTermF64 term{t < 3 ? t : 3, t == 5, norm, w.acc.p, w.source.p,
+                                          d_status, IC_HESSIAN, IC_SOURCE};
+        if (poisson::hessian_source_f64(w.pd.p, w.pw.p, M, w.work.p, w.tw.p, h, term, d_status,
+                                        s) < 0)
+            return *err = "IC Hessian pass launch failed", HYOWON_ECUDA;
+    }
+    // S -> S_k, row-major, in the work buffer
+    if (cufftExecD2Z(w.fft_m.r2c, w.source.p, reinterpret_cast<cufftDoubleComplex*>(w.work.p)) !=
+        CUFFT_SUCCESS)
+        return *err = "IC r2c of the 2LPT source failed", HYOWON_ECUDA;
+    if ((rc = displacements(w.work.p, 0, true, p.x2, p.p2, IC_PSI2))) return rc;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return *err = "IC kernels failed", HYOWON_ECUDA;
+    return HYOWON_OK;
+}
+}  // namespace
+
+// HYOWON_IC_FUSED: 2LPT on power-of-two IC meshes through generate_fused.
+#ifndef HYOWON_IC_FUSED
+#define HYOWON_IC_FUSED 1
+#endif
+
 int generate_device(const Params& p, const double2* d_amp, double* const d_pos[3],
                     double* const d_mom[3], unsigned int* d_status, cudaStream_t s,
-                    const char** err) {
+                    const char** err, Workspace* ws) {
+    if (HYOWON_IC_FUSED && p.order == 2 && poisson::supported(p.M)) {
+        if (ws) return generate_fused(p, d_amp, d_pos, d_mom, d_status, s, err, *ws);
+        Workspace local;
+        return generate_fused(p, d_amp, d_pos, d_mom, d_status, s, err, local);
+    }
     const int M = p.M, N = p.N;
     const uint64_t half = static_cast<uint64_t>(M) * M * (M / 2 + 1);
     const uint64_t cells = static_cast<uint64_t>(M) * M * M;
@@ -583,15 +749,17 @@ int generate_device(const Params& p, const double2* d_amp, double* const d_pos[3
     if ((folded || !second) && (rc = fft_n.make(N, false, s, err))) return rc;
     const cufftHandle c2r_n = (folded || !second) ? fft_n.c2r : fft_m.c2r;
 
-    auto displacements = [&](const double2* src, bool second_order, double xf, double pf,
-                             unsigned int flag) -> int {
+    auto displacements = [&](const double2* src, int src_cc, bool second_order, double xf,
+                             double pf, unsigned int flag) -> int {
         for (int a = 0; a < 3; ++a) {
             if (small_n)
                 k_displacement<uint32_t><<<grid(half_n), 256, 0, s>>>(N, M, p.L, a, p.K,
-                                                                      second_order, src, disp_k);
+                                                                      second_order, src, src_cc,
+                                                                      disp_k);
             else
                 k_displacement<uint64_t><<<grid(half_n), 256, 0, s>>>(N, M, p.L, a, p.K,
-                                                                      second_order, src, disp_k);
+                                                                      second_order, src, src_cc,
+                                                                      disp_k);
             if (cufftExecZ2D(c2r_n, reinterpret_cast<cufftDoubleComplex*>(disp_k), disp_r) !=
                 CUFFT_SUCCESS)
                 return *err = "IC c2r failed", HYOWON_ECUDA;
@@ -604,7 +772,7 @@ int generate_device(const Params& p, const double2* d_amp, double* const d_pos[3
     k_lattice<<<grid(n), 256, 0, s>>>(N, p.L / static_cast<double>(N), d_pos[0], d_pos[1],
                                       d_pos[2], d_mom[0], d_mom[1], d_mom[2]);
     if ((rc = field_device(p, d_amp, delta.p, d_status, s, err))) return rc;
-    if ((rc = displacements(delta.p, false, 1.0, p.p1, IC_PSI1))) return rc;
+    if ((rc = displacements(delta.p, 0, false, 1.0, p.p1, IC_PSI1))) return rc;
     if (second) {
         static const int pairs[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
         for (int t = 0; t < 6; ++t) {
@@ -624,7 +792,7 @@ int generate_device(const Params& p, const double2* d_amp, double* const d_pos[3
         if (cufftExecD2Z(fft_m.r2c, source.p, reinterpret_cast<cufftDoubleComplex*>(delta.p)) !=
             CUFFT_SUCCESS)
             return *err = "IC r2c of the 2LPT source failed", HYOWON_ECUDA;
-        if ((rc = displacements(delta.p, true, p.x2, p.p2, IC_PSI2))) return rc;
+        if ((rc = displacements(delta.p, 0, true, p.x2, p.p2, IC_PSI2))) return rc;
     }
     if (cudaStreamSynchronize(s) != cudaSuccess) return *err = "IC kernels failed", HYOWON_ECUDA;
     return HYOWON_OK;

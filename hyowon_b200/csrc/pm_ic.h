@@ -43,13 +43,24 @@ int upload_amplitudes(const Params& p, uint64_t n_power, const double* power, do
 // Maps the status word to a hyowon_status and message (0 when clean).
 int status_code(unsigned int st, const char** err);
 
-// Device. RandomField::generate into d_modes (M * M * (M/2+1)).
+// Device. RandomField::generate into d_modes (M * M * (M/2+1)): row-major
+// when cc == 0, else the five-pass transform's chunked layout with cc kz
+// columns per chunk (poisson::chunk_columns_f64).
 int field_device(const Params& p, const double2* d_amp, double2* d_modes, unsigned int* d_status,
-                 cudaStream_t s, const char** err);
+                 cudaStream_t s, const char** err, int cc = 0);
+// Work arrays and plans of a 2LPT generation on a power-of-two IC mesh
+// (about four IC-mesh fields), kept between generations of the same (N, M, L)
+// by whoever owns the workspace.
+struct Workspace;
+Workspace* workspace_create();
+void workspace_destroy(Workspace* w);
+
 // The whole generate branch into d_pos[3] / d_mom[3] (N^3 each, particle order).
+// With ws, the work arrays come from (and stay in) ws; else they are
+// allocated and freed within the call.
 int generate_device(const Params& p, const double2* d_amp, double* const d_pos[3],
                     double* const d_mom[3], unsigned int* d_status, cudaStream_t s,
-                    const char** err);
+                    const char** err, Workspace* ws = nullptr);
 
 }  // namespace ic
 }  // namespace hyowon

@@ -181,9 +181,18 @@ k_z_forward(const SRC* __restrict__ in, cx_t<T>* __restrict__ H, const cx_t<T>* 
 
 // c2r of CZ rows per block: Z[k] = (X[k] + conj X[M-k]) + i W_N^-k (X[k] - conj X[M-k]),
 // inverse length-M transform, real output pairs (Re, Im).
-template <typename T, int LOG2N>
+// Stores the two reals (row element 2jj, 2jj+1) of a z-inverse output pair.
+struct StorePair {
+    template <typename T, typename C>
+    __device__ __forceinline__ void operator()(T* out, size_t idx, C v) const {
+        __stcs(reinterpret_cast<C*>(out + idx), v);
+    }
+};
+
+template <typename T, int LOG2N, typename EPI>
 __global__ void __launch_bounds__(Geo<T, LOG2N>::TZ, HYOWON_FFT_MINB_Z)
-k_z_inverse(const cx_t<T>* __restrict__ H, T* __restrict__ out, const cx_t<T>* __restrict__ tw) {
+k_z_inverse(const cx_t<T>* __restrict__ H, T* __restrict__ out, const cx_t<T>* __restrict__ tw,
+            EPI epi) {
     using G = Geo<T, LOG2N>;
     using C = cx_t<T>;
     constexpr int S = G::SZ;
@@ -228,7 +237,7 @@ k_z_inverse(const cx_t<T>* __restrict__ H, T* __restrict__ out, const cx_t<T>* _
     for (int e = tid; e < G::CZ * G::M; e += G::TZ) {
         const int r = e / G::M;
         const int jj = e % G::M;
-        __stcs(reinterpret_cast<C*>(out + (row0 + r) * G::N + 2 * jj), sm[jj * S + r]);
+        epi(out, (row0 + r) * G::N + 2 * jj, sm[jj * S + r]);
     }
 }
 
@@ -273,6 +282,60 @@ struct DevGreenF32 {
     }
 };
 
+// 2LPT Hessian symbol k_a k_b / k^2 (mixed terms 0 on either axis's Nyquist
+// plane; k = 0 gives 0), wavenumbers (2 pi m) / L from a table formed with
+// the same two roundings: the arithmetic of the IC generator's Hessian
+// kernel, rounded operation by operation.
+struct DevHessianF64 {
+    HessianF64 h;
+    int N;
+    __device__ __forceinline__ double2 operator()(int ix, int iy, int iz, double2 v) const {
+        const double k[3] = {__ldg(&h.k[ix]), __ldg(&h.k[iy]), __ldg(&h.k[iz])};
+        const double k2 = __dadd_rn(__dadd_rn(__dmul_rn(k[0], k[0]), __dmul_rn(k[1], k[1])),
+                                    __dmul_rn(k[2], k[2]));
+        if (k2 == 0.0) return make_double2(0.0, 0.0);
+        const bool even = (N & 1) == 0;
+        const int ia = h.a == 0 ? ix : (h.a == 1 ? iy : iz);
+        const int ib = h.b == 0 ? ix : (h.b == 1 ? iy : iz);
+        const double ka = h.a == 0 ? k[0] : (h.a == 1 ? k[1] : k[2]);
+        const double kb = h.b == 0 ? k[0] : (h.b == 1 ? k[1] : k[2]);
+        const bool mixed_nyquist = h.a != h.b && even && (ia == N / 2 || ib == N / 2);
+        const double q = __ddiv_rn(mixed_nyquist ? 0.0 : __dmul_rn(ka, kb), k2);
+        return make_double2(__dmul_rn(v.x, q), __dmul_rn(v.y, q));
+    }
+};
+
+// z-inverse epilogue folding the normalised field h into the 2LPT source,
+// the IC generator's source kernel applied to each output pair:
+// op 0: acc = h; 1: src = acc h, acc += h; 2: src += acc h; 3: src -= h h.
+struct SourceEpiF64 {
+    SourceTermF64 t;
+    __device__ __forceinline__ void operator()(double*, size_t idx, double2 v) const {
+        const double h0 = __dmul_rn(v.x, t.norm), h1 = __dmul_rn(v.y, t.norm);
+        if (!isfinite(h0) || !isfinite(h1)) atomicOr(t.status, t.hessian_flag);
+        double2* acc = reinterpret_cast<double2*>(t.acc + idx);
+        double2* src = reinterpret_cast<double2*>(t.src + idx);
+        if (t.op == 0) {
+            *acc = make_double2(h0, h1);
+            return;
+        }
+        double2 out;
+        if (t.op == 1) {
+            const double2 a = *acc;
+            out = make_double2(__dmul_rn(a.x, h0), __dmul_rn(a.y, h1));
+            *acc = make_double2(__dadd_rn(a.x, h0), __dadd_rn(a.y, h1));
+        } else if (t.op == 2) {
+            const double2 a = *acc, sv = *src;
+            out = make_double2(__dadd_rn(sv.x, __dmul_rn(a.x, h0)), __dadd_rn(sv.y, __dmul_rn(a.y, h1)));
+        } else {
+            const double2 sv = *src;
+            out = make_double2(__dsub_rn(sv.x, __dmul_rn(h0, h0)), __dsub_rn(sv.y, __dmul_rn(h1, h1)));
+        }
+        if (t.last && (!isfinite(out.x) || !isfinite(out.y))) atomicOr(t.status, t.source_flag);
+        *src = out;
+    }
+};
+
 // Bounded polls of a pipeline barrier before a block gives up (each poll may
 // suspend for a hardware-chosen interval; a healthy wait needs a few).
 constexpr unsigned kWaitLimit = 1u << 24;
@@ -286,7 +349,10 @@ constexpr unsigned kWaitLimit = 1u << 24;
 // block transforms the current one (dense rows, no padding: a half/quarter
 // warp reads one 64-byte row). With GREEN (the x pass): forward transform,
 // Green's multiply, inverse transform. Results are stored from registers.
-template <typename T, int LOG2N, int AXIS, int SIGN, bool GREEN, typename GF>
+// MODE 0: one transform (SIGN); 1: forward transform, Green's multiply,
+// inverse transform (the x pass of the potential solve); 2: the symbol
+// `green` applied to the untransformed tile, then one transform (SIGN).
+template <typename T, int LOG2N, int AXIS, int SIGN, int MODE, typename GF>
 __global__ void __launch_bounds__(Geo<T, LOG2N>::TC, sizeof(T) == 4 ? HYOWON_FFT_MINB_C32 : HYOWON_FFT_MINB_C64)
 k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
           const cx_t<T>* __restrict__ tw, GF green, unsigned int* status) {
@@ -361,8 +427,22 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
         const int seq = static_cast<int>(t % G::N);
         const int kz = kc * G::CC + c;
         C v[16];
-        fft::smem_to_registers<LOG2N, SIGN, G::CC, S>(sm, tw, G::N, c, j, v);
-        if constexpr (GREEN) {
+        if constexpr (MODE == 2) {
+            // element j + q P of column c, untransformed
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = sm[(j + q * P) * S + c];
+            if (kz < G::Hz) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    v[q] = AXIS == 0 ? green(j + q * P, seq, kz, v[q]) : green(seq, j + q * P, kz, v[q]);
+            }
+            __syncthreads();
+            fft::first_stage_to_smem<LOG2N, SIGN, G::CC, S>(v, sm, c, j);
+            fft::rest_to_registers<LOG2N, SIGN, G::CC, S>(sm, tw, G::N, c, j, v);
+        } else {
+            fft::smem_to_registers<LOG2N, SIGN, G::CC, S>(sm, tw, G::N, c, j, v);
+        }
+        if constexpr (MODE == 1) {
             if (kz < G::Hz) {
 #pragma unroll
                 for (int q = 0; q < 16; ++q)
@@ -397,18 +477,18 @@ int z_forward(const SRC* in, cx_t<T>* H, const cx_t<T>* tw, unsigned long long* 
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
-template <typename T, int LOG2N>
-int z_inverse(const cx_t<T>* H, T* out, const cx_t<T>* tw, cudaStream_t s) {
+template <typename T, int LOG2N, typename EPI = StorePair>
+int z_inverse(const cx_t<T>* H, T* out, const cx_t<T>* tw, cudaStream_t s, EPI epi = EPI{}) {
     using G = Geo<T, LOG2N>;
-    if (!prepare(k_z_inverse<T, LOG2N>, G::smem_zi)) return -1;
+    if (!prepare(k_z_inverse<T, LOG2N, EPI>, G::smem_zi)) return -1;
     const unsigned blocks = static_cast<unsigned>(static_cast<size_t>(G::N) * G::N / G::CZ);
-    k_z_inverse<T, LOG2N><<<blocks, G::TZ, G::smem_zi, s>>>(H, out, tw);
+    k_z_inverse<T, LOG2N, EPI><<<blocks, G::TZ, G::smem_zi, s>>>(H, out, tw, epi);
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
 // AXIS 1: y transforms of every (kc, kx) block; AXIS 0: x transforms of
 // every (kc, ky) column set.
-template <typename T, int LOG2N, int AXIS, int SIGN, bool GREEN, typename GF>
+template <typename T, int LOG2N, int AXIS, int SIGN, int MODE, typename GF>
 int columns(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF green, unsigned int* status,
             cudaStream_t s);
 
@@ -424,30 +504,30 @@ template <typename T, typename SRC, int LOG2N>
 int forward_t(const Plan* p, const SRC* in, cx_t<T>* H, const cx_t<T>* tw, unsigned long long* qsum,
               unsigned int* status, cudaStream_t s) {
     if (z_forward<T, SRC, LOG2N>(in, H, tw, qsum, s) < 0) return -1;
-    if (columns<T, LOG2N, kPlainAxis, -1, false>(p, H, tw, NoGreen{}, status, s) < 0) return -1;
+    if (columns<T, LOG2N, kPlainAxis, -1, 0>(p, H, tw, NoGreen{}, status, s) < 0) return -1;
     return 2;
 }
 
 template <typename T, int LOG2N, typename GF>
 int green_t(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF g, unsigned int* status,
             cudaStream_t s) {
-    return columns<T, LOG2N, kGreenAxis, -1, true>(p, H, tw, g, status, s);
+    return columns<T, LOG2N, kGreenAxis, -1, 1>(p, H, tw, g, status, s);
 }
 
 template <typename T, int LOG2N>
 int inverse_t(const Plan* p, cx_t<T>* H, T* out, const cx_t<T>* tw, unsigned int* status,
               cudaStream_t s) {
-    if (columns<T, LOG2N, kPlainAxis, +1, false>(p, H, tw, NoGreen{}, status, s) < 0) return -1;
+    if (columns<T, LOG2N, kPlainAxis, +1, 0>(p, H, tw, NoGreen{}, status, s) < 0) return -1;
     if (z_inverse<T, LOG2N>(H, out, tw, s) < 0) return -1;
     return 2;
 }
 
-template <typename T, int LOG2N, int AXIS, int SIGN, bool GREEN, typename GF>
+template <typename T, int LOG2N, int AXIS, int SIGN, int MODE, typename GF>
 int columns(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF green, unsigned int* status,
             cudaStream_t s) {
     using G = Geo<T, LOG2N>;
     if (!p || p->N != G::N) return -1;
-    auto kernel = k_columns<T, LOG2N, AXIS, SIGN, GREEN, GF>;
+    auto kernel = k_columns<T, LOG2N, AXIS, SIGN, MODE, GF>;
     if (!prepare(kernel, G::smem_c)) return -1;
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess
@@ -602,6 +682,41 @@ int inverse_f64(const Plan* p, int N, double2* modes, double* phi, const double2
                 unsigned int* status, cudaStream_t s) {
     if (!supported(N) || !p || p->fp32) return -1;
     HYOWON_DISPATCH(N, (inverse_t<double, LG>(p, modes, phi, tw, status, s)))
+}
+
+namespace {
+template <int LOG2N>
+int hessian_source_t(const Plan* pd, const Plan* pw, int N, double2* work, const double2* tw,
+                     const HessianF64& h, const SourceTermF64& t, unsigned int* status,
+                     cudaStream_t s) {
+    // symbol then inverse x: tiles read from the spectrum of pd, stored to work
+    if (columns<double, LOG2N, 0, +1, 2>(pd, work, tw, DevHessianF64{h, N}, status, s) < 0)
+        return -1;
+    if (columns<double, LOG2N, 1, +1, 0>(pw, work, tw, NoGreen{}, status, s) < 0) return -1;
+    if (z_inverse<double, LOG2N, SourceEpiF64>(work, nullptr, tw, s, SourceEpiF64{t}) < 0)
+        return -1;
+    return 3;
+}
+}  // namespace
+
+int hessian_source_f64(const Plan* pd, const Plan* pw, int N, double2* work, const double2* tw,
+                       const HessianF64& h, const SourceTermF64& t, unsigned int* status,
+                       cudaStream_t s) {
+    if (!supported(N) || !pd || !pw || pd->fp32 || pw->fp32) return -1;
+    HYOWON_DISPATCH(N, (hessian_source_t<LG>(pd, pw, N, work, tw, h, t, status, s)))
+}
+
+int chunk_columns_f64(int N) {
+    switch (log2_of(N)) {
+    case 5: return Geo<double, 5>::CC;
+    case 6: return Geo<double, 6>::CC;
+    case 7: return Geo<double, 7>::CC;
+    case 8: return Geo<double, 8>::CC;
+    case 9: return Geo<double, 9>::CC;
+    case 10: return Geo<double, 10>::CC;
+    case 11: return Geo<double, 11>::CC;
+    default: return 0;
+    }
 }
 
 int forward_f32(const Plan* p, int N, const float* mesh, float2* modes, const float2* tw,

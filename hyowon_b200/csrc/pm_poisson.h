@@ -60,6 +60,35 @@ struct GreenF32 {
     const float* c_green;
 };
 
+// Kz columns per chunk of the FP64 chunked half spectrum: element
+// (kx, ky, kz) of an N^3 transform sits at
+// (kz / CC) N^2 CC + (kx N + ky) CC + kz % CC.
+int chunk_columns_f64(int N);
+
+// One Hessian field of the 2LPT source of the IC generator
+// (LPTDisplacement, src/ic/lpt_displacement.cpp:386-520): H_ab = c2r(d k_a k_b /
+// k^2) from the fully transformed spectrum d (chunked, tensor maps in pd),
+// normalised by t.norm and folded into the real accumulators t.acc / t.src
+// (SourceTermF64::op), in three passes: the symbol and the inverse x
+// transform into `work` (maps in pw), the inverse y transform, and the c2r
+// along z whose epilogue does the folding.
+struct HessianF64 {
+    const double* k;   // k[i] = (2 pi m(i)) / L for array index i (m the signed mode)
+    int a, b;
+};
+struct SourceTermF64 {
+    int op;            // 0: acc = h; 1: src = acc h, acc += h; 2: src += acc h; 3: src -= h^2
+    int last;          // check the source for finiteness
+    double norm;       // 1 / N^3
+    double* acc;
+    double* src;
+    unsigned int* status;
+    unsigned int hessian_flag, source_flag;
+};
+int hessian_source_f64(const Plan* pd, const Plan* pw, int N, double2* work, const double2* tw,
+                       const HessianF64& h, const SourceTermF64& t, unsigned int* status,
+                       cudaStream_t s);
+
 // Each returns the number of kernels launched, or -1 if a launch failed.
 // status receives ST_PIPELINE if a pipelined pass gives up waiting.
 int forward_f64(const Plan* p, int N, const double* mass, double2* modes, const double2* tw,

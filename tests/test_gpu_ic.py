@@ -180,3 +180,31 @@ def test_full_size_pairing_and_variance():
     ratio = np.abs(f[sel]) ** 2 / (amp[s[sel], 0] ** 2)
     n = ratio.size
     assert abs(ratio.mean() - 1.0) < 6.0 / math.sqrt(n), (ratio.mean(), n)
+
+
+def test_handle_keeps_work_arrays_between_generations(ic_golden):
+    """hyowon_pm_generate_ics keeps its work arrays in the handle: repeated
+    generations, a change of lattice / IC mesh, and a generation after a KDK
+    step (which gives the arrays back) all write the standalone call's state."""
+    L = float(ic_golden["box"])
+    p16, c16 = params_of(ic_golden, "n16_2lpt")
+    pb, cb = params_of(ic_golden, "n16_2lpt_fixed_pair_b")
+    p32 = ic.ICParams(32, L, 5, p16.a_start, lpt_order=2, factors=p16.factors)
+    w32 = ic.power_table(p32, ic.start_spectrum(p16.a_start))
+    ref16 = ic.generate_ics(p16, c16["power"])
+    refb = ic.generate_ics(pb, cb["power"])
+    ref32 = ic.generate_ics(p32, w32)
+    comps = ("x", "y", "z", "px", "py", "pz")
+    with hb.PMSolver(hb.MeshGeometry(L, 32), hb.PMForceMethod.pure_pm(False)) as s:
+        for p, power, ref in ((p16, c16["power"], ref16), (p16, c16["power"], ref16),
+                              (pb, cb["power"], refb), (p32, w32, ref32),
+                              (p16, c16["power"], ref16)):
+            s.generate_ics(p, power, 1.0)
+            d = s.download(acc=False)
+            for k in comps:
+                assert np.array_equal(d[k], ref[k]), k
+        s.kdk_step(1e-4, 1e-4, 1e-4)
+        s.generate_ics(p16, c16["power"], 1.0)
+        d = s.download(acc=False)
+        for k in comps:
+            assert np.array_equal(d[k], ref16[k]), k
