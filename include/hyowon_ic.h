@@ -81,7 +81,11 @@ int hyowon_ic_generate(const hyowon_ic_params_t* p, uint64_t n_power, const doub
 
 /* The same, written straight into the solver's device-resident particle
  * state (replacing it); every particle gets uniform_mass
- * (SimulationParameters::particle_mass). */
+ * (SimulationParameters::particle_mass). For 2LPT on a power-of-two IC mesh
+ * the handle keeps the generation's work arrays (four M^3 binary64 fields:
+ * 34 GB at M = 1024) and plans until its next upload, step, force solve,
+ * power spectrum or destroy, so that generating several realisations
+ * (seeds) allocates once. Errors are read with hyowon_pm_last_error(h). */
 int hyowon_pm_generate_ics(hyowon_pm_t h, const hyowon_ic_params_t* p, uint64_t n_power,
                            const double* power, double uniform_mass);
 
