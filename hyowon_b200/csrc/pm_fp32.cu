@@ -59,8 +59,21 @@ __device__ __forceinline__ uint32_t cell_of(uint32_t u, int N, uint32_t& frac) {
     return static_cast<uint32_t>(p >> 32);
 }
 
-__device__ __forceinline__ uint32_t cell_index(uint32_t ix, uint32_t iy, uint32_t iz, int N) {
-    return (ix * static_cast<uint32_t>(N) + iy) * static_cast<uint32_t>(N) + iz;
+// Row-major cell index; 64-bit because a mesh side above 1625 has more than
+// 2^32 cells (the row ix N + iy still fits 32 bits).
+__device__ __forceinline__ uint64_t cell_index(uint32_t ix, uint32_t iy, uint32_t iz, int N) {
+    return static_cast<uint64_t>(ix * static_cast<uint32_t>(N) + iy) * static_cast<uint32_t>(N) + iz;
+}
+
+// The same in index type IDX: the gather uses 32-bit indices whenever the
+// mesh has at most 2^32 cells (fewer registers for its 32 stencil loads).
+template <typename IDX>
+__device__ __forceinline__ IDX cell_index_t(uint32_t ix, uint32_t iy, uint32_t iz, int N) {
+    return static_cast<IDX>(ix * static_cast<uint32_t>(N) + iy) * static_cast<uint32_t>(N) + iz;
+}
+
+inline bool cells_fit_u32(int N) {
+    return static_cast<uint64_t>(N) * N * N <= 0xffffffffull;
 }
 
 __device__ __forceinline__ uint32_t to_fixed(double x, double L, bool& ok) {
@@ -101,8 +114,8 @@ __global__ void k_key(uint32_t n, const uint32_t* __restrict__ ux, const uint32_
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t f;
-    const uint32_t b = cell_index(cell_of(ux[i], N, f), cell_of(uy[i], N, f), cell_of(uz[i], N, f), N)
-        >> shift;
+    const uint32_t b = static_cast<uint32_t>(
+        cell_index(cell_of(ux[i], N, f), cell_of(uy[i], N, f), cell_of(uz[i], N, f), N) >> shift);
     key[i] = b;
     rank[i] = bucket_rank(count, b);
 }
@@ -150,8 +163,8 @@ __global__ void k_kick_drift_key(uint32_t n, const uint32_t* __restrict__ ux,
         pyo[i] = qy;
         pzo[i] = qz;
         uint32_t f;
-        const uint32_t b = cell_index(cell_of(nx, N, f), cell_of(ny, N, f), cell_of(nz, N, f), N)
-            >> shift;
+        const uint32_t b = static_cast<uint32_t>(
+            cell_index(cell_of(nx, N, f), cell_of(ny, N, f), cell_of(nz, N, f), N) >> shift);
         if (with_rank) {
             key[i] = b;
             rank[i] = bucket_rank(count, b);
@@ -500,6 +513,7 @@ __global__ void k_interp_add(uint32_t n, const float* __restrict__ field,
 #ifndef HYOWON_GATHER_MINB
 #define HYOWON_GATHER_MINB 1
 #endif
+template <typename IDX>
 __global__ void __launch_bounds__(kThreads, HYOWON_GATHER_MINB)
 k_gather_kick(uint32_t n, const float* __restrict__ phi, const uint32_t* __restrict__ ux,
               const uint32_t* __restrict__ uy, const uint32_t* __restrict__ uz,
@@ -520,7 +534,7 @@ k_gather_kick(uint32_t n, const float* __restrict__ phi, const uint32_t* __restr
                        iy + 2 >= N ? iy + 2 - N : iy + 2};
     const int zs[4] = {iz == 0 ? N - 1 : iz - 1, iz, iz + 1 == N ? 0 : iz + 1,
                        iz + 2 >= N ? iz + 2 - N : iz + 2};
-#define PHI(a_, b_, c_) __ldg(&phi[cell_index(xs[a_], ys[b_], zs[c_], N)])
+#define PHI(a_, b_, c_) __ldg(&phi[cell_index_t<IDX>(xs[a_], ys[b_], zs[c_], N)])
     float c[2][2][2], xm[2][2], xp[2][2], ym[2][2], yp[2][2], zm[2][2], zp[2][2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
@@ -1038,10 +1052,16 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
         rec(ev, 5, s);
         const float inv_two_dx = static_cast<float>(1.0 / (2.0 * st->L / N));
         ++st->launches;
-        k_gather_kick<<<blocks_for(n), kThreads, 0, s>>>(
-            n, st->rmesh, st->pos[P][0], st->pos[P][1], st->pos[P][2],
-            st->mom[M][0], st->mom[M][1], st->mom[M][2], st->acc[0], st->acc[1],
-            st->acc[2], kick ? 1 : 0, K2f, pxo, pyo, pzo, N, inv_two_dx, d_status);
+        if (cells_fit_u32(N))
+            k_gather_kick<uint32_t><<<blocks_for(n), kThreads, 0, s>>>(
+                n, st->rmesh, st->pos[P][0], st->pos[P][1], st->pos[P][2],
+                st->mom[M][0], st->mom[M][1], st->mom[M][2], st->acc[0], st->acc[1],
+                st->acc[2], kick ? 1 : 0, K2f, pxo, pyo, pzo, N, inv_two_dx, d_status);
+        else
+            k_gather_kick<uint64_t><<<blocks_for(n), kThreads, 0, s>>>(
+                n, st->rmesh, st->pos[P][0], st->pos[P][1], st->pos[P][2],
+                st->mom[M][0], st->mom[M][1], st->mom[M][2], st->acc[0], st->acc[1],
+                st->acc[2], kick ? 1 : 0, K2f, pxo, pyo, pzo, N, inv_two_dx, d_status);
         rec(ev, 6, s);
         return HYOWON_OK;
     }
@@ -1057,10 +1077,16 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
         rec(ev, 5, s);
         const float inv_two_dx = static_cast<float>(1.0 / (2.0 * st->L / N));
         ++st->launches;
-        k_gather_kick<<<blocks_for(n), kThreads, 0, s>>>(
-            n, st->rmesh, st->pos[P][0], st->pos[P][1], st->pos[P][2],
-            st->mom[M][0], st->mom[M][1], st->mom[M][2], st->acc[0], st->acc[1],
-            st->acc[2], kick ? 1 : 0, K2f, pxo, pyo, pzo, N, inv_two_dx, d_status);
+        if (cells_fit_u32(N))
+            k_gather_kick<uint32_t><<<blocks_for(n), kThreads, 0, s>>>(
+                n, st->rmesh, st->pos[P][0], st->pos[P][1], st->pos[P][2],
+                st->mom[M][0], st->mom[M][1], st->mom[M][2], st->acc[0], st->acc[1],
+                st->acc[2], kick ? 1 : 0, K2f, pxo, pyo, pzo, N, inv_two_dx, d_status);
+        else
+            k_gather_kick<uint64_t><<<blocks_for(n), kThreads, 0, s>>>(
+                n, st->rmesh, st->pos[P][0], st->pos[P][1], st->pos[P][2],
+                st->mom[M][0], st->mom[M][1], st->mom[M][2], st->acc[0], st->acc[1],
+                st->acc[2], kick ? 1 : 0, K2f, pxo, pyo, pzo, N, inv_two_dx, d_status);
         rec(ev, 6, s);
         return HYOWON_OK;
     }

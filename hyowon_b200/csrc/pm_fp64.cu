@@ -20,10 +20,23 @@ inline unsigned blocks_for(uint64_t n, int threads = kThreads) {
     return static_cast<unsigned>((n + threads - 1) / threads);
 }
 
-__device__ __forceinline__ uint32_t cell_index(int ix, int iy, int iz, int N) {
-    return (static_cast<uint32_t>(ix) * static_cast<uint32_t>(N) + static_cast<uint32_t>(iy))
-               * static_cast<uint32_t>(N)
-        + static_cast<uint32_t>(iz);
+// Row-major cell index; 64-bit because a mesh side above 1625 has more than
+// 2^32 cells (the row ix N + iy still fits 32 bits).
+__device__ __forceinline__ uint64_t cell_index(int ix, int iy, int iz, int N) {
+    const uint32_t row = static_cast<uint32_t>(ix) * static_cast<uint32_t>(N) + static_cast<uint32_t>(iy);
+    return static_cast<uint64_t>(row) * static_cast<uint32_t>(N) + static_cast<uint32_t>(iz);
+}
+
+// The same in index type IDX: the gather uses 32-bit indices whenever the
+// mesh has at most 2^32 cells (fewer registers for its 32 stencil loads).
+template <typename IDX>
+__device__ __forceinline__ IDX cell_index_t(int ix, int iy, int iz, int N) {
+    const uint32_t row = static_cast<uint32_t>(ix) * static_cast<uint32_t>(N) + static_cast<uint32_t>(iy);
+    return static_cast<IDX>(row) * static_cast<uint32_t>(N) + static_cast<uint32_t>(iz);
+}
+
+inline bool cells_fit_u32(int N) {
+    return static_cast<uint64_t>(N) * N * N <= 0xffffffffull;
 }
 
 __global__ void k_validate_inputs(uint32_t n, const double* __restrict__ x,
@@ -55,7 +68,7 @@ __global__ void k_key(uint32_t n, const double* __restrict__ x, const double* __
                                  : ST_NONFINITE_INPUT);
         bx = by = bz = 0;
     }
-    const uint32_t b = cell_index(bx, by, bz, a.N) >> shift;
+    const uint32_t b = static_cast<uint32_t>(cell_index(bx, by, bz, a.N) >> shift);
     key[i] = b;
     rank[i] = bucket_rank(count, b);
 }
@@ -108,7 +121,7 @@ __global__ void k_kick_drift_key(uint32_t n, const double* __restrict__ x,
         pyo[i] = qy;
         pzo[i] = qz;
         if (with_key) {
-            const uint32_t b = cell_index(bx, by, bz, a.N) >> shift;
+            const uint32_t b = static_cast<uint32_t>(cell_index(bx, by, bz, a.N) >> shift);
             key[i] = b;
             rank[i] = bucket_rank(count, b);
         }
@@ -395,6 +408,7 @@ __device__ __forceinline__ bool gather_axis_fast(const double (&c)[2][2][2], con
 #ifndef HYOWON_GATHER64_MINB
 #define HYOWON_GATHER64_MINB 3
 #endif
+template <typename IDX>
 __global__ void __launch_bounds__(kThreads, HYOWON_GATHER64_MINB)
 k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restrict__ x,
               const double* __restrict__ y, const double* __restrict__ z,
@@ -419,7 +433,7 @@ k_gather_kick(uint32_t n, const double* __restrict__ phi, const double* __restri
                        iy + 2 >= N ? iy + 2 - N : iy + 2};
     const int zs[4] = {iz == 0 ? N - 1 : iz - 1, iz, iz + 1 == N ? 0 : iz + 1,
                        iz + 2 >= N ? iz + 2 - N : iz + 2};
-#define PHI(a_, b_, c_) __ldg(&phi[cell_index(xs[a_], ys[b_], zs[c_], N)])
+#define PHI(a_, b_, c_) __ldg(&phi[cell_index_t<IDX>(xs[a_], ys[b_], zs[c_], N)])
     double c[2][2][2];
 #pragma unroll
     for (int u = 0; u < 2; ++u)
@@ -604,9 +618,14 @@ void launch_gather_kick_f64(uint32_t n, const double* phi, const ParticlesF64& p
                             double* pxo, double* pyo, double* pzo, Axis a,
                             unsigned int* status, cudaStream_t s) {
     if (n == 0) return;
-    k_gather_kick<<<blocks_for(n), kThreads, 0, s>>>(n, phi, p.x, p.y, p.z, p.px, p.py, p.pz,
-                                                     ax, ay, az, do_kick, K2, pxo, pyo, pzo,
-                                                     a, 1.0 / (2.0 * a.dx), status);
+    if (cells_fit_u32(a.N))
+        k_gather_kick<uint32_t><<<blocks_for(n), kThreads, 0, s>>>(
+            n, phi, p.x, p.y, p.z, p.px, p.py, p.pz, ax, ay, az, do_kick, K2, pxo, pyo, pzo, a,
+            1.0 / (2.0 * a.dx), status);
+    else
+        k_gather_kick<uint64_t><<<blocks_for(n), kThreads, 0, s>>>(
+            n, phi, p.x, p.y, p.z, p.px, p.py, p.pz, ax, ay, az, do_kick, K2, pxo, pyo, pzo, a,
+            1.0 / (2.0 * a.dx), status);
 }
 
 void launch_kick_only_f64(uint32_t n, const ParticlesF64& p, const double* ax,

@@ -767,7 +767,11 @@ int hyowon_pm_upload(hyowon_pm_t h, uint64_t n64, const double* x, const double*
                      double uniform_mass) {
     release_ic_workspace(h);
     if (!h) return HYOWON_EINVAL;
-    if (n64 == 0 || n64 > 0xFFFFFFF0ull) return fail(h, HYOWON_EINVAL, "particle count must be in [1, 2^32-16]");
+    // no particles: PMSolver's exact input-mass identity throws std::runtime_error
+    // for a zero particle count (src/gravity/pm_solver.cpp:664-679)
+    if (n64 == 0)
+        return fail(h, HYOWON_ERUNTIME, "PMSolver exact input mass identity must be finite and positive");
+    if (n64 > 0xFFFFFFF0ull) return fail(h, HYOWON_EINVAL, "particle count must be at most 2^32-16");
     if (!x || !y || !z) return fail(h, HYOWON_EINVAL, "position arrays must be non-null");
     if (!masses && (!std::isfinite(uniform_mass) || uniform_mass <= 0.0))
         return fail(h, HYOWON_EINVAL, "PMSolver uniform mass must be finite and positive");

@@ -132,8 +132,6 @@ class PMSolver:
         for a in (acc_x, acc_y, acc_z):
             if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]):
                 raise ValueError("acceleration outputs must be C-contiguous float64 arrays")
-        if n == 0:
-            raise ValueError("PMSolver exact input mass identity must be finite and positive")
         x, y, z = _f64(pos_x), _f64(pos_y), _f64(pos_z)
         m = None if uniform_mass is not None else _f64(masses)
         rc = nat.lib().hyowon_pm_forces_host(self._h, n, nat.dptr(x), nat.dptr(y), nat.dptr(z),

@@ -56,7 +56,9 @@ typedef struct hyowon_pm_s* hyowon_pm_t;
  * include/cosmo_nbody/gravity/pm_solver.hpp:52-56) together with
  * MeshGeometry(L, N_g) (include/cosmo_nbody/mesh/mesh_geometry.hpp:18-62) and
  * PMForceMethod::pure_pm / treepm_long_range. split_scale is r_s for
- * HYOWON_TREEPM_LONG_RANGE and ignored otherwise. */
+ * HYOWON_TREEPM_LONG_RANGE and ignored otherwise. mesh_size is 2 .. 2048
+ * (HYOWON_EINVAL outside); meshes above 1625 have more than 2^32 cells and
+ * are indexed in 64 bits. */
 int hyowon_pm_create(double box_size, uint64_t mesh_size, int method,
                      int deconvolve_cic, double split_scale, int precision,
                      hyowon_pm_t* out);
@@ -70,7 +72,9 @@ const char* hyowon_pm_last_error(hyowon_pm_t h);
  * into device memory: positions (any finite value; wrapped on device), canonical
  * momenta p = a^2 dx/dt, and either per-particle masses (masses != NULL) or one
  * uniform mass. Momenta may be NULL (zero). Accelerations become invalid until
- * the next force solve. */
+ * the next force solve. n = 0 fails with HYOWON_ERUNTIME, as PMSolver's exact
+ * input-mass identity does for a zero particle count
+ * (src/gravity/pm_solver.cpp:664-679); n is at most 2^32 - 16. */
 int hyowon_pm_upload(hyowon_pm_t h, uint64_t n, const double* x, const double* y,
                      const double* z, const double* px, const double* py,
                      const double* pz, const double* masses, double uniform_mass);
