@@ -29,6 +29,7 @@ state, all inside the timed region. Multi-GPU runs are independent replicas
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import math
 import os
@@ -68,16 +69,31 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    The sampler is started, and its first reading awaited (up to 10 s), before
+    the region opens; readings every 50 ms are kept only when their timestamp
+    lies inside the region, so start-up and idle readings after it are left out.
+    """
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 50
 
     def __init__(self, device_index=0):
         self.dev = device_index
         self.proc = None
         self.path = None
+        self.t_open = None
+        self.t_close = None
+
+    def _lines(self):
+        try:
+            with open(self.path) as f:
+                return [ln for ln in f.read().splitlines() if ln.count(",") >= 9]
+        except OSError:
+            return []
 
     def __enter__(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -85,29 +101,44 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
+        if self.proc:
+            deadline = time.time() + 10.0
+            while time.time() < deadline and self.proc.poll() is None and not self._lines():
+                time.sleep(0.02)
+        self.t_open = time.time()
         return self
 
     def __exit__(self, *exc):
+        self.t_close = time.time()
         if self.proc:
+            # the reading in flight at the close lands within one interval
+            time.sleep(2 * self.INTERVAL_MS / 1000.0)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
+    @staticmethod
+    def _stamp(text):
+        try:
+            return datetime.datetime.strptime(text.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
     def summary(self):
         rows = []
-        try:
-            for line in open(self.path):
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        except OSError:
-            pass
+        for line in self._lines():
+            parts = [p.strip() for p in line.split(",")]
+            t = self._stamp(parts[0])
+            if t is None or self.t_open is None or self.t_close is None:
+                continue
+            if self.t_open <= t <= self.t_close:
+                rows.append(parts[1:])
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]

@@ -2,19 +2,20 @@
 // passes over HBM (see pm_poisson.h for the pass structure).
 //
 // The half spectrum is held kz-chunk-major: H[kc][kx][ky][kzc] with
-// kz = kc * CC + kzc, CC = 16 FP32 / 8 FP64 complex values (128 bytes), so
-//  * a y-pass tile (kc, kx) is one contiguous N * 128-byte block,
-//  * an x-pass tile (kc, ky) reads 128-byte runs inside one N^2 * 128-byte
+// kz = kc * CC + kzc, CC = 8 FP32 / 4 FP64 complex values (64 bytes; half
+// that at N = 2048), so
+//  * a y-pass tile (kc, kx) is one contiguous N * 64-byte block,
+//  * an x-pass tile (kc, ky) reads 64-byte runs inside one N^2 * 64-byte
 //    chunk (a small page footprint instead of the whole 4-8 GB mesh),
-//  * a z-pass block of CZ consecutive rows writes CZ * 128 contiguous bytes
+//  * a z-pass block of CZ consecutive rows writes CZ * 64 contiguous bytes
 //    per chunk.
 // The last chunk holds the Nyquist plane kz = N/2 and CC-1 unused columns
 // (memory and transform work +1/(N/(2 CC)+1)).
 //
 // Bytes moved per solve on an N^3 mesh with b-byte reals: z forward reads the
-// N^3 mass values and writes H, the x, y(+Green)
-// and x passes read and write H in place, z inverse reads H and writes the
-// N^3 potential.
+// N^3 mass values and writes H; the y forward, x (forward, Green's multiply,
+// inverse) and y inverse passes read and write H in place; z inverse reads H
+// and writes the N^3 potential.
 #include "pm_poisson.h"
 
 #include "pm_common.cuh"

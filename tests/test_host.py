@@ -115,3 +115,37 @@ def test_particle_mass():
     # rho_crit0 = 3 H0^2 / (8 pi G) = 27.75 (1e10 Msun/h) / (Mpc/h)^3
     assert ic.RHO_CRIT0 == pytest.approx(27.754, rel=1e-3)
     assert ic.particle_mass(100.0, 32) == pytest.approx(27.754 * 0.3 * (100 / 32) ** 3, rel=1e-3)
+
+
+def test_clock_sampler_keeps_readings_inside_the_timed_region(tmp_path, monkeypatch):
+    """bench.py's clock sampler, driven by a stand-in nvidia-smi that prints a
+    timestamped reading every 50 ms: it waits for the first reading, keeps only
+    those stamped inside the region, and names active slowdown reasons."""
+    import sys
+    import time
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text(
+        "#!" + sys.executable + "\n"
+        "import datetime, sys, time\n"
+        "time.sleep(0.3)\n"
+        "i = 0\n"
+        "while True:\n"
+        "    t = datetime.datetime.now().strftime('%Y/%m/%d %H:%M:%S.%f')[:-3]\n"
+        "    slow = 'Active' if i == 3 else 'Not Active'\n"
+        "    print(f'{t}, 0, 1965, 1965, 700.00, 0x0, Not Active, Not Active, {slow}, Not Active',"
+        " flush=True)\n"
+        "    i += 1\n"
+        "    time.sleep(0.05)\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", str(tmp_path) + os.pathsep + os.environ["PATH"])
+    import bench
+    with bench.ClockSampler(0) as clk:
+        time.sleep(0.5)
+    s = clk.summary()
+    # about 10 readings in 0.5 s; none of the 0.3 s start-up is in the region
+    assert 5 <= s["samples"] <= 12, s
+    assert s["sm_mhz"] == 1965.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_thermal_slowdown"], s
+    with bench.ClockSampler(0) as clk:
+        pass
+    assert clk.summary()["samples"] <= 1
