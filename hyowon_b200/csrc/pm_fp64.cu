@@ -405,8 +405,10 @@ __device__ __forceinline__ bool gather_axis_fast(const double (&c)[2][2][2], con
 // potential values of the 4x4x4 stencil footprint are loaded once: the 2x2x2
 // block first, then the two outer faces of one axis at a time, so each axis
 // sum is formed in the reference's corner order with few values live.
+// Five blocks per SM (48 registers, the rest spilled to L1) hide the stencil
+// loads' latency best: at c3 7.31 ms against 7.80 at four and 8.18 at three.
 #ifndef HYOWON_GATHER64_MINB
-#define HYOWON_GATHER64_MINB 3
+#define HYOWON_GATHER64_MINB 5
 #endif
 template <typename IDX>
 __global__ void __launch_bounds__(kThreads, HYOWON_GATHER64_MINB)
