@@ -276,8 +276,16 @@ inline int deposit_rows(int N) {
     return ty > N ? N : ty;
 }
 
+#ifndef HYOWON_DEPOSIT_MINB
+#define HYOWON_DEPOSIT_MINB 0
+#endif
+#if HYOWON_DEPOSIT_MINB > 0
+#define HYOWON_DEPOSIT_BOUNDS __launch_bounds__(kDepositThreads, HYOWON_DEPOSIT_MINB)
+#else
+#define HYOWON_DEPOSIT_BOUNDS __launch_bounds__(kDepositThreads)
+#endif
 template <typename OUT>
-__global__ void __launch_bounds__(kDepositThreads)
+__global__ void HYOWON_DEPOSIT_BOUNDS
 k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy,
                 const uint32_t* __restrict__ uz, const uint32_t* __restrict__ order,
                 const uint32_t* __restrict__ offset, int shift, int N, int TY,
