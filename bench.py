@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--form", default="fp32", choices=["fp64", "fp32"])
+    ap.add_argument("--sort-interval", type=int, default=None,
+                    help="re-sort the particles every this many steps (library default 4)")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip timing the other arithmetic form")
     ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c3h"])
@@ -434,6 +436,8 @@ def main():
         """Device-resident K-step throughput of one arithmetic form."""
         solver = hb.PMSolver(hb.MeshGeometry(L, N), hb.PMForceMethod.pure_pm(False), form)
         ic.lpt_on_device(solver, noise, n_side, a0, m_p)
+        if args.sort_interval is not None:
+            solver.set_sort_interval(args.sort_interval)
         ics = solver.download(acc=False) if (not args.no_e2e and form == args.form) else None
         solver.solve_forces()
         solver.set_timing(True)
@@ -542,7 +546,8 @@ def main():
             "config": {"workload": args.config, "form": args.form, "particles": n, "mesh": N,
                        "box": L, "z_start": c["z_start"], "seed": c["seed"],
                        "l2": "inputs larger than L2 (meshes and particle arrays >> 126 MB)",
-                       "parallelism": f"replicas{world}"},
+                       "parallelism": f"replicas{world}",
+                       "sort_interval": 4 if args.sort_interval is None else args.sort_interval},
             "phases_ms_avg": phases,
             "other_form": compare,
             "roofline": roofline,

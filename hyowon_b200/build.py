@@ -25,6 +25,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "-I", os.path.join(ROOT, "include"), "-I", CSRC, "--expt-relaxed-constexpr"]
+# Extra nvcc flags for every unit, e.g. HYOWON_NVCC_DEFS="-DHYOWON_KICK32_MINB=4" to
+# build a tuning variant (pass --force: the object files do not track flags).
+COMMON += os.environ.get("HYOWON_NVCC_DEFS", "").split()
 
 # (source, extra flags)
 UNITS = [
