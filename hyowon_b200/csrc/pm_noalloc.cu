@@ -11,9 +11,11 @@
 // per call from n * max mass), which also makes the result independent of the
 // order in which atomics land: two calls on the same input give the same bits.
 //
-// Set-up: the first call on each device resolves the scratch address with
-// cudaGetSymbolAddress (this can load the module and so may allocate inside the
-// driver); make one call on a device before capturing work on it.
+// Set-up: the first call on each device (and again after the device's driver
+// context changes, e.g. after cudaDeviceReset) resolves the scratch address
+// with cudaGetSymbolAddress, with that device current; this can load the
+// module and so may allocate inside the driver. The call is synchronous and
+// reads a status word back, so it refuses a capturing stream (HYOWON_EINVAL).
 //
 // Zeroing: the header and the first N^3 accumulation cells must start at zero;
 // every call zeroes them itself as its first kernel, so nothing is required of
@@ -95,10 +97,7 @@ __global__ void k_na_deposit(uint32_t n, const double* __restrict__ x,
                              unsigned long long* scratch) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || scratch[0] != 0ull) return;
-    const double max_mass = mass ? __longlong_as_double(static_cast<long long>(scratch[1]))
-                                 : uniform_mass;
-    if (!(max_mass > 0.0)) return;  // all-zero masses: the mesh stays zero
-    const int S = fixed_exponent(n, max_mass);
+    // Cell assignment first: a non-finite position is an error whatever the masses.
     int ix, iy, iz;
     double tx, ty, tz;
     if (!(cic_coord_f64(x[i], a, ix, tx) & cic_coord_f64(y[i], a, iy, ty)
@@ -106,6 +105,15 @@ __global__ void k_na_deposit(uint32_t n, const double* __restrict__ x,
         atomicOr(&scratch[0], static_cast<unsigned long long>(ST_CELL_ESCAPE));
         return;
     }
+    const double max_mass = mass ? __longlong_as_double(static_cast<long long>(scratch[1]))
+                                 : uniform_mass;
+    if (!(max_mass > 0.0)) return;  // all-zero masses: the mesh stays zero
+    if (!isfinite(static_cast<double>(n) * max_mass)) {
+        // the fixed-point exponent needs a finite total-mass bound
+        atomicOr(&scratch[0], static_cast<unsigned long long>(ST_NONFINITE_INPUT));
+        return;
+    }
+    const int S = fixed_exponent(n, max_mass);
     const double m = mass ? mass[i] : uniform_mass;
     const double wx[2] = {1.0 - tx, tx};
     const double wy[2] = {1.0 - ty, ty};
@@ -141,7 +149,7 @@ __global__ void k_na_to_mesh(uint32_t n, uint32_t cells_n, const double* __restr
     if (c >= cells_n || scratch[0] != 0ull) return;
     const double max_mass = mass ? __longlong_as_double(static_cast<long long>(scratch[1]))
                                  : uniform_mass;
-    if (!(max_mass > 0.0) || n == 0) {
+    if (!(max_mass > 0.0) || n == 0 || !isfinite(static_cast<double>(n) * max_mass)) {
         mesh[c] = 0.0;
         return;
     }
@@ -150,7 +158,10 @@ __global__ void k_na_to_mesh(uint32_t n, uint32_t cells_n, const double* __restr
 }
 
 std::mutex g_lock[kMaxDevices];
+// Scratch address per device, valid for the driver context it was resolved in
+// (a cudaDeviceReset or another context on the device needs a new address).
 unsigned long long* g_scratch_ptr[kMaxDevices] = {};
+CUcontext g_scratch_ctx[kMaxDevices] = {};
 thread_local char g_err[256] = "";
 
 int fail(int code, const char* fmt, ...) {
@@ -164,30 +175,41 @@ int fail(int code, const char* fmt, ...) {
 // cuMemGetAddressRange through the runtime's driver entry point (no link-time
 // dependency on libcuda): the allocation that contains a device pointer.
 using AddressRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+
+template <typename F>
+F driver_fn(const char* name) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint(name, &f, cudaEnableDefault, &q) != cudaSuccess
+        || q != cudaDriverEntryPointSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return reinterpret_cast<F>(f);
+}
 
 AddressRangeFn address_range_fn() {
-    static AddressRangeFn fn = [] {
-        void* f = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q)
-                != cudaSuccess
-            || q != cudaDriverEntryPointSuccess) {
-            cudaGetLastError();
-            return static_cast<AddressRangeFn>(nullptr);
-        }
-        return reinterpret_cast<AddressRangeFn>(f);
-    }();
+    static AddressRangeFn fn = driver_fn<AddressRangeFn>("cuMemGetAddressRange");
     return fn;
 }
 
-// True when [p, p + bytes) is device (or managed) memory inside one allocation.
-bool device_extent_ok(const void* p, uint64_t bytes) {
+CtxGetCurrentFn ctx_get_current_fn() {
+    static CtxGetCurrentFn fn = driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+    return fn;
+}
+
+// True when [p, p + bytes) is device memory of device `dev` (or managed
+// memory) inside one allocation. Another GPU's memory is refused: the kernels
+// would read and write it over the peer path, or fault without peer access.
+bool device_extent_ok(const void* p, uint64_t bytes, int dev) {
     cudaPointerAttributes at{};
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
     if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) return false;
+    if (at.type == cudaMemoryTypeDevice && at.device != dev) return false;
     AddressRangeFn fn = address_range_fn();
     if (!fn) return false;
     CUdeviceptr base = 0;
@@ -216,8 +238,10 @@ extern "C" int hyowon_cic_deposit_noalloc(double box_size, uint64_t mesh_size, u
                     "mesh size %llu outside [2, %d]: the static scratch holds at most %d^3 cells",
                     static_cast<unsigned long long>(mesh_size), kMaxMesh, kMaxMesh);
     if (n >= (1ull << 32)) return fail(HYOWON_EINVAL, "particle count must be below 2^32");
-    if (!masses && !(std::isfinite(uniform_mass) && uniform_mass >= 0.0))
-        return fail(HYOWON_EINVAL, "uniform mass must be finite and non-negative");
+    if (!masses && !(std::isfinite(uniform_mass) && uniform_mass >= 0.0
+                     && std::isfinite(static_cast<double>(n) * uniform_mass)))
+        return fail(HYOWON_EINVAL,
+                    "uniform mass must be finite and non-negative, with n * mass finite");
     if (!mesh || (n > 0 && (!x || !y || !z)))
         return fail(HYOWON_EINVAL, "null position or mesh pointer");
     int dev = 0;
@@ -227,17 +251,34 @@ extern "C" int hyowon_cic_deposit_noalloc(double box_size, uint64_t mesh_size, u
     }
     const uint64_t pbytes = n * sizeof(double);
     const uint64_t mbytes = mesh_size * mesh_size * mesh_size * sizeof(double);
-    if (!device_extent_ok(mesh, mbytes))
-        return fail(HYOWON_EINVAL, "mesh must be device memory of at least %llu bytes",
-                    static_cast<unsigned long long>(mbytes));
-    if (n > 0 && (!device_extent_ok(x, pbytes) || !device_extent_ok(y, pbytes)
-                  || !device_extent_ok(z, pbytes) || (masses && !device_extent_ok(masses, pbytes))))
+    if (!device_extent_ok(mesh, mbytes, dev))
         return fail(HYOWON_EINVAL,
-                    "positions and masses must be device memory of at least %llu bytes each",
-                    static_cast<unsigned long long>(pbytes));
+                    "mesh must be device memory of the current device (%d), at least %llu bytes",
+                    dev, static_cast<unsigned long long>(mbytes));
+    if (n > 0 && (!device_extent_ok(x, pbytes, dev) || !device_extent_ok(y, pbytes, dev)
+                  || !device_extent_ok(z, pbytes, dev)
+                  || (masses && !device_extent_ok(masses, pbytes, dev))))
+        return fail(HYOWON_EINVAL,
+                    "positions and masses must be device memory of the current device (%d), "
+                    "at least %llu bytes each",
+                    dev, static_cast<unsigned long long>(pbytes));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HYOWON_EINVAL, "stream is not usable on the current device");
+    }
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(HYOWON_EINVAL,
+                    "the call waits for its own work and reads a status word back, so it "
+                    "cannot be issued on a capturing stream");
 
     std::lock_guard<std::mutex> guard(g_lock[dev]);
-    if (!g_scratch_ptr[dev]) {
+    CUcontext ctx = nullptr;
+    CtxGetCurrentFn get_ctx = ctx_get_current_fn();
+    if (!get_ctx || get_ctx(&ctx) != CUDA_SUCCESS || !ctx)
+        return fail(HYOWON_ECUDA, "no current CUDA context on device %d", dev);
+    if (!g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) {
@@ -245,9 +286,9 @@ extern "C" int hyowon_cic_deposit_noalloc(double box_size, uint64_t mesh_size, u
             return fail(HYOWON_ECUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
         }
         g_scratch_ptr[dev] = static_cast<unsigned long long*>(p);
+        g_scratch_ctx[dev] = ctx;
     }
     unsigned long long* scratch = g_scratch_ptr[dev];
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
 
     const int N = static_cast<int>(mesh_size);
     const uint32_t cells = static_cast<uint32_t>(mesh_size * mesh_size * mesh_size);
@@ -257,13 +298,17 @@ extern "C" int hyowon_cic_deposit_noalloc(double box_size, uint64_t mesh_size, u
     a.dx = box_size / static_cast<double>(N);
     a.upper = std::nextafter(static_cast<double>(N), 0.0);
     a.N = N;
-    constexpr int T = 256;
-    k_na_zero<<<static_cast<unsigned>((kHeaderWords + cells + T - 1) / T), T, 0, s>>>(scratch, cells);
+    constexpr uint64_t T = 256;
+    // block counts in 64 bits: n may be as large as 2^32 - 1
+    const unsigned zero_blocks = static_cast<unsigned>((kHeaderWords + cells + T - 1) / T);
+    const unsigned particle_blocks = static_cast<unsigned>((n + T - 1) / T);
+    const unsigned cell_blocks = static_cast<unsigned>((static_cast<uint64_t>(cells) + T - 1) / T);
+    k_na_zero<<<zero_blocks, T, 0, s>>>(scratch, cells);
     if (nn > 0) {
-        if (masses) k_na_max_mass<<<(nn + T - 1) / T, T, 0, s>>>(nn, masses, scratch);
-        k_na_deposit<<<(nn + T - 1) / T, T, 0, s>>>(nn, x, y, z, masses, uniform_mass, a, scratch);
+        if (masses) k_na_max_mass<<<particle_blocks, T, 0, s>>>(nn, masses, scratch);
+        k_na_deposit<<<particle_blocks, T, 0, s>>>(nn, x, y, z, masses, uniform_mass, a, scratch);
     }
-    k_na_to_mesh<<<(cells + T - 1) / T, T, 0, s>>>(nn, cells, masses, uniform_mass, scratch, mesh);
+    k_na_to_mesh<<<cell_blocks, T, 0, s>>>(nn, cells, masses, uniform_mass, scratch, mesh);
     unsigned long long status = 0ull;
     cudaError_t e = cudaMemcpyAsync(&status, scratch, sizeof(status), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -272,7 +317,8 @@ extern "C" int hyowon_cic_deposit_noalloc(double box_size, uint64_t mesh_size, u
         return fail(HYOWON_ECUDA, "deposit launch: %s", cudaGetErrorString(e));
     }
     if (status & ST_NONFINITE_INPUT)
-        return fail(HYOWON_EINVAL, "non-finite or negative particle mass");
+        return fail(HYOWON_EINVAL,
+                    "particle masses must be finite and non-negative, with n * max mass finite");
     if (status & ST_CELL_ESCAPE)
         return fail(HYOWON_ELOGIC, "non-finite position: CIC cell assignment left the mesh");
     return HYOWON_OK;

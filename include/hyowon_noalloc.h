@@ -30,14 +30,18 @@ extern "C" {
  * deposit to about n * 2^-61 relative to the total mass.
  *
  * x, y, z (n each), masses (n, or NULL for uniform_mass) and mesh are DEVICE
- * pointers on the current device; stream is a cudaStream_t (NULL: the legacy
- * default stream). The call allocates nothing, enqueues its kernels on stream
- * and waits for them; it returns HYOWON_OK, HYOWON_EINVAL (mesh_size outside
- * [2, HYOWON_NOALLOC_MAX_MESH], n >= 2^32, host or too-small buffers, a
- * non-finite or negative mass), HYOWON_ELOGIC (a non-finite position) or
- * HYOWON_ECUDA. On an error the mesh is not written. The first call on a
- * device sets up the scratch address; make it before capturing stream work.
- * Calls on one device are serialised: they share the scratch.
+ * pointers of the current device (another GPU's memory is refused); stream is
+ * a cudaStream_t of that device (NULL: the legacy default stream). The call
+ * allocates nothing, enqueues its kernels on stream and waits for them; it
+ * returns HYOWON_OK, HYOWON_EINVAL (mesh_size outside
+ * [2, HYOWON_NOALLOC_MAX_MESH], n >= 2^32, host, peer or too-small buffers, a
+ * non-finite or negative mass, n * max mass not finite, a capturing stream),
+ * HYOWON_ELOGIC (a non-finite position, whatever the masses) or HYOWON_ECUDA.
+ * On an error the mesh is not written. The first call on a device (and the
+ * first after its driver context changes, e.g. after cudaDeviceReset) resolves
+ * the scratch address with that device current. The call is synchronous and
+ * reads a status word back, so it cannot be issued on a stream that is being
+ * captured. Calls on one device are serialised: they share the scratch.
  */
 int hyowon_cic_deposit_noalloc(double box_size, uint64_t mesh_size, uint64_t n,
                                const double* x, const double* y, const double* z,

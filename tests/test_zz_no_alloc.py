@@ -115,3 +115,50 @@ def test_noalloc_deposit_errors_leave_mesh_untouched():
                                         None, 1.0, host.ctypes.data, stream)
     assert rc == 1
     assert "device memory" in lib.hyowon_noalloc_last_error().decode()
+    # pinned host memory is not device memory either
+    pinned = torch.zeros(N ** 3, dtype=torch.float64).pin_memory()
+    rc = lib.hyowon_cic_deposit_noalloc(L, N, n, dx.data_ptr(), dy.data_ptr(), dz.data_ptr(),
+                                        None, 1.0, pinned.data_ptr(), stream)
+    assert rc == 1
+    assert torch.all(pinned == 0.0).item()
+
+
+@pytest.mark.gpu
+def test_noalloc_deposit_checks_positions_and_mass_range_whatever_the_masses():
+    """A non-finite position fails even when every mass is zero (nothing would
+    be deposited), and masses whose total n * max_mass overflows binary64 are
+    refused instead of giving a meaningless fixed-point scale."""
+    import torch
+
+    lib = noalloc_lib()
+    dev = torch.device("cuda", 0)
+    N, n, L = 16, 1000, 10.0
+    rng = np.random.default_rng(5)
+    pos = [rng.uniform(0.0, L, n) for _ in range(3)]
+    pos[2][11] = np.inf
+    dx, dy, dz = (torch.from_numpy(a).to(dev) for a in pos)
+    mesh = torch.full((N ** 3,), 7.0, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    rc = lib.hyowon_cic_deposit_noalloc(L, N, n, dx.data_ptr(), dy.data_ptr(), dz.data_ptr(),
+                                        None, 0.0, mesh.data_ptr(), stream)
+    assert rc == 2, lib.hyowon_noalloc_last_error().decode()
+    zero = torch.zeros(n, dtype=torch.float64, device=dev)
+    rc = lib.hyowon_cic_deposit_noalloc(L, N, n, dx.data_ptr(), dy.data_ptr(), dz.data_ptr(),
+                                        zero.data_ptr(), 0.0, mesh.data_ptr(), stream)
+    assert rc == 2, lib.hyowon_noalloc_last_error().decode()
+    assert torch.all(mesh == 7.0).item()
+    pos[2][11] = 1.0
+    dz = torch.from_numpy(pos[2]).to(dev)
+    huge = torch.full((n,), 1e306, dtype=torch.float64, device=dev)
+    rc = lib.hyowon_cic_deposit_noalloc(L, N, n, dx.data_ptr(), dy.data_ptr(), dz.data_ptr(),
+                                        huge.data_ptr(), 0.0, mesh.data_ptr(), stream)
+    assert rc == 1, lib.hyowon_noalloc_last_error().decode()
+    assert torch.all(mesh == 7.0).item()
+    rc = lib.hyowon_cic_deposit_noalloc(L, N, n, dx.data_ptr(), dy.data_ptr(), dz.data_ptr(),
+                                        None, 1e306, mesh.data_ptr(), stream)
+    assert rc == 1
+    # all-zero masses with finite positions give an empty mesh
+    rc = lib.hyowon_cic_deposit_noalloc(L, N, n, dx.data_ptr(), dy.data_ptr(), dz.data_ptr(),
+                                        zero.data_ptr(), 0.0, mesh.data_ptr(), stream)
+    assert rc == 0, lib.hyowon_noalloc_last_error().decode()
+    assert torch.all(mesh == 0.0).item()
