@@ -225,9 +225,9 @@ def phase_bytes(form, n, N, sort_fraction):
 
 
 # DRAM bytes (read + write) per launch of the single-kernel phases on the c3
-# workload, from the ncu --set full capture of the half-size c3 workload (c3h:
-# 1/8 of the particles and mesh cells, profiles/step_kernels_c3h.md) times 8;
-# each kernel's traffic scales with the particles and cells it processes.
+# workload, from an ncu --set full capture of the half-size c3 workload (c3h:
+# 1/8 of the particles and mesh cells) times 8; each kernel's traffic scales
+# with the particles and cells it processes.
 TRAFFIC_C3 = {
     ("fp32", "deposit"): 8 * (273 + 484) * 1e6,
     ("fp32", "green"): 8 * (554 + 499) * 1e6,
@@ -239,29 +239,35 @@ TRAFFIC_C3 = {
 
 
 def run_reference(args, world, rank):
-    """The reference's own CPU implementation (oracle/_ref) on the host cores."""
+    """The reference's own CPU implementation (oracle/_ref) on the host cores.
+
+    Nothing of the product package runs here: the initial conditions come
+    from oracle/workload.py and the reference's own LinearPowerSpectrum, FFT
+    and LPTDisplacement; the timed region is the reference's TimeStepper +
+    LeapfrogIntegrator + PMSolver loop."""
     if rank != 0:
         return
-    from hyowon_b200 import ic
-    from oracle.bindings import Reference
-    from oracle.lpt_oracle import lpt_ics
-    cfg_name = args.config
-    c = ic.CONFIGS[cfg_name]
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    from oracle import workload
+    from oracle.bindings import Reference
+    cfg_name = args.config
+    c = workload.CONFIGS[cfg_name]
     ref = Reference()
-    a0, dl = ic.config_schedule(cfg_name)
-    # Bounded sample of the workload: the first steps of the schedule; the c3
-    # workload (31 GB of host RAM in the reference) is sampled one step at a time.
+    a0, dl = workload.schedule(cfg_name)
     n_side = c["n_side"]
-    noise = ic.white_noise(n_side, c["seed"])
-    st = lpt_ics(noise, n_side, c["box"], a0)
+    st = workload.reference_ics(ref, cfg_name)
     for k in ("ax", "ay", "az"):
         st[k] = np.zeros_like(st["x"])
-    m_p = ic.particle_mass(c["box"], n_side)
+    m_p = workload.particle_mass(c["box"], n_side)
+    # Bounded sample of the workload: the first steps of the schedule; the c3
+    # workload (31 GB of host RAM in the reference) is sampled two steps at a time.
     steps = max(1, min(args.steps, 2 if cfg_name == "c3" else args.steps))
     _, secs = ref.kdk_run(c["box"], c["mesh"], st, a0, 1.0, dl, steps, m_p)
     value = n_side ** 3 * steps / secs
+    libs = workload.loaded_native_libraries()
+    if any("hyowon_b200" in lib for lib in libs):
+        raise RuntimeError(f"the reference arm loaded the product library: {libs}")
     line = {
         "impl": "reference", "metric": "particle-steps/s", "value": value,
         "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": steps, "warmup": 0,
@@ -271,37 +277,43 @@ def run_reference(args, world, rank):
                    "box": c["box"]},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
                          "kind": "reference",
-                         "sample": f"{steps} KDK step(s) of {cfg_name} after the initial force"},
+                         "sample": f"{steps} KDK step(s) of {cfg_name} after the initial force; "
+                                   f"reference Release build (-O3 -DNDEBUG, OpenMP on, "
+                                   f"OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS')}, "
+                                   f"OMP_PROC_BIND={os.environ.get('OMP_PROC_BIND', 'unset')}), "
+                                   f"FFT: oracle/fft3d.c in place of FFTW3 (not installed)"},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "native_libraries": libs,
     }
     print(json.dumps(line), flush=True)
 
 
 def cpu_baseline_sample(cfg_name):
     """Times the reference (oracle/_ref) on a bounded sample: KDK steps of the
-    c2-sized problem when the full configuration would exceed ~30 s."""
+    c2-sized problem when the full configuration would exceed ~30 s. Its
+    initial conditions are the reference's own (oracle/workload.py)."""
     try:
-        from hyowon_b200 import ic
+        from oracle import workload
         from oracle.bindings import Reference
-        from oracle.lpt_oracle import lpt_ics
         ref = Reference()
     except Exception as e:  # pragma: no cover
         return {"value": None, "unit": "particle-steps/s", "cores": os.cpu_count(),
                 "kind": "reference", "sample": f"unavailable: {e}"}
     name = "c2" if cfg_name in ("c3", "c3h") else cfg_name
-    c = ic.CONFIGS[name]
-    a0, dl = ic.config_schedule(name)
-    st = lpt_ics(ic.white_noise(c["n_side"], c["seed"]), c["n_side"], c["box"], a0)
+    c = workload.CONFIGS[name]
+    a0, dl = workload.schedule(name)
+    st = workload.reference_ics(ref, name)
     for k in ("ax", "ay", "az"):
         st[k] = np.zeros_like(st["x"])
-    steps = 3 if name == "c2" else 8
+    steps = 8 if name == "c2" else 16
     _, secs = ref.kdk_run(c["box"], c["mesh"], st, a0, 1.0, dl, steps,
-                          ic.particle_mass(c["box"], c["n_side"]))
+                          workload.particle_mass(c["box"], c["n_side"]))
     return {"value": c["n_side"] ** 3 * steps / secs, "unit": "particle-steps/s",
             "cores": os.cpu_count(), "kind": "reference",
             "sample": f"{steps} KDK steps of {name} ({c['n_side']}^3 particles, "
-                      f"{c['mesh']}^3 mesh) on all host threads"}
+                      f"{c['mesh']}^3 mesh) on all host threads, reference Release build "
+                      f"with OpenMP"}
 
 
 IC_WORKLOAD = dict(n_side=512, box=1000.0, z_start=49.0, seed=7, lpt_order=2)
@@ -319,13 +331,13 @@ def ic_cpu_baseline():
     """The reference's RandomField + LPTDisplacement (oracle/_ref) on the host
     cores for the 64^3 lattice, 2LPT, 128^3 IC mesh (same cell size)."""
     try:
-        from hyowon_b200 import ic
+        from oracle import workload
         from oracle.bindings import Reference, write_power_spectrum_file
         ref = Reference()
     except Exception as e:  # pragma: no cover
         return {"value": None, "unit": "particles/s", "cores": os.cpu_count(),
                 "kind": "reference", "sample": f"unavailable: {e}"}
-    k, P = ic.bbks_table()
+    k, P = workload.bbks_table()
     with tempfile.TemporaryDirectory() as tmp:
         path = os.path.join(tmp, "pk.txt")
         write_power_spectrum_file(path, k, P, 0.0)
@@ -438,7 +450,7 @@ def main():
         ic.lpt_on_device(solver, noise, n_side, a0, m_p)
         if args.sort_interval is not None:
             solver.set_sort_interval(args.sort_interval)
-        ics = solver.download(acc=False) if (not args.no_e2e and form == args.form) else None
+        ics = solver.download(acc=False) if not args.no_e2e else None
         solver.solve_forces()
         solver.set_timing(True)
         solver.run(K1[:args.warmup], D[:args.warmup], K2[:args.warmup])
@@ -493,8 +505,7 @@ def main():
                      "frac": step_bytes / (ms_per_step * 1e-3) / 1e9 / hbm}
 
     # -- end to end through the C ABI with host buffers -------------------------
-    e2e = None
-    if not args.no_e2e:
+    def measure_e2e(e2e_solver, ics):
         import torch
         comps = ("x", "y", "z", "px", "py", "pz")
         pinned = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in comps}
@@ -502,7 +513,6 @@ def main():
         for k in comps:
             pinned[k][:] = ics[k]
             result[k][:] = 0.0   # touch the pages before the timed region
-        e2e_solver = solver
         t0 = time.perf_counter()
         e2e_solver.upload(pinned["x"], pinned["y"], pinned["z"], pinned["px"], pinned["py"],
                           pinned["pz"], uniform_mass=m_p)
@@ -514,23 +524,46 @@ def main():
             e2e_secs = max_over_ranks(e2e_secs * 1e3) * 1e-3
         h2d = 6 * 8 * n + 24 * args.steps
         d2h = 6 * 8 * n + 8 * args.steps
-        e2e = {"value": whole_job_rate(world, n, args.steps, e2e_secs * 1e3),
-               "unit": "particle-steps/s",
-               "h2d_bytes_per_step": h2d / args.steps,
-               "d2h_bytes_per_step": d2h / args.steps,
-               "note": "pinned host buffers: upload of the IC positions and momenta, K "
-                       "hyowon_pm_kdk_step calls (K1, D, K2 in, max drift out), download of "
-                       "the final positions and momenta"}
+        return {"value": whole_job_rate(world, n, args.steps, e2e_secs * 1e3),
+                "unit": "particle-steps/s",
+                "h2d_bytes_per_step": h2d / args.steps,
+                "d2h_bytes_per_step": d2h / args.steps,
+                "note": "pinned host buffers: upload of the IC positions and momenta, K "
+                        "hyowon_pm_kdk_step calls (K1, D, K2 in, max drift out), download of "
+                        "the final positions and momenta"}
 
+    e2e = None if args.no_e2e else measure_e2e(solver, ics)
+    final = solver.download() if args.form == "fp64" else None
     solver.close()
     compare = None
     if not args.no_compare:
         other = "fp64" if args.form == "fp32" else "fp32"
-        s2, _, t2, dev2, _, _ = measure(other)
+        s2, ics2, t2, dev2, _, _ = measure(other)
+        e2e2 = None if args.no_e2e else measure_e2e(s2, ics2)
+        if other == "fp64":
+            final = s2.download()
         s2.close()
         v2 = whole_job_rate(world, n, args.steps, dev2)
         compare = {"form": other, "value": v2, "ms_per_step": dev2 / args.steps,
-                   "ratio_fp32_over_fp64": (value / v2) if args.form == "fp32" else (v2 / value)}
+                   "ratio_fp32_over_fp64": (value / v2) if args.form == "fp32" else (v2 / value),
+                   "e2e": e2e2}
+
+    # -- the precision form's force error at the state the binary64 run reached
+    force_error = None
+    if final is not None:
+        with hb.PMSolver(hb.MeshGeometry(L, N), hb.PMForceMethod.pure_pm(False), "fp32") as s3:
+            s3.upload(final["x"], final["y"], final["z"], uniform_mass=m_p)
+            s3.solve_forces()
+            f32 = s3.download()
+        num = sum(float(np.sum((f32[k] - final[k]) ** 2)) for k in ("ax", "ay", "az"))
+        den = sum(float(np.sum(final[k] ** 2)) for k in ("ax", "ay", "az"))
+        # the binary64 handle last ran the e2e leg (K steps from the ICs), else W + K
+        reached = args.steps if not args.no_e2e else total_steps
+        a_end = a0 * math.exp(dl * reached) if reached <= c["steps"] else None
+        force_error = {"fp32_vs_fp64_force_rel_rms": math.sqrt(num / den),
+                       "state": f"the binary64 run's state after {reached} steps from the ICs"
+                                + (f" (a = {a_end:.4f})" if a_end else ""),
+                       "particles": n}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -554,6 +587,7 @@ def main():
             "step_roofline": step_roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "force_error": force_error,
             "gpu_launches": launches,
             "clocks": clock_summary,
             "wall_s_timed_region": wall,

@@ -40,12 +40,29 @@ def build_oracle() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def build_reference(ref_root: str = "/root/reference") -> bool:
+def reference_root(ref_root: str | None = None) -> str:
+    """The reference source tree: the argument, else $HYOWON_REF_ROOT, else
+    the REF_ROOT default of oracle/ref/Makefile (the recipe that reads it)."""
+    if ref_root:
+        return ref_root
+    env = os.environ.get("HYOWON_REF_ROOT")
+    if env:
+        return env
+    with open(os.path.join(HERE, "ref", "Makefile")) as f:
+        for line in f:
+            if line.startswith("REF_ROOT") and "?=" in line:
+                return line.split("?=", 1)[1].strip()
+    return ""
+
+
+def build_reference(ref_root: str | None = None) -> bool:
     """Compile the reference's hot path into oracle/_ref when its tree exists."""
-    if not os.path.isdir(ref_root):
+    root = reference_root(ref_root)
+    if not root or not os.path.isdir(root):
         return os.path.exists(REF_SO)
-    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"),
-                    f"REF_ROOT={ref_root}"], check=True)
+    jobs = str(max(1, min(16, os.cpu_count() or 1)))
+    subprocess.run(["make", "-s", f"-j{jobs}", "-C", os.path.join(HERE, "ref"),
+                    f"REF_ROOT={root}"], check=True)
     return True
 
 
@@ -397,6 +414,23 @@ class Reference:
         if particles:
             out.update(st)
         return out
+
+    def lpt_white_noise(self, L, N, noise, pk_path, z_pk, z_start):
+        """1LPT state from white noise through the reference's LinearPowerSpectrum,
+        FFTBackend and LPTDisplacement (ref_lpt_white_noise). Returns a dict
+        x..pz plus a_start, D1, f1, H."""
+        noise = np.ascontiguousarray(noise, dtype=np.float64).reshape(-1)
+        if noise.size != N ** 3:
+            raise ValueError("noise must hold N^3 values")
+        meta = np.zeros(4)
+        st = {k: np.zeros(N ** 3) for k in ("x", "y", "z", "px", "py", "pz")}
+        self.lib.ref_lpt_white_noise.argtypes = None
+        rc = self.lib.ref_lpt_white_noise(_c_double(L), _c_u64(N), _dp(noise), pk_path.encode(),
+                                          _c_double(z_pk), _c_double(z_start), _dp(meta),
+                                          *(_dp(st[k]) for k in ("x", "y", "z", "px", "py", "pz")))
+        self._check(rc, "ref_lpt_white_noise")
+        st.update(a_start=meta[0], D1=meta[1], f1=meta[2], H=meta[3])
+        return st
 
 
 # The semantic header LinearPowerSpectrum requires

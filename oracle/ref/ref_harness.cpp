@@ -45,6 +45,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <numbers>
 #include <optional>
 #include <span>
 #include <stdexcept>
@@ -676,4 +677,103 @@ int ref_generate_ics(double L, std::uint64_t N, std::uint64_t mesh_request, std:
     });
 }
 
+// First-order LPT initial conditions from seeded white noise w[N^3] (unit
+// variance per lattice cell), the configs' IC recipe driven through the
+// reference's own classes: the spectrum is the reference's
+// LinearPowerSpectrum (natural cubic log-log spline of the P(k) file at
+// z_pk, scaled to z_start, src/ic/linear_power_spectrum.cpp:649-664), the r2c
+// is the reference's FFTBackend (this build's shim), delta_k = r2c(w)
+// * sqrt(P(k) N^3 / L^3) (the variance normalisation of
+// src/ic/random_field.cpp:119-129 for noise of unit variance per cell,
+// k = 0 set to zero), and the displacement and momenta are
+// LPTDisplacement::apply_to_arrays (src/ic/lpt_displacement.cpp:150-384) on the
+// corner lattice of src/ic/initial_conditions.cpp:295-313. meta receives
+// a_start, D1, f1, H at a_start.
+int ref_lpt_white_noise(double L, std::uint64_t N, const double* noise, const char* pk_path,
+                        double z_pk, double z_start, double* meta, double* x, double* y,
+                        double* z, double* px, double* py, double* pz) {
+    return guarded([&] {
+        config::GravityParams g;
+        g.solver = "PM";
+        g.deconvolve_cic = core::ExplicitBoolean(false);
+        config::BoxParams b;
+        b.L = L;
+        b.N = N;
+        b.N_mesh = N;
+        config::TimeParams t;
+        t.z_start = z_start;
+        t.z_final = 0.0;
+        t.delta_ln_a = 0.1;
+        config::ICParams ic;
+        ic.mode = "generate";
+        ic.lpt_order = 1;
+        ic.seed = 1;
+        ic.mesh_per_dimension = N;
+        ic.power_spectrum_file = pk_path;
+        ic.power_spectrum_redshift = z_pk;
+        ic.power_spectrum_fidelity = "precision_boltzmann";
+        ic.amplitude_mode = "gaussian";
+        ic.phase_pairing = "independent";
+        config::OutputParams o;
+        config::SimulationParameters cfg(flat_lcdm(0.3, 0.7), b, g, t, ic, o);
+        cosmology::CosmologyModel cosmo(cfg.get_cosmology());
+        const double a0 = 1.0 / (1.0 + z_start);
+        if (meta) {
+            meta[0] = a0;
+            meta[1] = cosmo.D1(a0);
+            meta[2] = cosmo.f1(a0);
+            meta[3] = cosmo.H(a0);
+        }
+        ic::LinearPowerSpectrum pk(cfg);
+        const mesh::MeshGeometry geom(L, N);
+        mesh::FFTBackend fft(geom);
+        mesh::RealField w(geom.real_size());
+        std::memcpy(w.data(), noise, sizeof(double) * geom.real_size());
+        mesh::ComplexField delta(geom.complex_size());
+        fft.forward(w, delta);
+        const std::uint64_t H = N / 2 + 1;
+        const double kf = 2.0 * std::numbers::pi / L;
+        const double n3_over_l3 = (static_cast<double>(N) * static_cast<double>(N)
+                                   * static_cast<double>(N)) / (L * L * L);
+#pragma omp parallel for schedule(static)
+        for (std::uint64_t i = 0; i < N; ++i) {
+            const double mx = static_cast<double>(i <= N / 2 ? static_cast<std::int64_t>(i)
+                                                             : static_cast<std::int64_t>(i) - static_cast<std::int64_t>(N));
+            for (std::uint64_t j = 0; j < N; ++j) {
+                const double my = static_cast<double>(j <= N / 2 ? static_cast<std::int64_t>(j)
+                                                                 : static_cast<std::int64_t>(j) - static_cast<std::int64_t>(N));
+                for (std::uint64_t k = 0; k < H; ++k) {
+                    const double mz = static_cast<double>(k);
+                    const std::uint64_t idx = (i * N + j) * H + k;
+                    if (i == 0 && j == 0 && k == 0) {
+                        delta[idx] = 0.0;
+                        continue;
+                    }
+                    const double kmag = kf * std::sqrt(mx * mx + my * my + mz * mz);
+                    delta[idx] *= std::sqrt(pk.evaluate(kmag) * n3_over_l3);
+                }
+            }
+        }
+        const std::uint64_t n = N * N * N;
+        std::vector<double> ax(n), ay(n), az(n), bx(n, 0.0), by(n, 0.0), bz(n, 0.0);
+        const double dx = L / static_cast<double>(N);
+        for (std::uint64_t i = 0; i < N; ++i)
+            for (std::uint64_t j = 0; j < N; ++j)
+                for (std::uint64_t k = 0; k < N; ++k) {
+                    const std::uint64_t p = (i * N + j) * N + k;
+                    ax[p] = static_cast<double>(i) * dx;
+                    ay[p] = static_cast<double>(j) * dx;
+                    az[p] = static_cast<double>(k) * dx;
+                }
+        ic::LPTDisplacement::apply_to_arrays(cfg, cosmo, fft, delta, ax, ay, az, bx, by, bz);
+        std::memcpy(x, ax.data(), sizeof(double) * n);
+        std::memcpy(y, ay.data(), sizeof(double) * n);
+        std::memcpy(z, az.data(), sizeof(double) * n);
+        std::memcpy(px, bx.data(), sizeof(double) * n);
+        std::memcpy(py, by.data(), sizeof(double) * n);
+        std::memcpy(pz, bz.data(), sizeof(double) * n);
+    });
+}
+
 }  // extern "C"
+

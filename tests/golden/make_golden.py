@@ -37,7 +37,14 @@ Fixtures:
 
     python tests/golden/make_golden.py --only diag    # c1_diag.npz alone
     python tests/golden/make_golden.py --only pk      # pk.npz alone
+  lpt.npz             the white-noise 1LPT map of the configurations through the
+                      reference (LinearPowerSpectrum of the BBKS table file,
+                      FFTBackend r2c, LPTDisplacement::apply_to_arrays on the
+                      corner lattice; oracle/workload.py + ref_lpt_white_noise):
+                      LPT_CASES (c1, and 16^3 at z = 19 in a 50 Mpc/h box)
+
     python tests/golden/make_golden.py --only ic      # ic.npz alone
+    python tests/golden/make_golden.py --only lpt     # lpt.npz alone
 """
 from __future__ import annotations
 
@@ -168,10 +175,38 @@ def ic_fixture(ref):
     np.savez_compressed(os.path.join(HERE, "ic.npz"), **out)
 
 
+# name, lattice side, box, seed, z_start
+LPT_CASES = [
+    ("c1", 32, 100.0, 1, 49.0),
+    ("s16_z19", 16, 50.0, 3, 19.0),
+]
+
+
+def lpt_fixture(ref):
+    """lpt.npz: the reference's 1LPT state from the configs' white noise."""
+    import tempfile
+    from oracle import workload
+    from oracle.bindings import write_power_spectrum_file
+    k, P = workload.bbks_table()
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "pk.txt")
+        write_power_spectrum_file(path, k, P, 0.0)
+        for name, n_side, box, seed, z_start in LPT_CASES:
+            noise = workload.white_noise(n_side, seed)
+            st = ref.lpt_white_noise(box, n_side, noise, path, 0.0, z_start)
+            out.update({f"{name}__{f}": np.asarray(st[f]) for f in
+                        ("x", "y", "z", "px", "py", "pz", "a_start", "D1", "f1", "H")})
+            out[f"{name}__args"] = np.array([n_side, box, seed, z_start])
+    np.savez_compressed(os.path.join(HERE, "lpt.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
-    ap.add_argument("--only", choices=["diag", "pk", "ic"], default=None)
+    ap.add_argument("--ref-root", default=None,
+                    help="reference source tree (default: $HYOWON_REF_ROOT, else the "
+                         "REF_ROOT default of oracle/ref/Makefile)")
+    ap.add_argument("--only", choices=["diag", "pk", "ic", "lpt"], default=None)
     args = ap.parse_args()
     build_reference(args.ref_root)
     ref = Reference()
@@ -183,6 +218,9 @@ def main():
         return
     if args.only == "ic":
         ic_fixture(ref)
+        return
+    if args.only == "lpt":
+        lpt_fixture(ref)
         return
 
     # -- schedules --------------------------------------------------------
@@ -274,6 +312,7 @@ def main():
     diag_fixture(ref)
     pk_fixture(ref)
     ic_fixture(ref)
+    lpt_fixture(ref)
     print(f"c1 reference evolution: {c['steps']} steps in {secs:.2f} s")
 
 
