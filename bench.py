@@ -11,6 +11,20 @@ inputs: no public dataset is involved.
                     [--config c1|c2|c3|c3h] [--impl ours|reference]
     python bench.py --workload ic [--steps K] [--warmup W]
 
+`--workload adjoint` times the differentiation form on its configuration
+(128^3 particles, L = 256 Mpc/h, 128^3 mesh, 1LPT at z = 19 from white noise
+seed 3, 16 KDK steps to z = 0, loss against the z = 0 CIC density of seed 4,
+checkpoints every 4 steps): a "step" is one loss-and-gradient evaluation
+(hyowon_vjp_1lpt_pm), and the line carries (forward + adjoint) / forward
+against the production forward (hyowon_pm_lpt_ics + hyowon_pm_run + the CIC
+mass mesh of the same model) in both arithmetic forms.
+
+`--workload treepm` times the TreePM force on its configuration (256^3
+particles, L = 256 Mpc/h, 256^3 mesh, r_s = 1.25 cells, r_cut = 4.5 r_s,
+opening angle 0.5, softening 1/30 of the mean spacing, the clustered z = 0
+state of a 64-step PM run of seed 5): a "step" is one KDK step with the TreePM
+force (long range plus the octree short range of every particle).
+
 `--workload ic` times HYOWON's generated initial conditions instead (the
 Philox Fourier field and 2LPT of the 512^3 lattice on the automatic 1024^3 IC
 mesh, L = 1000, z = 49): a "step" is one whole generation through
@@ -58,7 +72,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="step", choices=["step", "ic"])
+    ap.add_argument("--workload", default="step", choices=["step", "ic", "adjoint", "treepm"])
     return ap.parse_args()
 
 
@@ -410,11 +424,140 @@ def run_ic(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args, rank):
+    """Differentiation form on c4 (see the module docstring)."""
+    if rank != 0:
+        return
+    import hyowon_b200 as hb
+    from hyowon_b200 import ic
+    from hyowon_b200.adjoint import DifferentiablePM
+    c = ic.CONFIGS["c4"]
+    n_side, N, L = c["n_side"], c["mesh"], c["box"]
+    a0, dl = ic.config_schedule("c4")
+    noise = ic.white_noise(n_side, c["seed"])
+    res = {}
+    for form in ("fp64", "fp32"):
+        dpm = DifferentiablePM(L, n_side, N, a0, c["steps"], form, ckpt_every=4)
+        target = dpm.final_delta(ic.white_noise(n_side, 4))
+        for _ in range(max(1, args.warmup)):
+            dpm.loss_and_grad(noise, target)
+        t0 = time.perf_counter()
+        internal = []
+        for _ in range(args.steps):
+            dpm.loss_and_grad(noise, target)
+            internal.append(dpm.last_timings)
+        grad_s = (time.perf_counter() - t0) / args.steps
+        # the production forward of the same model on a PM handle
+        K1, D, K2 = hb.TimeStepper(a0, 1.0, dl).factors()
+        m = ic.particle_mass(L, n_side)
+        mesh = np.empty(N ** 3)
+        with hb.PMSolver(hb.MeshGeometry(L, N), hb.PMForceMethod.pure_pm(False), form) as s:
+            for _ in range(max(1, args.warmup)):
+                ic.lpt_on_device(s, noise, n_side, a0, m)
+                s.run(K1, D, K2)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                ic.lpt_on_device(s, noise, n_side, a0, m)
+                s.run(K1, D, K2)
+                nat_rc = hb.lib().hyowon_pm_download_mass_mesh(s.handle, mesh.ctypes.data_as(
+                    __import__("ctypes").POINTER(__import__("ctypes").c_double)))
+                if nat_rc:
+                    raise RuntimeError("mass mesh download failed")
+            fwd_s = (time.perf_counter() - t0) / args.steps
+        fi = float(np.median([t["forward_ms"] for t in internal]))
+        ri = float(np.median([t["reverse_ms"] for t in internal]))
+        res[form] = {"gradient_ms": 1e3 * grad_s, "production_forward_ms": 1e3 * fwd_s,
+                     "cost_ratio_vs_production_forward": grad_s / fwd_s,
+                     "adjoint_module_forward_ms": fi, "adjoint_module_reverse_ms": ri,
+                     "cost_ratio_vs_own_forward": (fi + ri) / fi}
+    n = n_side ** 3
+    line = {
+        "metric": "(forward + adjoint) / forward cost", "value": res["fp64"]["cost_ratio_vs_production_forward"],
+        "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["fp64"]["gradient_ms"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"c4 differentiable PM: {n_side}^3 particles, {N}^3 mesh, "
+                               f"L = {L}, 1LPT at z = {c['z_start']}, {c['steps']} KDK steps, "
+                               f"checkpoints every 4", "seed": c["seed"], "target_seed": 4,
+                   "timing": "wall clock around the synchronous calls (inputs and outputs "
+                             "in host memory on both sides)"},
+        "forms": res,
+        "gradient_particle_steps_per_s": n * c["steps"] / (res["fp64"]["gradient_ms"] * 1e-3),
+        "e2e": {"value": res["fp64"]["cost_ratio_vs_production_forward"], "unit": "x",
+                "h2d_bytes_per_step": 8 * (n + N ** 3), "d2h_bytes_per_step": 8 * n},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_treepm(args, rank):
+    """TreePM KDK steps on c5 (see the module docstring)."""
+    if rank != 0:
+        return
+    import hyowon_b200 as hb
+    from hyowon_b200 import ic
+    n_side, L, N, seed = 256, 256.0, 256, 5
+    a0 = 1.0 / 50.0
+    K1, D, K2 = hb.TimeStepper(a0, 1.0, math.log(1.0 / a0) / 64).factors()
+    m = ic.particle_mass(L, n_side)
+    with hb.PMSolver(hb.MeshGeometry(L, N), hb.PMForceMethod.pure_pm(False)) as s:
+        ic.lpt_on_device(s, ic.white_noise(n_side, seed), n_side, a0, m)
+        s.run(K1, D, K2)
+        st = s.download(acc=False)
+    r_s = 1.25 * L / N
+    eps = (L / n_side) / 30.0
+    n = n_side ** 3
+    # late steps of a continued run: K1/D/K2 of a step of the same size at a = 1
+    dl = math.log(1.0 / a0) / 64
+    sched = hb.TimeStepper(1.0 / math.exp(dl * (args.warmup + args.steps)), 1.0, dl).factors()
+    res = {}
+    for form in ("fp64", "fp32"):
+        with hb.PMSolver(hb.MeshGeometry(L, N), hb.PMForceMethod.treepm_long_range(r_s), form) as s:
+            s.upload(st["x"], st["y"], st["z"], st["px"], st["py"], st["pz"], uniform_mass=m)
+            sx, sy, sz, info = s.treepm_short_forces(0.5, eps, 4.5 * r_s)
+            s.set_treepm_short_range(0.5, eps, 4.5 * r_s)
+            s.solve_forces()
+            W = args.warmup
+            s.run(sched[0][:W], sched[1][:W], sched[2][:W])
+            s.set_timing(True)
+            with ClockSampler() as clk:
+                t0 = time.perf_counter()
+                s.run(sched[0][W:W + args.steps], sched[1][W:W + args.steps],
+                      sched[2][W:W + args.steps])
+                wall = time.perf_counter() - t0
+            tm = s.last_timing()
+            res[form] = {"ms_per_step": tm["total"] / args.steps, "wall_ms_per_step": 1e3 * wall / args.steps,
+                         "short_range_build_ms": info["build_ms"], "short_range_walk_ms": info["walk_ms"],
+                         "tree_nodes": info["nodes"], "visits_per_target": info["visits_per_target"],
+                         "interactions_per_target": info["interactions_per_target"],
+                         "clocks": clk.summary()}
+    v = n / (res["fp64"]["ms_per_step"] * 1e-3)
+    line = {
+        "metric": "particle-steps/s", "value": v, "unit": "particle-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["fp64"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"c5 TreePM KDK: {n_side}^3 particles, {N}^3 mesh, L = {L}, "
+                               f"r_s = 1.25 cells, r_cut = 4.5 r_s, theta = 0.5, eps = L/{n_side}/30, "
+                               "clustered z = 0 state of a 64-step PM run", "seed": seed,
+                   "l2": "particle arrays and meshes >> 126 MB"},
+        "forms": res,
+        "other_form": {"form": "fp32", "value": n / (res["fp32"]["ms_per_step"] * 1e-3)},
+        "e2e": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = setup_dist()
     if args.workload == "ic":
         run_ic(args, rank)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args, rank)
+        return
+    if args.workload == "treepm":
+        run_treepm(args, rank)
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -108,10 +108,17 @@ _SIGS = {
     "hyowon_vjp_1lpt_pm": (c_int, [c_void_p, P_double, P_double, P_double, P_double,
                                    P_double, P_double]),
     "hyowon_vjp_last_error": (ctypes.c_char_p, []),
+    "hyowon_pm_vjp": (c_int, [c_void_p, c_void_p, P_double, P_double, P_double, P_double,
+                              P_double, P_double]),
     "hyowon_treepm_short_forces": (c_int, [c_void_p, c_u64, P_double, P_double, P_double, c_u64,
                                            ctypes.POINTER(ctypes.c_uint32), P_double, P_double,
                                            P_double, P_double]),
     "hyowon_treepm_last_error": (ctypes.c_char_p, []),
+    "hyowon_pm_set_treepm_short_range": (c_int, [c_void_p, c_double, c_double, c_double]),
+    "hyowon_pm_debug_set_wait_limit": (c_int, [c_void_p, ctypes.c_uint]),
+    "hyowon_pm_debug_offset_mass_target": (c_int, [c_void_p, c_double]),
+    "hyowon_pm_treepm_short_forces": (c_int, [c_void_p, c_double, c_double, c_double]
+                                      + [P_double] * 4),
     "hyowon_cic_deposit_noalloc": (c_int, [c_double, c_u64, c_u64, c_void_p, c_void_p,
                                            c_void_p, c_void_p, c_double, c_void_p, c_void_p]),
     "hyowon_noalloc_last_error": (ctypes.c_char_p, []),

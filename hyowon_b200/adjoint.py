@@ -27,7 +27,11 @@ class DifferentiablePM:
     """noise -> 1LPT -> KDK steps -> CIC density; loss and d loss / d noise."""
 
     def __init__(self, box, n_side, mesh, a_start, n_steps, precision="fp64", ckpt_every=4,
-                 model: CosmologyModel = None):
+                 model: CosmologyModel = None, solver=None):
+        """With `solver` (a pure-PM PMSolver of this box, mesh and form) the
+        VJP runs on that handle (hyowon_pm_vjp), which keeps the adjoint's
+        plans and work arrays between calls."""
+        self.solver = solver
         model = model or CosmologyModel()
         self.box, self.n_side, self.mesh = float(box), int(n_side), int(mesh)
         self.precision = {"fp64": 0, "fp32": 1}[precision]
@@ -57,12 +61,18 @@ class DifferentiablePM:
         delta = np.empty(self.mesh ** 3) if want_delta else None
         t = np.zeros(4)
         cfg = self._cfg()
-        rc = nat.lib().hyowon_vjp_1lpt_pm(ctypes.byref(cfg), nat.dptr(noise), nat.dptr(target),
-                                          ctypes.byref(loss), nat.dptr(grad), nat.dptr(delta),
-                                          nat.dptr(t))
-        if rc != nat.OK:
-            msg = nat.lib().hyowon_vjp_last_error().decode(errors="replace")
-            raise nat._EXC.get(rc, RuntimeError)(f"hyowon_vjp_1lpt_pm: {msg}")
+        if self.solver is not None:
+            rc = nat.lib().hyowon_pm_vjp(self.solver.handle, ctypes.byref(cfg), nat.dptr(noise),
+                                         nat.dptr(target), ctypes.byref(loss), nat.dptr(grad),
+                                         nat.dptr(delta), nat.dptr(t))
+            nat.raise_for(rc, self.solver.handle, "hyowon_pm_vjp")
+        else:
+            rc = nat.lib().hyowon_vjp_1lpt_pm(ctypes.byref(cfg), nat.dptr(noise), nat.dptr(target),
+                                              ctypes.byref(loss), nat.dptr(grad), nat.dptr(delta),
+                                              nat.dptr(t))
+            if rc != nat.OK:
+                msg = nat.lib().hyowon_vjp_last_error().decode(errors="replace")
+                raise nat._EXC.get(rc, RuntimeError)(f"hyowon_vjp_1lpt_pm: {msg}")
         self.last_timings = {"forward_ms": t[0], "reverse_ms": t[1], "force_solves": t[2],
                              "force_vjps": t[3]}
         return loss.value, grad, delta

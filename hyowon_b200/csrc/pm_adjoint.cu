@@ -29,6 +29,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -36,6 +37,8 @@
 #include "hyowon_pm.h"
 #include "pm_common.cuh"
 #include "pm_lpt.h"
+#include "pm_adjoint.h"
+#include "pm_poisson.h"
 
 namespace hyowon::adj {
 
@@ -484,23 +487,48 @@ public:
         }
         lap_ = dmalloc<R>(N_, owned_);
         ACK(cudaMemcpy(lap_, lap.data(), sizeof(R) * N_, cudaMemcpyHostToDevice));
-        AFFT(cufftCreate(&r2c_));
-        AFFT(cufftCreate(&c2r_));
-        plans_ = true;
-        cufftSetAutoAllocation(r2c_, 0);
-        cufftSetAutoAllocation(c2r_, 0);
-        size_t w1 = 0, w2 = 0;
-        AFFT(cufftMakePlan3d(r2c_, N_, N_, N_, FFTTypes<R>::R2C, &w1));
-        AFFT(cufftMakePlan3d(c2r_, N_, N_, N_, FFTTypes<R>::C2R, &w2));
-        void* ws = dmalloc<char>(w1 > w2 ? w1 : w2, owned_);
-        cufftSetWorkArea(r2c_, ws);
-        cufftSetWorkArea(c2r_, ws);
-        cufftSetStream(r2c_, s_);
-        cufftSetStream(c2r_, s_);
+        four_pi_G_ = 4.0 * pi * G;
+        scale_ = 1.0 / (dx * dx * dx) / static_cast<double>(cells_);
+        five_ = poisson::supported(N_);
+        if (five_) {
+            // the production five-pass solve: own transforms with the Green's
+            // multiply fused into the x pass (chunked half spectrum)
+            const size_t elems = sizeof(R) == 8 ? poisson::modes_elements_f64(N_)
+                                                : poisson::modes_elements_f32(N_);
+            modes_ = dmalloc<C>(elems, owned_);
+            const char* perr = nullptr;
+            plan_ = poisson::create_plan(N_, sizeof(R) == 4, modes_, &perr);
+            if (!plan_) throw Fail{HYOWON_ECUDA, perr ? perr : "five-pass plan"};
+            std::vector<double> t(2 * static_cast<size_t>(N_));
+            poisson::twiddles(N_, t.data());
+            std::vector<C> tc(N_);
+            for (int i = 0; i < N_; ++i) {
+                tc[i].x = static_cast<R>(t[2 * i]);
+                tc[i].y = static_cast<R>(t[2 * i + 1]);
+            }
+            tw_ = dmalloc<C>(N_, owned_);
+            ACK(cudaMemcpy(tw_, tc.data(), sizeof(C) * N_, cudaMemcpyHostToDevice));
+            c_green_dev_ = dmalloc<R>(1, owned_);
+            ACK(cudaMemcpy(c_green_dev_, &c_green_, sizeof(R), cudaMemcpyHostToDevice));
+        } else {
+            AFFT(cufftCreate(&r2c_));
+            AFFT(cufftCreate(&c2r_));
+            plans_ = true;
+            cufftSetAutoAllocation(r2c_, 0);
+            cufftSetAutoAllocation(c2r_, 0);
+            size_t w1 = 0, w2 = 0;
+            AFFT(cufftMakePlan3d(r2c_, N_, N_, N_, FFTTypes<R>::R2C, &w1));
+            AFFT(cufftMakePlan3d(c2r_, N_, N_, N_, FFTTypes<R>::C2R, &w2));
+            void* ws = dmalloc<char>(w1 > w2 ? w1 : w2, owned_);
+            cufftSetWorkArea(r2c_, ws);
+            cufftSetWorkArea(c2r_, ws);
+            cufftSetStream(r2c_, s_);
+            cufftSetStream(c2r_, s_);
+            modes_ = dmalloc<C>(half_, owned_);
+        }
         mesh_ = dmalloc<R>(cells_, owned_);
         phi_own_ = dmalloc<R>(cells_, owned_);
         phi_ = phi_own_;
-        modes_ = dmalloc<C>(half_, owned_);
         status_ = dmalloc<unsigned int>(1, owned_);
         ACK(cudaMemsetAsync(status_, 0, sizeof(unsigned int), s_));
         for (int a = 0; a < 3; ++a) {
@@ -510,7 +538,17 @@ public:
         }
     }
 
+    // A later call with the same geometry (box, mesh, lattice, form) reuses the
+    // engine: its plans and work arrays; the rest of the configuration (P(k)
+    // table, schedule, masses, checkpoints) is the call's own.
+    bool same_geometry(const VjpConfig& c) const {
+        return c.box_size == cfg_.box_size && c.mesh_size == cfg_.mesh_size
+            && c.n_side == cfg_.n_side && c.precision == cfg_.precision;
+    }
+    void set_config(const VjpConfig& c) { cfg_ = c; }
+
     ~Engine() {
+        poisson::destroy_plan(plan_);
         if (plans_) {
             cufftDestroy(r2c_);
             cufftDestroy(c2r_);
@@ -538,7 +576,29 @@ public:
                                           acc_[1], acc_[2]);
     }
 
+    // out = A in: r2c, Green's function (k = 0 zeroed), c2r with 1/N^3. On
+    // power-of-two meshes the production five-pass solve (Green's multiply
+    // inside the x pass; A is self-adjoint, so the adjoint uses it as is);
+    // elsewhere cuFFT with a separate multiply.
     void apply_green(R* in, R* out) {
+        if (five_) {
+            int k = 0;
+            if constexpr (sizeof(R) == 8) {
+                // no mass check here: the source is a mass mesh or a divergence
+                const poisson::GreenF64 g{lap_, nullptr, four_pi_G_, scale_, 0, 0.0, INFINITY,
+                                          status_};
+                k = poisson::forward_f64(plan_, N_, in, modes_, tw_, status_, s_) < 0
+                        || poisson::green_f64(plan_, N_, modes_, tw_, g, s_) < 0
+                        || poisson::inverse_f64(plan_, N_, modes_, out, tw_, status_, s_) < 0;
+            } else {
+                const poisson::GreenF32 g{lap_, nullptr, 0, c_green_dev_};
+                k = poisson::forward_f32(plan_, N_, in, modes_, tw_, status_, s_) < 0
+                        || poisson::green_f32(plan_, N_, modes_, tw_, g, status_, s_) < 0
+                        || poisson::inverse_f32(plan_, N_, modes_, out, tw_, status_, s_) < 0;
+            }
+            if (k) throw Fail{HYOWON_ECUDA, "potential solve launch failed"};
+            return;
+        }
         AFFT(FFTTypes<R>::fwd(r2c_, in, modes_));
         k_green<R, C><<<nb(half_), kT, 0, s_>>>(N_, modes_, lap_, c_green_);
         AFFT(FFTTypes<R>::inv(c2r_, modes_, out));
@@ -750,6 +810,11 @@ private:
     R inv_two_dx_ = 0, c_green_ = 0;
     R* lap_ = nullptr;
     cufftHandle r2c_ = 0, c2r_ = 0;
+    bool five_ = false;               // power-of-two mesh: five-pass solve
+    poisson::Plan* plan_ = nullptr;
+    C* tw_ = nullptr;
+    R* c_green_dev_ = nullptr;
+    double four_pi_G_ = 0.0, scale_ = 0.0;
     bool plans_ = false;
     R* mesh_ = nullptr;
     R* phi_own_ = nullptr;
@@ -766,6 +831,51 @@ private:
 thread_local std::string g_adj_err;
 
 }  // namespace
+
+// Engines kept by a PM handle between its VJP calls.
+struct Cache {
+    Engine<double>* e64 = nullptr;
+    Engine<float>* e32 = nullptr;
+    ~Cache() {
+        delete e64;
+        delete e32;
+    }
+};
+
+void destroy_cache(Cache* c) { delete c; }
+
+int run_cached(Cache** cache, const VjpConfig& cfg, cudaStream_t s, const double* noise,
+               const double* target_delta, double* loss, double* grad_noise,
+               double* final_delta, double* timings, std::string* err) {
+    try {
+        if (!*cache) *cache = new Cache();
+        Cache* c = *cache;
+        if (cfg.precision == HYOWON_FP64) {
+            if (c->e64 && !c->e64->same_geometry(cfg)) {
+                delete c->e64;
+                c->e64 = nullptr;
+            }
+            if (!c->e64) c->e64 = new Engine<double>(cfg, s);
+            c->e64->set_config(cfg);
+            c->e64->run(noise, target_delta, loss, grad_noise, final_delta, timings);
+        } else {
+            if (c->e32 && !c->e32->same_geometry(cfg)) {
+                delete c->e32;
+                c->e32 = nullptr;
+            }
+            if (!c->e32) c->e32 = new Engine<float>(cfg, s);
+            c->e32->set_config(cfg);
+            c->e32->run(noise, target_delta, loss, grad_noise, final_delta, timings);
+        }
+    } catch (const Fail& f) {
+        if (err) *err = f.msg;
+        return f.code;
+    } catch (const std::bad_alloc&) {
+        if (err) *err = "out of host memory";
+        return HYOWON_ENOMEM;
+    }
+    return HYOWON_OK;
+}
 
 }  // namespace hyowon::adj
 

@@ -422,9 +422,11 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
     if (qsum) block_sum_to(local, qsum);
 }
 
+// `expect_offset` is 0 except in tests of the failure path, which move the
+// expected sum off the exact one.
 __global__ void k_check_mass(const unsigned long long* qsum, const FixedPlan* plan,
-                             unsigned int* status) {
-    if (threadIdx.x == 0 && *qsum != plan->residual) raise_status(status, ST_MASS);
+                             unsigned long long expect_offset, unsigned int* status) {
+    if (threadIdx.x == 0 && *qsum != plan->residual + expect_offset) raise_status(status, ST_MASS);
 }
 
 __global__ void k_green(int N, float2* __restrict__ modes, const float* __restrict__ lap,
@@ -692,6 +694,11 @@ struct State {
     int step_P = 0, step_M = 0;  // position / momentum sets of the step in flight
     bool step_sorted = false;
     uint64_t launches = 0;  // kernels launched (cuFFT's excluded)
+    // TreePM short range: called between the long-range accumulation and the
+    // K2 kick with the position set of the solve (null: long range alone).
+    ShortRangeHook short_range = nullptr;
+    void* short_ctx = nullptr;
+    unsigned long long mass_check_offset = 0;  // tests of the mass-check failure path
     std::string err;
 };
 
@@ -1042,7 +1049,7 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
     int rc = deposit_tiles<float>(st, P, order, st->rmesh, st->d_qsum, d_status, s);
     if (rc) return rc;
     ++st->launches;
-    k_check_mass<<<1, 32, 0, s>>>(st->d_qsum, st->d_plan, d_status);
+    k_check_mass<<<1, 32, 0, s>>>(st->d_qsum, st->d_plan, st->mass_check_offset, d_status);
     float* const pxo = st->mom[1 - M][0];
     float* const pyo = st->mom[1 - M][1];
     float* const pzo = st->mom[1 - M][2];
@@ -1118,6 +1125,10 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
         k_interp_add<<<blocks_for(n), kThreads, 0, s>>>(n, st->rmesh, st->pos[P][0],
                                                         st->pos[P][1], st->pos[P][2], N,
                                                         st->acc[a], d_status);
+    }
+    if (st->short_range) {
+        const int rc = st->short_range(st->short_ctx, s, P);
+        if (rc) return rc;
     }
     rec(ev, 5, s);
     if (kick) {
@@ -1279,15 +1290,49 @@ __global__ void k_widen_positions(uint32_t n, const uint32_t* __restrict__ u, do
 }
 
 int positions_f64(State* st, cudaStream_t s, double* x, double* y, double* z) {
+    return positions_f64_of_set(st, s, st->pc, x, y, z);
+}
+
+int positions_f64_of_set(State* st, cudaStream_t s, int P, double* x, double* y, double* z) {
     double* outs[3] = {x, y, z};
     for (int a = 0; a < 3; ++a) {
         ++st->launches;
-        k_widen_positions<<<blocks_for(st->n), kThreads, 0, s>>>(st->n, st->pos[st->pc][a],
+        k_widen_positions<<<blocks_for(st->n), kThreads, 0, s>>>(st->n, st->pos[P][a],
                                                                  st->L / kTwo32, outs[a]);
     }
     CK(cudaPeekAtLastError());
     return HYOWON_OK;
 }
+
+__global__ void k_add_acc(uint32_t n, const double* __restrict__ ax, const double* __restrict__ ay,
+                          const double* __restrict__ az, float* __restrict__ gx,
+                          float* __restrict__ gy, float* __restrict__ gz) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    gx[i] += static_cast<float>(ax[i]);
+    gy[i] += static_cast<float>(ay[i]);
+    gz[i] += static_cast<float>(az[i]);
+}
+
+int add_accelerations(State* st, cudaStream_t s, const double* ax, const double* ay,
+                      const double* az) {
+    ++st->launches;
+    k_add_acc<<<blocks_for(st->n), kThreads, 0, s>>>(st->n, ax, ay, az, st->acc[0], st->acc[1],
+                                                     st->acc[2]);
+    CK(cudaPeekAtLastError());
+    return HYOWON_OK;
+}
+
+void set_mass_check_offset(State* st, unsigned long long units) { st->mass_check_offset = units; }
+
+void set_wait_limit(State* st, unsigned polls) { poisson::set_wait_limit(st->fft_plan, polls); }
+
+void set_short_range_hook(State* st, ShortRangeHook fn, void* ctx) {
+    st->short_range = fn;
+    st->short_ctx = ctx;
+}
+
+const uint32_t* current_ids(State* st) { return st->id[st->ic]; }
 
 int diagnostics(State* st, cudaStream_t s, bool with_potential, double* scratch, double* sums) {
     diag::InputsF32 in{};

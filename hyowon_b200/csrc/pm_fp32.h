@@ -26,6 +26,9 @@ namespace fp32 {
 
 struct State;
 
+// TreePM short-range hook (see set_short_range_hook).
+using ShortRangeHook = int (*)(void* ctx, cudaStream_t s, int position_set);
+
 int create(State** out, double L, int N, int method, int deconvolve, double r_s,
            const double* lap, const double* win, double four_pi_G, cudaStream_t s);
 void destroy(State* st);
@@ -59,6 +62,23 @@ int diagnostics(State* st, cudaStream_t s, bool with_potential, double* scratch,
 // the particle count, in the current storage order.
 int positions_f64(State* st, cudaStream_t s, double* x, double* y, double* z);
 int download_mass_mesh(State* st, cudaStream_t s, unsigned int* d_status, double* mesh);
+// Positions of set P (0/1) widened to binary64.
+int positions_f64_of_set(State* st, cudaStream_t s, int P, double* x, double* y, double* z);
+// acc[i] += (float) a[i] for the accelerations of the solve in flight.
+int add_accelerations(State* st, cudaStream_t s, const double* ax, const double* ay,
+                      const double* az);
+// TreePM long-range solves call fn(ctx, s, P) after the three long-range
+// gathers and before the K2 kick, P the position set of the solve; fn adds the
+// short-range accelerations (add_accelerations). A non-zero return aborts the
+// solve with that status. fn null: long range alone.
+void set_short_range_hook(State* st, ShortRangeHook fn, void* ctx);
+// Failure-path tests: the expected fixed-point mesh sum is moved by `units`
+// (0 restores the exact check), and the column passes' pipeline waits give up
+// after `polls` polls.
+void set_mass_check_offset(State* st, unsigned long long units);
+void set_wait_limit(State* st, unsigned polls);
+// slot -> particle index of the current storage order.
+const uint32_t* current_ids(State* st);
 // The device state as snapshot components (positions as u32 fixed point,
 // momenta FP32), the slot -> particle index, and the staging area available
 // between force solves (the half-spectrum buffer, *stage_doubles doubles).

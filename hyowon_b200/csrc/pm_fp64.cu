@@ -3,10 +3,14 @@
 //
 // Compiled with --fmad=false: every product and sum below rounds exactly as
 // the reference's -ffp-contract=off build does, in the reference's operation
-// order (cited per kernel). Summation across particles (the deposit) uses
-// atomics and therefore differs from the reference's plane-ordered sum only in
-// rounding.
+// order (cited per kernel). Summation across particles (the deposit) is exact
+// fixed-point integer arithmetic rounded once per cell (k_deposit_tiles), so the
+// mesh is the same bits run to run whatever order the atomics land in, as the
+// reference's plane-ordered sum is; the two differ by the rounding of the
+// reference's sequential binary64 sum.
 #include <cuda_runtime.h>
+
+#include <cmath>
 
 #include "pm_kernels.h"
 
@@ -173,6 +177,168 @@ __global__ void k_deposit(uint32_t n, const double* __restrict__ x,
             }
         }
     }
+}
+
+// Deterministic binary64 deposit (CICMassAssignment::deposit,
+// src/mesh/mass_assignment_deposit.inc:193-240, whose plane-owned sum is
+// deterministic whatever the thread count, :302-333).
+//
+// Owner-computes tiles: one block per tile of TY mesh rows (x0, y0 .. y0+TY-1,
+// all z). Each particle term t = m*wx*wy*wz (the reference's product order, in
+// binary64) is converted exactly in scale to fixed point, q = rint(t 2^(62-e))
+// with m_max < 2^e, so q <= 2^62; q is split at bit W into hi = q >> W and
+// lo = q mod 2^W, and both halves are summed by integer atomics into two
+// shared-memory arrays. W = 63 - floor(log2(8 max_bucket)) keeps every lo sum
+// below 2^64 (a cell's contributors lie in 8 buckets), so no carry is lost and
+// the cell holds the exact integer sum hi_sum 2^W + lo_sum of its quantised
+// terms, independent of atomic order. Each cell is written once, that sum
+// correctly rounded to binary64 and scaled by 2^(e-62) (exact). Quantisation:
+// at most 2^(e-63) per term, below the rounding of one binary64 add of a
+// typical cell.
+//
+// Contributors are the particles whose base cell lies in plane x0 (weight
+// 1 - fx) or x0-1 (weight fx) and rows y0-1 .. y0+TY-1: at most four contiguous
+// ranges of the cell-ordered particles, found through the bucket starts
+// `offset` (`order`: cell-order slot -> particle slot, or null when the arrays
+// are in cell order). A bucket can straddle a range edge, so each particle is
+// kept only in the range of its own plane and row; the ranges are disjoint in
+// (plane, row), so every contributor counts once.
+constexpr int kTileThreads = 256;
+#ifndef HYOWON_DEPOSIT64_TILE_CELLS
+#define HYOWON_DEPOSIT64_TILE_CELLS 2048
+#endif
+
+__device__ __forceinline__ int fixed_split_bits(const uint32_t* max_count) {
+    const unsigned long long c = 8ull * (*max_count > 0u ? *max_count : 1u);
+    return 63 - (63 - __clzll(c));   // 63 - floor(log2 c)
+}
+
+// hi 2^W + lo as a 128-bit integer, correctly rounded to binary64 (the bits
+// below the leading 64 fold into a sticky bit).
+__device__ __forceinline__ double fixed_to_double(unsigned long long hi, unsigned long long lo,
+                                                  int W) {
+    unsigned long long low = hi << W;
+    unsigned long long high = hi >> (64 - W);
+    low += lo;
+    high += low < lo ? 1ull : 0ull;
+    if (high == 0ull) return __ull2double_rn(low);
+    const int lz = __clzll(high);
+    unsigned long long top = lz ? (high << lz) | (low >> (64 - lz)) : high;
+    const unsigned long long rest = lz ? (low << lz) : low;
+    top |= rest != 0ull ? 1ull : 0ull;
+    return ldexp(__ull2double_rn(top), 64 - lz);
+}
+
+__global__ void __launch_bounds__(kTileThreads)
+k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
+                const double* __restrict__ z, const double* __restrict__ mass,
+                double uniform_mass, const uint32_t* __restrict__ order,
+                const uint32_t* __restrict__ offset, int shift, Axis a, int TY,
+                const uint32_t* __restrict__ max_count, int e_max, double* __restrict__ mesh,
+                const unsigned int* status) {
+    extern __shared__ __align__(16) unsigned long long acc[];
+    __shared__ uint32_t seg_p0[4], seg_len[4];
+    __shared__ int seg_plane[4], seg_row_lo[4], seg_row_hi[4], seg_own[4];
+    __shared__ int seg_n;
+    if (*status & ST_BLOCKS_PUBLISH) return;
+    const int N = a.N;
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.y;
+    const int y0 = blockIdx.x * TY;
+    const int ty = N - y0 < TY ? N - y0 : TY;
+    const int halo = ty == N ? 0 : 1;
+    const int tcells = ty * N;
+    unsigned long long* acc_lo = acc;
+    unsigned long long* acc_hi = acc + static_cast<size_t>(TY) * N;
+    if (tid == 0) {
+        int ns = 0;
+        for (int own = 1; own >= 0; --own) {
+            const int p = own ? x0 : (x0 == 0 ? N - 1 : x0 - 1);
+            int lo[2], hi[2], nr = 0;
+            if (halo && y0 == 0) {
+                lo[nr] = N - 1; hi[nr++] = N - 1;
+                lo[nr] = 0; hi[nr++] = ty - 1;
+            } else {
+                lo[nr] = y0 - halo; hi[nr++] = y0 + ty - 1;
+            }
+            for (int k = 0; k < nr; ++k) {
+                const uint64_t c_lo = (static_cast<uint64_t>(p) * N + lo[k]) * N;
+                const uint64_t c_hi = (static_cast<uint64_t>(p) * N + hi[k]) * N + (N - 1);
+                const uint32_t b0 = offset[c_lo >> shift];
+                const uint32_t b1 = offset[(c_hi >> shift) + 1];
+                seg_p0[ns] = b0;
+                seg_len[ns] = b1 - b0;
+                seg_plane[ns] = p;
+                seg_row_lo[ns] = lo[k];
+                seg_row_hi[ns] = hi[k];
+                seg_own[ns] = own;
+                ++ns;
+            }
+        }
+        seg_n = ns;
+    }
+    for (int e = tid; e < tcells; e += kTileThreads) {
+        acc_lo[e] = 0ull;
+        acc_hi[e] = 0ull;
+    }
+    __syncthreads();
+    const int W = fixed_split_bits(max_count);
+    const unsigned long long lo_mask = (1ull << W) - 1ull;
+    const int to_fixed = 62 - e_max;
+    const int ns = seg_n;
+    for (int g = 0; g < ns; ++g) {
+        const uint32_t p0 = seg_p0[g];
+        const uint32_t len = seg_len[g];
+        const int plane = seg_plane[g];
+        const int row_lo = seg_row_lo[g], row_hi = seg_row_hi[g];
+        const bool own = seg_own[g] != 0;
+        for (uint32_t v = tid; v < len; v += kTileThreads) {
+            const uint32_t i = order ? order[p0 + v] : p0 + v;
+            int ix, iy, iz;
+            double tx, ty_, tz;
+            if (!(cic_coord_f64(x[i], a, ix, tx) & cic_coord_f64(y[i], a, iy, ty_)
+                  & cic_coord_f64(z[i], a, iz, tz)))
+                continue;   // never in cell order: the key pass raised the status
+            if (ix != plane || iy < row_lo || iy > row_hi) continue;
+            const double m = mass ? mass[i] : uniform_mass;
+            const double mx = m * (own ? 1.0 - tx : tx);
+            const double wy[2] = {1.0 - ty_, ty_};
+            const double wz[2] = {1.0 - tz, tz};
+            const int gz[2] = {iz, iz + 1 == N ? 0 : iz + 1};
+#pragma unroll
+            for (int oy = 0; oy < 2; ++oy) {
+                const int row = iy + oy == N ? 0 : iy + oy;
+                const int ly = row - y0;
+                if (ly < 0 || ly >= ty) continue;
+                const double mxy = mx * wy[oy];
+                unsigned long long* rlo = acc_lo + ly * N;
+                unsigned long long* rhi = acc_hi + ly * N;
+#pragma unroll
+                for (int oz = 0; oz < 2; ++oz) {
+                    const unsigned long long q =
+                        static_cast<unsigned long long>(llrint(ldexp(mxy * wz[oz], to_fixed)));
+                    if (q == 0ull) continue;
+                    atomicAdd(rlo + gz[oz], q & lo_mask);
+                    const unsigned long long qh = q >> W;
+                    if (qh) atomicAdd(rhi + gz[oz], qh);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    double* out = mesh + (static_cast<uint64_t>(x0) * N + y0) * N;
+    const int from_fixed = e_max - 62;
+    for (int e = tid; e < tcells; e += kTileThreads)
+        out[e] = ldexp(fixed_to_double(acc_hi[e], acc_lo[e], W), from_fixed);
+}
+
+__global__ void k_max_count64(uint32_t nb, const uint32_t* __restrict__ count,
+                              uint32_t* max_count) {
+    uint32_t m = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+        m = max(m, count[i]);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(max_count, m);
 }
 
 // Pure-PM Green's function (src/mesh/green_function.cpp:165-207) applied to the
@@ -588,6 +754,42 @@ void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,
     if (n == 0) return;
     k_deposit<<<blocks_for(n), kThreads, 0, s>>>(n, p.x, p.y, p.z, mass, uniform_mass, a,
                                                  mesh, status);
+}
+
+int deposit_tile_rows_f64(int N) {
+    int ty = HYOWON_DEPOSIT64_TILE_CELLS / N;
+    if (ty < 1) ty = 1;
+    return ty > N ? N : ty;
+}
+
+int deposit_mass_exponent_f64(double max_mass) {
+    int e = 0;
+    if (max_mass > 0.0) std::frexp(max_mass, &e);   // max_mass < 2^e
+    return e;
+}
+
+cudaError_t launch_deposit_tiles_f64(const ParticlesF64& p, const double* mass,
+                                     double uniform_mass, const uint32_t* order,
+                                     const SortWork& w, Axis a, const uint32_t* max_count,
+                                     int e_max, double* mesh, const unsigned int* status,
+                                     cudaStream_t s) {
+    const int N = a.N;
+    const int TY = deposit_tile_rows_f64(N);
+    const size_t smem = 16 * static_cast<size_t>(TY) * N;
+    cudaError_t e = cudaFuncSetAttribute(k_deposit_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const dim3 grid(static_cast<unsigned>((N + TY - 1) / TY), static_cast<unsigned>(N));
+    k_deposit_tiles<<<grid, kTileThreads, smem, s>>>(p.x, p.y, p.z, mass, uniform_mass, order,
+                                                     w.offset, w.shift, a, TY, max_count, e_max,
+                                                     mesh, status);
+    return cudaPeekAtLastError();
+}
+
+void launch_max_count_f64(uint32_t n_buckets, const uint32_t* count, uint32_t* max_count,
+                          cudaStream_t s) {
+    k_max_count64<<<stream_blocks(n_buckets, kThreads), kThreads, 0, s>>>(n_buckets, count,
+                                                                          max_count);
 }
 
 

@@ -7,7 +7,9 @@
 //   2. exclusive scan of the bucket histogram;
 //   3. scatter P' -> P in bucket order (skipped on a device error: nothing is
 //      published, as LeapfrogIntegrator's preflight, leapfrog_integrator.cpp:170-190);
-//   4. deposit, D2Z, Green (+ density normalisation, 1/N^3, mass check), Z2D;
+//   4. deterministic fixed-point tile deposit (particles located through the
+//      bucket offsets and, between re-sorts, the cell-order index), D2Z,
+//      Green (+ density normalisation, 1/N^3, mass check), Z2D;
 //   5. gather_kick: A = -grad(phi) at P, p'' = p' + A*K2 into the spare
 //      momentum buffer, published by a pointer swap after the status check.
 #include <cuda_runtime.h>
@@ -31,6 +33,11 @@
 #include "pm_snapshot.h"
 #include "pm_lpt.h"
 #include "pm_pk.h"
+#include "pm_tree.h"
+#include "hyowon_treepm.h"
+#include "hyowon_debug.h"
+#include "hyowon_adjoint.h"
+#include "pm_adjoint.h"
 
 using namespace hyowon;
 
@@ -99,9 +106,16 @@ struct hyowon_pm_s {
     bool has_masses = false;
     double input_mass = 0.0;
     double mass_tol = 0.0;
+    double mass_target_offset = 0.0;  // failure-path tests (hyowon_debug.h)
 
     SortWork sort{};
     uint32_t sort_cap_buckets = 0;
+    uint32_t* order = nullptr;        // cell-order slot -> particle slot (n)
+    uint32_t* d_max_count = nullptr;  // largest bucket count of the last keying
+    double max_mass = 0.0;            // largest particle mass (fixed-point scale)
+    // What the bucket offsets describe for the current position set:
+    // 0 nothing, 1 the arrays themselves are in cell order, 2 `order` holds it.
+    int order_state = 0;
 
     unsigned int* d_status = nullptr;
     unsigned long long* d_maxdrift = nullptr;
@@ -110,6 +124,14 @@ struct hyowon_pm_s {
     unsigned long long* h_maxdrift = nullptr;   // pinned
 
     fp32::State* f32 = nullptr;  // precision form (pm_fp32.cu)
+
+    hyowon::adj::Cache* adj = nullptr;  // adjoint engines of hyowon_pm_vjp
+
+    // TreePM short range (hyowon_pm_set_treepm_short_range)
+    bool treepm_short = false;
+    hyowon_treepm_params tp{};
+    double* tree_buf = nullptr;       // 6 n doubles: widened positions, short-range output
+    uint32_t tree_cap = 0;
 
     bool timing = false;
     cudaEvent_t ev[8] = {};
@@ -204,8 +226,11 @@ void free_particles(hyowon_pm_t h) {
     }
     cudaFree(h->sort.key);
     cudaFree(h->sort.rank);
+    cudaFree(h->order);
     h->sort.key = h->sort.rank = nullptr;
+    h->order = nullptr;
     h->cap = 0;
+    h->order_state = 0;
 }
 
 int ensure_capacity(hyowon_pm_t h, uint32_t n, bool masses) {
@@ -222,6 +247,7 @@ int ensure_capacity(hyowon_pm_t h, uint32_t n, bool masses) {
     for (int a = 0; a < 3; ++a) CK(dalloc(&h->acc[a], n));
     CK(dalloc(&h->sort.key, n));
     CK(dalloc(&h->sort.rank, n));
+    CK(dalloc(&h->order, n));
     h->cap = n;
     return HYOWON_OK;
 }
@@ -263,6 +289,7 @@ void set_input_mass(hyowon_pm_t h, double total, uint32_t n) {
 void release_ic_workspace(hyowon_pm_t h) {
     if (h && h->ic_ws) {
         hyowon::ic::workspace_destroy(h->ic_ws);
+    hyowon::adj::destroy_cache(h->adj);
         h->ic_ws = nullptr;
     }
 }
@@ -283,6 +310,9 @@ int sort_current(hyowon_pm_t h) {
     launch_key_f64(n, set_view(h, h->pc, h->mc), h->axis, h->sort, h->d_status, h->stream);
     h->launches += launch_exclusive_scan(h->sort.count, h->sort.offset, h->sort.n_buckets + 1, h->sort.scan_tmp,
                           h->stream);
+    CK(cudaMemsetAsync(h->d_max_count, 0, sizeof(uint32_t), h->stream));
+    ++h->launches;
+    launch_max_count_f64(h->sort.n_buckets, h->sort.count, h->d_max_count, h->stream);
     const double* src[8];
     double* dst[8];
     int k = 0;
@@ -311,16 +341,45 @@ int sort_current(hyowon_pm_t h) {
     h->mc = 1 - h->mc;
     h->ic = 1 - h->ic;
     h->sorted = true;
+    h->order_state = 1;
     return HYOWON_OK;
 }
+
+// Cell order of the current position set through the order index (its
+// arrays stay where they are): keys, bucket offsets, order, largest bucket.
+int index_current(hyowon_pm_t h) {
+    const uint32_t n = h->n;
+    CK(cudaMemsetAsync(h->sort.count, 0, sizeof(uint32_t) * (h->sort.n_buckets + 1), h->stream));
+    ++h->launches;
+    launch_key_f64(n, set_view(h, h->pc, h->mc), h->axis, h->sort, h->d_status, h->stream);
+    h->launches += launch_exclusive_scan(h->sort.count, h->sort.offset, h->sort.n_buckets + 1,
+                                         h->sort.scan_tmp, h->stream);
+    ++h->launches;
+    launch_order(n, h->sort.key, h->sort.rank, h->sort.offset, h->order, h->d_status, h->stream);
+    CK(cudaMemsetAsync(h->d_max_count, 0, sizeof(uint32_t), h->stream));
+    ++h->launches;
+    launch_max_count_f64(h->sort.n_buckets, h->sort.count, h->d_max_count, h->stream);
+    unsigned int st = 0;
+    int rc = read_status(h, &st);
+    if (rc) return rc;
+    if (st) return status_to_code(h, st);
+    h->order_state = 2;
+    return HYOWON_OK;
+}
+
+// The order argument of the binary64 deposit for the current set.
+const uint32_t* current_order(hyowon_pm_t h) { return h->order_state == 2 ? h->order : nullptr; }
 
 void record(hyowon_pm_t h, int i) {
     if (h->timing) cudaEventRecord(h->ev[i], h->stream);
 }
 
+int add_short_range_f64(hyowon_pm_t h, int pset);
+
 // Deposit -> FFT -> Green -> inverse FFT -> gather (+ K2 into the spare momenta).
 // Leaves the status check to the caller.
-int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2) {
+int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2,
+                  const uint32_t* order) {
     const uint32_t n = h->n;
     const int N = h->N;
     const size_t cells = static_cast<size_t>(N) * N * N;
@@ -328,11 +387,13 @@ int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2) {
         return fp32::enqueue_force(h->f32, h->stream, h->d_status, kick, K2, h->timing ? h->ev : nullptr);
     }
     const ParticlesF64 p = set_view(h, pset, mset);
+    (void)cells;
     record(h, 1);
-    CK(cudaMemsetAsync(h->mesh, 0, sizeof(double) * cells, h->stream));
     ++h->launches;
-    launch_deposit_f64(n, p, h->has_masses ? h->mass[h->ic] : nullptr, h->uniform_mass, h->axis,
-                       h->mesh, h->d_status, h->stream);
+    CK(launch_deposit_tiles_f64(p, h->has_masses ? h->mass[h->ic] : nullptr, h->uniform_mass,
+                                order, h->sort, h->axis, h->d_max_count,
+                                deposit_mass_exponent_f64(h->max_mass), h->mesh, h->d_status,
+                                h->stream));
     record(h, 2);
     double* const pxo = h->mom[1 - mset][0];
     double* const pyo = h->mom[1 - mset][1];
@@ -343,7 +404,7 @@ int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2) {
         h->launches += k;
         record(h, 3);
         const poisson::GreenF64 g{h->lap, h->win, h->four_pi_G, h->field_scale, h->deconvolve,
-                                  h->input_mass, h->mass_tol, h->d_status};
+                                  h->input_mass + h->mass_target_offset, h->mass_tol, h->d_status};
         k = poisson::green_f64(h->fft_plan, N, h->modes, h->tw, g, h->stream);
         if (k < 0) return fail(h, HYOWON_ECUDA, "potential solve: Green pass launch failed");
         h->launches += k;
@@ -363,7 +424,8 @@ int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2) {
     if (h->method == HYOWON_PURE_PM) {
         ++h->launches;
         launch_green_f64(N, h->modes, h->lap, h->win, h->four_pi_G, h->field_scale, h->deconvolve,
-                         h->input_mass, h->mass_tol, h->d_status, h->stream);
+                         h->input_mass + h->mass_target_offset, h->mass_tol, h->d_status,
+                         h->stream);
         record(h, 4);
         CKFFT(cufftExecZ2D(h->plan_c2r, reinterpret_cast<cufftDoubleComplex*>(h->modes), h->mesh));
         record(h, 5);
@@ -377,7 +439,8 @@ int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2) {
     // plain CIC gather added to the zeroed acceleration.
     ++h->launches;
     launch_green_spectral_f64(N, h->L, h->modes, h->win, h->four_pi_G, h->field_scale, h->r_s,
-                              h->input_mass, h->mass_tol, h->d_status, h->stream);
+                              h->input_mass + h->mass_target_offset, h->mass_tol, h->d_status,
+                              h->stream);
     CK(cudaMemcpyAsync(h->phi_k, h->modes, sizeof(double2) * static_cast<size_t>(N) * N * (N / 2 + 1),
                        cudaMemcpyDeviceToDevice, h->stream));
     record(h, 4);
@@ -388,6 +451,10 @@ int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2) {
         CKFFT(cufftExecZ2D(h->plan_c2r, reinterpret_cast<cufftDoubleComplex*>(h->modes), h->mesh));
         ++h->launches;
         launch_interp_add_f64(n, h->mesh, p, h->axis, h->acc[a], h->d_status, h->stream);
+    }
+    if (h->treepm_short) {
+        int rc = add_short_range_f64(h, pset);
+        if (rc) return rc;
     }
     record(h, 5);
     if (kick) {
@@ -435,6 +502,57 @@ struct CallTimer {
     }
 };
 
+int ensure_tree_buffer(hyowon_pm_t h) {
+    if (h->tree_buf && h->tree_cap >= h->n) return HYOWON_OK;
+    cudaFree(h->tree_buf);
+    h->tree_buf = nullptr;
+    h->tree_cap = 0;
+    CK(dalloc(&h->tree_buf, 6 * static_cast<size_t>(h->n)));
+    h->tree_cap = h->n;
+    return HYOWON_OK;
+}
+
+// Short-range accelerations of position set pset added to the binary64
+// accelerations (the TreePM force method), unless an earlier kernel of the
+// step already failed.
+int add_short_range_f64(hyowon_pm_t h, int pset) {
+    unsigned int st = 0;
+    int rc = read_status(h, &st);
+    if (rc) return rc;
+    if (st) return HYOWON_OK;   // the status decides the outcome; K2 is gated on it
+    std::string err;
+    hyowon_treepm_params P = h->tp;
+    P.particle_mass = h->uniform_mass > 0.0 ? h->uniform_mass : 1.0;  // masses win when present
+    rc = tree::device_short_forces(P, h->n, h->pos[pset][0], h->pos[pset][1], h->pos[pset][2],
+                                   h->has_masses ? h->mass[h->ic] : nullptr, h->acc[0], h->acc[1],
+                                   h->acc[2], h->stream, nullptr, &err);
+    return rc ? fail(h, rc, "TreePM short range: " + err) : HYOWON_OK;
+}
+
+// The precision form's hook: widen set P, walk, add to its FP32 accelerations.
+int short_range_hook_f32(void* ctx, cudaStream_t s, int P) {
+    hyowon_pm_t h = static_cast<hyowon_pm_t>(ctx);
+    unsigned int st = 0;
+    int rc = read_status(h, &st);
+    if (rc) return rc;
+    if (st) return HYOWON_OK;
+    rc = ensure_tree_buffer(h);
+    if (rc) return rc;
+    const size_t n = h->n;
+    double* px = h->tree_buf;
+    double* out = h->tree_buf + 3 * n;
+    rc = fp32::positions_f64_of_set(h->f32, s, P, px, px + n, px + 2 * n);
+    if (rc) return status_or_cuda(h, rc);
+    CK(cudaMemsetAsync(out, 0, sizeof(double) * 3 * n, s));
+    std::string err;
+    hyowon_treepm_params Pm = h->tp;
+    Pm.particle_mass = h->uniform_mass;
+    rc = tree::device_short_forces(Pm, h->n, px, px + n, px + 2 * n, nullptr, out, out + n,
+                                   out + 2 * n, s, nullptr, &err);
+    if (rc) return fail(h, rc, "TreePM short range: " + err);
+    return status_or_cuda(h, fp32::add_accelerations(h->f32, s, out, out + n, out + 2 * n));
+}
+
 // Force solve at the current positions; accelerations become valid.
 int solve_force(hyowon_pm_t h) {
     if (!h->sorted) {
@@ -443,9 +561,13 @@ int solve_force(hyowon_pm_t h) {
         if (rc) return h->precision == HYOWON_FP32_FIXED ? status_or_cuda(h, rc) : rc;
         h->sorted = true;
     }
+    if (h->precision == HYOWON_FP64 && h->order_state == 0) {
+        int rc = index_current(h);
+        if (rc) return rc;
+    }
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
     record(h, 0);
-    int rc = enqueue_force(h, h->pc, h->mc, false, 0.0);
+    int rc = enqueue_force(h, h->pc, h->mc, false, 0.0, current_order(h));
     if (rc) return rc;
     unsigned int st = 0;
     rc = read_status(h, &st);
@@ -507,22 +629,32 @@ int kdk_step_impl(hyowon_pm_t h, double K1, double D, double K2, double* max_dri
     const bool sort_now = h->sort_interval <= 1 || h->since_sort + 1 >= h->sort_interval;
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
     CK(cudaMemsetAsync(h->d_maxdrift, 0, sizeof(unsigned long long), h->stream));
-    if (sort_now)
-        CK(cudaMemsetAsync(h->sort.count, 0, sizeof(uint32_t) * (h->sort.n_buckets + 1), h->stream));
+    CK(cudaMemsetAsync(h->sort.count, 0, sizeof(uint32_t) * (h->sort.n_buckets + 1), h->stream));
+    CK(cudaMemsetAsync(h->d_max_count, 0, sizeof(uint32_t), h->stream));
     record(h, 0);
     // 1. candidate = K1 kick + drift of the current state, into the spare set.
     const ParticlesF64 cur = set_view(h, h->pc, h->mc);
     const ParticlesF64 cand = set_view(h, 1 - h->pc, 1 - h->mc);
     ++h->launches;
     launch_kick_drift_key_f64(n, cur, h->acc[0], h->acc[1], h->acc[2], K1, D, h->axis, cand,
-                              h->sort, sort_now, h->d_maxdrift, h->d_status, h->stream);
-    // Positions / momenta of the force solve: the candidate set itself, or, on
-    // sort steps, the current set the candidate is scattered into in cell order.
+                              h->sort, true, h->d_maxdrift, h->d_status, h->stream);
+    // Positions / momenta of the force solve: the candidate set itself, in cell
+    // order through the order index, or, on sort steps, the current set the
+    // candidate is scattered into in cell order.
     int P = 1 - h->pc, M = 1 - h->mc;
     const int ic_before = h->ic;
+    h->launches += launch_exclusive_scan(h->sort.count, h->sort.offset, h->sort.n_buckets + 1,
+                                         h->sort.scan_tmp, h->stream);
+    ++h->launches;
+    launch_max_count_f64(h->sort.n_buckets, h->sort.count, h->d_max_count, h->stream);
+    const uint32_t* order = nullptr;
+    if (!sort_now) {
+        ++h->launches;
+        launch_order(n, h->sort.key, h->sort.rank, h->sort.offset, h->order, h->d_status,
+                     h->stream);
+        order = h->order;
+    }
     if (sort_now) {
-        h->launches += launch_exclusive_scan(h->sort.count, h->sort.offset, h->sort.n_buckets + 1,
-                                             h->sort.scan_tmp, h->stream);
         const double* src[8];
         double* dst[8];
         int k = 0;
@@ -546,18 +678,21 @@ int kdk_step_impl(hyowon_pm_t h, double K1, double D, double K2, double* max_dri
         h->ic = 1 - h->ic;
     }
     // Kernels after the candidate skip all writes when it failed (status gate).
-    int rc = enqueue_force(h, P, M, true, K2);
+    int rc = enqueue_force(h, P, M, true, K2, order);
     if (rc) return rc;
     unsigned int st = 0;
     rc = read_status(h, &st);
     if (rc) return rc;
     collect_timing(h);
     if (st & ST_BLOCKS_PUBLISH) {
-        // Nothing was published: state is that of the step's start.
+        // Nothing was published: state is that of the step's start; the bucket
+        // offsets now describe the unpublished candidate.
         h->ic = ic_before;
+        h->order_state = 0;
         return status_to_code(h, st);
     }
     h->pc = P;
+    h->order_state = sort_now ? 1 : 2;
     h->since_sort = sort_now ? 0 : h->since_sort + 1;
     if (st) {
         // Positions drifted and momenta K1-kicked are published; the force or
@@ -625,6 +760,7 @@ int hyowon_pm_create(double box_size, uint64_t mesh_size, int method, int deconv
     if (cudaMallocHost(reinterpret_cast<void**>(&h->h_status), sizeof(unsigned int)) != cudaSuccess
         || cudaMallocHost(reinterpret_cast<void**>(&h->h_maxdrift), sizeof(unsigned long long)) != cudaSuccess
         || dalloc(&h->d_status, 1) != cudaSuccess || dalloc(&h->d_maxdrift, 1) != cudaSuccess
+        || dalloc(&h->d_max_count, 1) != cudaSuccess
         || dalloc(&h->d_diag, diag::scratch_doubles()) != cudaSuccess)
         return bail(HYOWON_ENOMEM);
     for (auto& e : h->ev) {
@@ -719,6 +855,7 @@ int hyowon_pm_destroy(hyowon_pm_t h) {
     if (!h) return HYOWON_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     hyowon::ic::workspace_destroy(h->ic_ws);
+    hyowon::adj::destroy_cache(h->adj);
     if (h->f32) fp32::destroy(h->f32);
     if (h->plans) {
         cufftDestroy(h->plan_r2c);
@@ -733,11 +870,13 @@ int hyowon_pm_destroy(hyowon_pm_t h) {
     cudaFree(h->lap);
     cudaFree(h->win);
     free_particles(h);
+    cudaFree(h->tree_buf);
     cudaFree(h->sort.count);
     cudaFree(h->sort.offset);
     cudaFree(h->sort.scan_tmp);
     cudaFree(h->d_status);
     cudaFree(h->d_maxdrift);
+    cudaFree(h->d_max_count);
     cudaFree(h->d_diag);
     if (h->h_status) cudaFreeHost(h->h_status);
     if (h->h_maxdrift) cudaFreeHost(h->h_maxdrift);
@@ -779,15 +918,18 @@ int hyowon_pm_upload(hyowon_pm_t h, uint64_t n64, const double* x, const double*
     h->has_state = false;
     h->acc_valid = false;
     h->sorted = false;
+    h->order_state = 0;
     // Input mass (pm_solver.cpp:87-118): uniform = correctly rounded m*n;
     // explicit masses summed in a wide accumulator.
     double total = 0.0;
+    double max_mass = masses ? 0.0 : uniform_mass;
     if (masses) {
         long double s = 0.0L, c = 0.0L;
         for (uint32_t i = 0; i < n; ++i) {
             const double m = masses[i];
             if (!std::isfinite(m) || m < 0.0)
                 return fail(h, HYOWON_EINVAL, "PMSolver explicit masses must be finite and non-negative");
+            max_mass = m > max_mass ? m : max_mass;
             const long double t = s + m;
             c += (std::fabs(s) >= std::fabs(static_cast<long double>(m))) ? (s - t) + m : (m - t) + s;
             s = t;
@@ -799,6 +941,7 @@ int hyowon_pm_upload(hyowon_pm_t h, uint64_t n64, const double* x, const double*
     if (!std::isfinite(total) || total <= 0.0)
         return fail(h, HYOWON_ERUNTIME, "PMSolver exact input mass identity must be finite and positive");
     set_input_mass(h, total, n);
+    h->max_mass = max_mass;
     h->uniform_mass = masses ? 0.0 : uniform_mass;
     h->has_masses = masses != nullptr;
     h->n = n;
@@ -860,6 +1003,7 @@ int hyowon_pm_lpt_ics(hyowon_pm_t h, uint64_t n_side, const double* noise, uint6
     const uint32_t n = static_cast<uint32_t>(n64);
     const int N = static_cast<int>(n_side);
     h->has_state = h->acc_valid = h->sorted = false;
+    h->order_state = 0;
     double* d_noise = nullptr;
     double* tab = nullptr;
     CK(dalloc(&d_noise, n64));
@@ -902,6 +1046,7 @@ int hyowon_pm_lpt_ics(hyowon_pm_t h, uint64_t n_side, const double* noise, uint6
     h->uniform_mass = uniform_mass;
     h->has_masses = false;
     set_input_mass(h, uniform_mass * static_cast<double>(n), n);
+    h->max_mass = uniform_mass;
     if (rc == HYOWON_OK) {
         if (h->precision == HYOWON_FP64) {
             h->pc = h->mc = h->ic = 0;
@@ -940,6 +1085,7 @@ int hyowon_pm_generate_ics(hyowon_pm_t h, const hyowon_ic_params_t* p, uint64_t 
     double2* d_amp = nullptr;
     if ((rc = hyowon::ic::upload_amplitudes(r, n_power, power, &d_amp, &err))) return fail(h, rc, err);
     h->has_state = h->acc_valid = h->sorted = false;
+    h->order_state = 0;
     double* tmp_pos[3] = {};
     double* tmp_mom[3] = {};
     if (h->precision == HYOWON_FP64) {
@@ -973,6 +1119,7 @@ int hyowon_pm_generate_ics(hyowon_pm_t h, const hyowon_ic_params_t* p, uint64_t 
     h->uniform_mass = uniform_mass;
     h->has_masses = false;
     set_input_mass(h, uniform_mass * static_cast<double>(n), n);
+    h->max_mass = uniform_mass;
     if (rc == HYOWON_OK) {
         if (h->precision == HYOWON_FP64) {
             h->pc = h->mc = h->ic = 0;
@@ -1208,11 +1355,16 @@ int hyowon_pm_download_mass_mesh(hyowon_pm_t h, double* mesh) {
     if (h->precision == HYOWON_FP32_FIXED)
         return status_or_cuda(h, fp32::download_mass_mesh(h->f32, h->stream, h->d_status, mesh));
     const size_t cells = static_cast<size_t>(h->N) * h->N * h->N;
+    if (h->order_state == 0) {
+        int rc = index_current(h);
+        if (rc) return rc;
+    }
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
-    CK(cudaMemsetAsync(h->mesh, 0, sizeof(double) * cells, h->stream));
     ++h->launches;
-    launch_deposit_f64(h->n, set_view(h, h->pc, h->mc), h->has_masses ? h->mass[h->ic] : nullptr,
-                       h->uniform_mass, h->axis, h->mesh, h->d_status, h->stream);
+    CK(launch_deposit_tiles_f64(set_view(h, h->pc, h->mc), h->has_masses ? h->mass[h->ic] : nullptr,
+                                h->uniform_mass, current_order(h), h->sort, h->axis,
+                                h->d_max_count, deposit_mass_exponent_f64(h->max_mass), h->mesh,
+                                h->d_status, h->stream));
     unsigned int st = 0;
     int rc = read_status(h, &st);
     if (rc) return rc;
@@ -1249,6 +1401,134 @@ int hyowon_pm_cell_coords(hyowon_pm_t h, int64_t* base, double* frac) {
     cudaFree(df);
     cudaFree(stage);
     return rc;
+}
+
+int hyowon_pm_set_treepm_short_range(hyowon_pm_t h, double theta, double softening,
+                                     double cutoff) {
+    if (!h) return HYOWON_EINVAL;
+    if (h->method != HYOWON_TREEPM_LONG_RANGE)
+        return fail(h, HYOWON_EINVAL, "TreePM short range needs a HYOWON_TREEPM_LONG_RANGE handle");
+    if (cutoff == 0.0) {
+        h->treepm_short = false;
+        if (h->f32) fp32::set_short_range_hook(h->f32, nullptr, nullptr);
+        h->acc_valid = false;
+        return HYOWON_OK;
+    }
+    if (!(std::isfinite(theta) && theta > 0.0) || !(std::isfinite(softening) && softening > 0.0)
+        || !(std::isfinite(cutoff) && cutoff > 0.0 && cutoff < 0.5 * h->L))
+        return fail(h, HYOWON_EINVAL,
+                    "TreePM parameters must be finite and positive with r_cut < L/2");
+    h->tp = hyowon_treepm_params{};
+    h->tp.box_size = h->L;
+    h->tp.split_scale = h->r_s;
+    h->tp.cutoff = cutoff;
+    h->tp.softening = softening;
+    h->tp.theta = theta;
+    h->tp.particle_mass = 1.0;   // the handle's mass at solve time is used
+    h->tp.precision = h->precision;
+    h->treepm_short = true;
+    if (h->f32) fp32::set_short_range_hook(h->f32, short_range_hook_f32, h);
+    h->acc_valid = false;
+    return HYOWON_OK;
+}
+
+int hyowon_pm_treepm_short_forces(hyowon_pm_t h, double theta, double softening, double cutoff,
+                                  double* ax, double* ay, double* az, double* stats) {
+    release_ic_workspace(h);
+    if (!h) return HYOWON_EINVAL;
+    if (!h->has_state) return fail(h, HYOWON_ELOGIC, "no particles uploaded");
+    if (h->method != HYOWON_TREEPM_LONG_RANGE)
+        return fail(h, HYOWON_EINVAL, "TreePM short range needs a HYOWON_TREEPM_LONG_RANGE handle");
+    if (!(std::isfinite(theta) && theta > 0.0) || !(std::isfinite(softening) && softening > 0.0)
+        || !(std::isfinite(cutoff) && cutoff > 0.0 && cutoff < 0.5 * h->L))
+        return fail(h, HYOWON_EINVAL,
+                    "TreePM parameters must be finite and positive with r_cut < L/2");
+    int rc = ensure_tree_buffer(h);
+    if (rc) return rc;
+    hyowon_treepm_params P{};
+    P.box_size = h->L;
+    P.split_scale = h->r_s;
+    P.cutoff = cutoff;
+    P.softening = softening;
+    P.theta = theta;
+    P.particle_mass = h->uniform_mass > 0.0 ? h->uniform_mass : 1.0;
+    P.precision = h->precision;
+    const size_t n = h->n;
+    double* pos = h->tree_buf;
+    double* out = h->tree_buf + 3 * n;
+    const double *x, *y, *z;
+    const double* masses = nullptr;
+    const uint32_t* id;
+    if (h->precision == HYOWON_FP32_FIXED) {
+        rc = fp32::positions_f64(h->f32, h->stream, pos, pos + n, pos + 2 * n);
+        if (rc) return status_or_cuda(h, rc);
+        x = pos;
+        y = pos + n;
+        z = pos + 2 * n;
+        id = fp32::current_ids(h->f32);
+    } else {
+        x = h->pos[h->pc][0];
+        y = h->pos[h->pc][1];
+        z = h->pos[h->pc][2];
+        masses = h->has_masses ? h->mass[h->ic] : nullptr;
+        id = h->id[h->ic];
+    }
+    CK(cudaMemsetAsync(out, 0, sizeof(double) * 3 * n, h->stream));
+    std::string err;
+    rc = tree::device_short_forces(P, h->n, x, y, z, masses, out, out + n, out + 2 * n, h->stream,
+                                   stats, &err);
+    if (rc) return fail(h, rc, "TreePM short range: " + err);
+    double* host[3] = {ax, ay, az};
+    for (int a = 0; a < 3; ++a) {
+        if (!host[a]) continue;
+        ++h->launches;
+        launch_unpermute_f64(h->n, id, out + a * n, pos + a * n, h->stream);
+        CK(cudaMemcpyAsync(host[a], pos + a * n, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                           h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return HYOWON_OK;
+}
+
+int hyowon_pm_debug_set_wait_limit(hyowon_pm_t h, unsigned polls) {
+    if (!h) return HYOWON_EINVAL;
+    if (h->fft_plan) poisson::set_wait_limit(h->fft_plan, polls);
+    if (h->f32) fp32::set_wait_limit(h->f32, polls);
+    return HYOWON_OK;
+}
+
+int hyowon_pm_debug_offset_mass_target(hyowon_pm_t h, double delta) {
+    if (!h || !std::isfinite(delta)) return HYOWON_EINVAL;
+    h->mass_target_offset = delta;
+    if (h->f32) {
+        const double u = std::fabs(delta);
+        fp32::set_mass_check_offset(h->f32, u >= 1.0 ? static_cast<unsigned long long>(u) : (delta != 0.0 ? 1ull : 0ull));
+    }
+    h->acc_valid = false;
+    return HYOWON_OK;
+}
+
+int hyowon_pm_vjp(hyowon_pm_t h, const hyowon_vjp_config* cfg, const double* noise,
+                  const double* target_delta, double* loss, double* grad_noise,
+                  double* final_delta, double* timings) {
+    release_ic_workspace(h);
+    if (!h) return HYOWON_EINVAL;
+    if (!cfg || !noise || !loss) return fail(h, HYOWON_EINVAL, "config, noise and loss must be non-null");
+    if (h->method != HYOWON_PURE_PM)
+        return fail(h, HYOWON_EINVAL, "the VJP differentiates the pure-PM step");
+    hyowon_vjp_config c = *cfg;
+    c.box_size = h->L;
+    c.mesh_size = static_cast<uint64_t>(h->N);
+    c.precision = h->precision;
+    if (c.n_side < 2 || c.n_steps < 1 || !c.K1 || !c.D || !c.K2 || c.n_nodes < 2 || !c.ln_k
+        || !c.ln_p || !c.ln_p_y2 || !(c.particle_mass > 0.0))
+        return fail(h, HYOWON_EINVAL, "invalid VJP configuration");
+    if (grad_noise && !target_delta)
+        return fail(h, HYOWON_EINVAL, "the gradient needs a target density");
+    std::string err;
+    const int rc = hyowon::adj::run_cached(&h->adj, c, h->stream, noise, target_delta, loss,
+                                           grad_noise, final_delta, timings, &err);
+    return rc ? fail(h, rc, "VJP: " + err) : HYOWON_OK;
 }
 
 int hyowon_pm_set_sort_interval(hyowon_pm_t h, int steps) {

@@ -39,6 +39,7 @@ struct Plan {
     CUtensorMap x;
     int N = 0;
     bool fp32 = false;
+    unsigned wait_limit = 1u << 24;  // polls of a pipeline wait before a block gives up
 };
 
 namespace {
@@ -338,7 +339,9 @@ struct SourceEpiF64 {
 };
 
 // Bounded polls of a pipeline barrier before a block gives up (each poll may
-// suspend for a hardware-chosen interval; a healthy wait needs a few).
+// suspend for a hardware-chosen interval; a healthy wait needs a few). The
+// first wait of each tile uses the plan's limit (this value unless a test
+// lowered it); draining the copies in flight after a failure always uses this.
 constexpr unsigned kWaitLimit = 1u << 24;
 
 // Complex transforms of the CC columns of each tile of the chunked half
@@ -356,7 +359,7 @@ constexpr unsigned kWaitLimit = 1u << 24;
 template <typename T, int LOG2N, int AXIS, int SIGN, int MODE, typename GF>
 __global__ void __launch_bounds__(Geo<T, LOG2N>::TC, sizeof(T) == 4 ? HYOWON_FFT_MINB_C32 : HYOWON_FFT_MINB_C64)
 k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
-          const cx_t<T>* __restrict__ tw, GF green, unsigned int* status) {
+          const cx_t<T>* __restrict__ tw, GF green, unsigned int* status, unsigned wait_limit) {
     using G = Geo<T, LOG2N>;
     using C = cx_t<T>;
     constexpr int P = G::N / 16;
@@ -410,7 +413,7 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
             tma::fence_proxy_async();
             issue(nt, static_cast<int>((i + NB - 1) % NB));
         }
-        const bool ok = tma::mbar_wait(&full[b], parity, kWaitLimit);
+        const bool ok = tma::mbar_wait(&full[b], parity, wait_limit);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
                 atomicOr(status, ST_PIPELINE);
@@ -539,7 +542,8 @@ int columns(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF green, unsigned int
     const unsigned tiles = static_cast<unsigned>(G::KC) * G::N;
     const unsigned full = static_cast<unsigned>(sms) * static_cast<unsigned>(per_sm);
     const unsigned grid = tiles < full ? tiles : full;
-    kernel<<<grid, G::TC, G::smem_c, s>>>(AXIS == 1 ? p->y : p->x, H, tw, green, status);
+    kernel<<<grid, G::TC, G::smem_c, s>>>(AXIS == 1 ? p->y : p->x, H, tw, green, status,
+                                          p->wait_limit);
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
@@ -666,6 +670,10 @@ Plan* create_plan(int N, bool fp32, void* modes, const char** err) {
 }
 
 void destroy_plan(Plan* p) { delete p; }
+
+void set_wait_limit(Plan* p, unsigned polls) {
+    if (p) p->wait_limit = polls;
+}
 
 int forward_f64(const Plan* p, int N, const double* mass, double2* modes, const double2* tw,
                 unsigned int* status, cudaStream_t s) {

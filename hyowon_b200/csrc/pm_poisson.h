@@ -33,6 +33,9 @@ size_t modes_elements_f32(int N);
 struct Plan;
 Plan* create_plan(int N, bool fp32, void* modes, const char** err);
 void destroy_plan(Plan* p);
+// Polls of each pipeline wait before a block of a column pass gives up with
+// ST_PIPELINE (default 2^24; tests lower it to exercise the failure path).
+void set_wait_limit(Plan* p, unsigned polls);
 
 // exp(-2 pi i m / N) for m < N as (re, im) pairs, rounded from long double.
 void twiddles(int N, double* re_im);

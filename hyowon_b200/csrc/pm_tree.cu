@@ -33,6 +33,7 @@
 #include "hyowon_treepm.h"
 #include "pm_common.cuh"
 #include "pm_kernels.h"
+#include "pm_tree.h"
 
 namespace hyowon::tree {
 
@@ -331,18 +332,23 @@ struct WalkParams {
     double L, r_cut, eps, theta, r_s, G, m;
 };
 
+// Targets: sorted slots tslot[t] (null: target t is sorted slot t, every
+// source). Output of target t goes to index out_idx[t] (null: t), written, or
+// added to what is there when `add`. Source masses: sorted sm[] (null: P.m).
 template <typename R>
 __global__ void __launch_bounds__(128)
 k_walk(uint32_t n_targets, const uint32_t* __restrict__ tslot, const double* __restrict__ sx,
        const double* __restrict__ sy, const double* __restrict__ sz,
-       const unsigned long long* __restrict__ skey, const Node* __restrict__ nodes,
-       uint32_t n_nodes, WalkParams P, double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
+       const double* __restrict__ sm, const unsigned long long* __restrict__ skey,
+       const Node* __restrict__ nodes, uint32_t n_nodes, WalkParams P,
+       const uint32_t* __restrict__ out_idx, int add, double* __restrict__ ax,
+       double* __restrict__ ay, double* __restrict__ az,
        unsigned long long* __restrict__ counters, unsigned int* status) {
     __shared__ uint32_t stack[4][kStack];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t t = (blockIdx.x * 4 + warp) * 32 + lane;
     const bool valid = t < n_targets;
-    uint32_t slot = valid ? tslot[t] : 0u;
+    uint32_t slot = valid ? (tslot ? tslot[t] : t) : 0u;
     const double tx = sx[slot], ty = sy[slot], tz = sz[slot];
     const unsigned long long tkey = skey[slot];
     const R eps2 = static_cast<R>(P.eps * P.eps);
@@ -395,7 +401,7 @@ k_walk(uint32_t n_targets, const uint32_t* __restrict__ tslot, const double* __r
                     const double r2 = dx * dx + dy * dy + dz * dz;
                     if (!(r2 < rc2) || r2 == 0.0) continue;
                     const R f = short_factor_impl<R>(static_cast<R>(r2), eps2, inv_rs, inv_rs3)
-                        * static_cast<R>(P.G * P.m);
+                        * static_cast<R>(P.G * (sm ? sm[i] : P.m));
                     fx += f * static_cast<R>(dx);
                     fy += f * static_cast<R>(dy);
                     fz += f * static_cast<R>(dz);
@@ -448,11 +454,64 @@ k_walk(uint32_t n_targets, const uint32_t* __restrict__ tslot, const double* __r
         }
     }
     if (valid) {
-        ax[t] = static_cast<double>(fx);
-        ay[t] = static_cast<double>(fy);
-        az[t] = static_cast<double>(fz);
+        const uint32_t o = out_idx ? out_idx[t] : t;
+        if (add) {
+            ax[o] += static_cast<double>(fx);
+            ay[o] += static_cast<double>(fy);
+            az[o] += static_cast<double>(fz);
+        } else {
+            ax[o] = static_cast<double>(fx);
+            ay[o] = static_cast<double>(fy);
+            az[o] = static_cast<double>(fz);
+        }
         atomicAdd(&counters[0], visits);
         atomicAdd(&counters[1], pairs);
+    }
+}
+
+// Per-particle masses: node mass and centre of mass summed bottom-up, one
+// level at a time from the deepest (leaves from their sources in sorted order,
+// internal nodes from their children in child order: a fixed order, so the
+// moments are the same bits run to run). A massless node keeps its cube centre.
+__global__ void k_gather_masses(uint32_t n, const uint32_t* __restrict__ val,
+                                const double* __restrict__ mass, double* __restrict__ sm) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) sm[i] = mass[val[i]];
+}
+
+__global__ void k_moments(uint32_t begin, uint32_t end, const double* __restrict__ sx,
+                          const double* __restrict__ sy, const double* __restrict__ sz,
+                          const double* __restrict__ sm, Node* __restrict__ nodes) {
+    const uint32_t k = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= end) return;
+    Node& nd = nodes[k];
+    double M = 0.0, X = 0.0, Y = 0.0, Z = 0.0;
+    if (nd.leaf) {
+        for (uint32_t i = nd.start; i < nd.end; ++i) {
+            const double m = sm[i];
+            M += m;
+            X += m * sx[i];
+            Y += m * sy[i];
+            Z += m * sz[i];
+        }
+    } else {
+        for (uint32_t c = 0; c < nd.n_child; ++c) {
+            const Node& ch = nodes[nd.first_child + c];
+            M += ch.mass;
+            X += ch.mass * ch.mx;
+            Y += ch.mass * ch.my;
+            Z += ch.mass * ch.mz;
+        }
+    }
+    nd.mass = M;
+    if (M > 0.0) {
+        nd.mx = X / M;
+        nd.my = Y / M;
+        nd.mz = Z / M;
+    } else {
+        nd.mx = nd.cx;
+        nd.my = nd.cy;
+        nd.mz = nd.cz;
     }
 }
 
@@ -508,26 +567,21 @@ thread_local std::string g_err;
 
 }  // namespace
 
-int short_forces(const hyowon_treepm_params& P, uint32_t n, const double* hx, const double* hy,
-                 const double* hz, uint32_t nt, const uint32_t* htargets, double* hax,
-                 double* hay, double* haz, double* stats) {
-    cudaStream_t s = nullptr;
-    TCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    struct StreamGuard {
-        cudaStream_t s;
-        ~StreamGuard() { cudaStreamDestroy(s); }
-    } guard{s};
+// Builds the octree of the n device sources (x, y, z; masses or, when null,
+// P.particle_mass) and walks the targets on stream s: with host_targets the
+// nt listed source indices, results written to ax/ay/az[target] in list order;
+// without (nt = n), every source in key order, results added to
+// ax/ay/az[source]. Output arrays are device memory. Device work is ordered on
+// s; the call returns after it has finished.
+int run(const hyowon_treepm_params& P, uint32_t n, const double* x, const double* y,
+        const double* z, const double* masses, const uint32_t* host_targets, uint32_t nt,
+        double* ax, double* ay, double* az, cudaStream_t s, double* stats) {
     Mem mem;
-    cudaEvent_t e0, e1, e2;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventCreate(&e2);
-    double* x = mem.get<double>(n);
-    double* y = mem.get<double>(n);
-    double* z = mem.get<double>(n);
-    TCK(cudaMemcpyAsync(x, hx, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    TCK(cudaMemcpyAsync(y, hy, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    TCK(cudaMemcpyAsync(z, hz, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    struct Events {
+        cudaEvent_t e[4] = {};
+        Events() { for (auto& v : e) cudaEventCreate(&v); }
+        ~Events() { for (auto& v : e) cudaEventDestroy(v); }
+    } ev;
     unsigned int* status = mem.get<unsigned int>(1);
     TCK(cudaMemsetAsync(status, 0, sizeof(unsigned int), s));
     double* wx = mem.get<double>(n);
@@ -535,7 +589,7 @@ int short_forces(const hyowon_treepm_params& P, uint32_t n, const double* hx, co
     double* wz = mem.get<double>(n);
     unsigned long long* key[2] = {mem.get<unsigned long long>(n), mem.get<unsigned long long>(n)};
     uint32_t* val[2] = {mem.get<uint32_t>(n), mem.get<uint32_t>(n)};
-    cudaEventRecord(e0, s);
+    cudaEventRecord(ev.e[0], s);
     k_keys<<<nb(n), kT, 0, s>>>(n, x, y, z, P.box_size, wx, wy, wz, key[0], val[0], status);
     // radix sort
     const uint32_t n_tiles = static_cast<uint32_t>((n + kTile - 1) / kTile);
@@ -566,6 +620,11 @@ int short_forces(const hyowon_treepm_params& P, uint32_t n, const double* hx, co
     k_gather_sorted<<<nb(n + 1), kT, 0, s>>>(n, sval, wx, wy, wz, P.box_size, sx, sy, sz, q[0],
                                              q[1], q[2], inv);
     for (int a = 0; a < 3; ++a) scan64(mem, q[a], pq[a], n + 1, s);
+    double* sm = nullptr;
+    if (masses) {
+        sm = mem.get<double>(n);
+        k_gather_masses<<<nb(n), kT, 0, s>>>(n, sval, masses, sm);
+    }
     // level-wise build
     const uint64_t cap = 6ull * n + 64;  // nodes; exceeding it is reported, not overrun
     Node* nodes = mem.get<Node>(cap);
@@ -580,6 +639,7 @@ int short_forces(const hyowon_treepm_params& P, uint32_t n, const double* hx, co
     uint32_t* node_of_run[2] = {mem.get<uint32_t>(n + 1), mem.get<uint32_t>(n + 1)};
     uint32_t node_base = 0, prev_runs = 0;
     int depth = 0;
+    std::vector<uint32_t> level_begin;
     for (int level = 0; level <= kBits; ++level) {
         const int c = level & 1, p = 1 - c;
         const int shift = 3 * (kBits - level);
@@ -603,62 +663,74 @@ int short_forces(const hyowon_treepm_params& P, uint32_t n, const double* hx, co
         if (level > 0)
             k_link<<<nb(prev_runs), kT, 0, s>>>(prev_runs, node_of_run[p], internal[p], nodes,
                                                 runid[c], node_of_run[c]);
+        level_begin.push_back(node_base);
         node_base += n_new;
         prev_runs = n_runs;
         depth = level;
     }
-    cudaEventRecord(e1, s);
-    // targets in key order for warp coherence
-    std::vector<uint32_t> inv_h(n);
-    TCK(cudaMemcpyAsync(inv_h.data(), inv, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
-    TCK(cudaStreamSynchronize(s));
-    std::vector<uint32_t> order(nt);
-    for (uint32_t i = 0; i < nt; ++i) {
-        if (htargets[i] >= n) throw Fail{HYOWON_EINVAL, "target index out of range"};
-        order[i] = i;
+    level_begin.push_back(node_base);
+    if (sm) {
+        for (int l = static_cast<int>(level_begin.size()) - 2; l >= 0; --l) {
+            const uint32_t b = level_begin[l], e = level_begin[l + 1];
+            k_moments<<<nb(e - b), kT, 0, s>>>(b, e, sx, sy, sz, sm, nodes);
+        }
     }
-    std::sort(order.begin(), order.end(),
-              [&](uint32_t a, uint32_t b) { return inv_h[htargets[a]] < inv_h[htargets[b]]; });
-    std::vector<uint32_t> slots(nt);
-    for (uint32_t i = 0; i < nt; ++i) slots[i] = inv_h[htargets[order[i]]];
-    uint32_t* dslots = mem.get<uint32_t>(nt);
-    TCK(cudaMemcpyAsync(dslots, slots.data(), sizeof(uint32_t) * nt, cudaMemcpyHostToDevice, s));
-    double* oax = mem.get<double>(nt);
-    double* oay = mem.get<double>(nt);
-    double* oaz = mem.get<double>(nt);
+    cudaEventRecord(ev.e[1], s);
+    const uint32_t* dslots = nullptr;
+    const uint32_t* out_idx = nullptr;
+    std::vector<uint32_t> order;
+    if (host_targets) {
+        // targets in key order for warp coherence; results land in key order
+        std::vector<uint32_t> inv_h(n);
+        TCK(cudaMemcpyAsync(inv_h.data(), inv, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+        TCK(cudaStreamSynchronize(s));
+        order.resize(nt);
+        for (uint32_t i = 0; i < nt; ++i) {
+            if (host_targets[i] >= n) throw Fail{HYOWON_EINVAL, "target index out of range"};
+            order[i] = i;
+        }
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+            return inv_h[host_targets[a]] < inv_h[host_targets[b]];
+        });
+        std::vector<uint32_t> slots(nt), dest(nt);
+        for (uint32_t i = 0; i < nt; ++i) {
+            slots[i] = inv_h[host_targets[order[i]]];
+            dest[i] = order[i];
+        }
+        uint32_t* d_slots = mem.get<uint32_t>(nt);
+        uint32_t* d_dest = mem.get<uint32_t>(nt);
+        TCK(cudaMemcpyAsync(d_slots, slots.data(), sizeof(uint32_t) * nt, cudaMemcpyHostToDevice, s));
+        TCK(cudaMemcpyAsync(d_dest, dest.data(), sizeof(uint32_t) * nt, cudaMemcpyHostToDevice, s));
+        TCK(cudaStreamSynchronize(s));
+        dslots = d_slots;
+        out_idx = d_dest;
+    } else {
+        out_idx = sval;   // sorted slot t holds source sval[t]
+    }
     unsigned long long* counters = mem.get<unsigned long long>(2);
     TCK(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s));
     const double G = 6.67430e-11 * (1e10 * 1.98847e30) / (3.085677581491367e22 * 1000.0 * 1000.0);
     WalkParams W{P.box_size, P.cutoff, P.softening, P.theta, P.split_scale, G, P.particle_mass};
-    cudaEventRecord(e2, s);
+    cudaEventRecord(ev.e[2], s);
     const unsigned blocks = static_cast<unsigned>((nt + 127) / 128);
+    const int add = host_targets ? 0 : 1;
     if (P.precision == HYOWON_FP64)
-        k_walk<double><<<blocks, 128, 0, s>>>(nt, dslots, sx, sy, sz, skey, nodes, node_base, W, oax, oay,
-                                               oaz, counters, status);
+        k_walk<double><<<blocks, 128, 0, s>>>(nt, dslots, sx, sy, sz, sm, skey, nodes, node_base, W,
+                                               out_idx, add, ax, ay, az, counters, status);
     else
-        k_walk<float><<<blocks, 128, 0, s>>>(nt, dslots, sx, sy, sz, skey, nodes, node_base, W, oax, oay,
-                                              oaz, counters, status);
-    cudaEvent_t e3;
-    cudaEventCreate(&e3);
-    cudaEventRecord(e3, s);
-    std::vector<double> bx(nt), by(nt), bz(nt);
-    TCK(cudaMemcpyAsync(bx.data(), oax, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
-    TCK(cudaMemcpyAsync(by.data(), oay, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
-    TCK(cudaMemcpyAsync(bz.data(), oaz, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
+        k_walk<float><<<blocks, 128, 0, s>>>(nt, dslots, sx, sy, sz, sm, skey, nodes, node_base, W,
+                                              out_idx, add, ax, ay, az, counters, status);
+    TCK(cudaPeekAtLastError());
+    cudaEventRecord(ev.e[3], s);
     unsigned long long cnt[2] = {0, 0};
     unsigned int st = 0;
     TCK(cudaMemcpyAsync(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost, s));
     TCK(cudaMemcpyAsync(&st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
     TCK(cudaStreamSynchronize(s));
-    for (uint32_t i = 0; i < nt; ++i) {
-        hax[order[i]] = bx[i];
-        hay[order[i]] = by[i];
-        haz[order[i]] = bz[i];
-    }
     if (stats) {
         float tb = 0.f, tw = 0.f;
-        cudaEventElapsedTime(&tb, e0, e1);
-        cudaEventElapsedTime(&tw, e2, e3);
+        cudaEventElapsedTime(&tb, ev.e[0], ev.e[1]);
+        cudaEventElapsedTime(&tw, ev.e[2], ev.e[3]);
         stats[0] = node_base;
         stats[1] = depth;
         stats[2] = nt ? static_cast<double>(cnt[0]) / nt : 0.0;
@@ -666,14 +738,48 @@ int short_forces(const hyowon_treepm_params& P, uint32_t n, const double* hx, co
         stats[4] = tb;
         stats[5] = tw;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
-    cudaEventDestroy(e3);
     if (st & ST_NONFINITE_INPUT) throw Fail{HYOWON_EINVAL, "source positions must be finite"};
     if (st & ST_CAPACITY) throw Fail{HYOWON_ERUNTIME, "tree walk exceeded its stack or iteration bound"};
     if (st & ST_CELL_ESCAPE) throw Fail{HYOWON_ELOGIC, "octree child link out of range"};
     return HYOWON_OK;
+}
+
+int short_forces(const hyowon_treepm_params& P, uint32_t n, const double* hx, const double* hy,
+                 const double* hz, uint32_t nt, const uint32_t* htargets, double* hax,
+                 double* hay, double* haz, double* stats) {
+    cudaStream_t s = nullptr;
+    TCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } guard{s};
+    Mem mem;
+    double* x = mem.get<double>(n);
+    double* y = mem.get<double>(n);
+    double* z = mem.get<double>(n);
+    TCK(cudaMemcpyAsync(x, hx, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    TCK(cudaMemcpyAsync(y, hy, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    TCK(cudaMemcpyAsync(z, hz, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    double* oax = mem.get<double>(nt);
+    double* oay = mem.get<double>(nt);
+    double* oaz = mem.get<double>(nt);
+    run(P, n, x, y, z, nullptr, htargets, nt, oax, oay, oaz, s, stats);
+    TCK(cudaMemcpyAsync(hax, oax, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
+    TCK(cudaMemcpyAsync(hay, oay, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
+    TCK(cudaMemcpyAsync(haz, oaz, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
+    TCK(cudaStreamSynchronize(s));
+    return HYOWON_OK;
+}
+
+int device_short_forces(const hyowon_treepm_params& P, uint32_t n, const double* x,
+                        const double* y, const double* z, const double* masses, double* ax,
+                        double* ay, double* az, cudaStream_t s, double* stats, std::string* err) {
+    try {
+        return run(P, n, x, y, z, masses, nullptr, n, ax, ay, az, s, stats);
+    } catch (const Fail& f) {
+        if (err) *err = f.msg;
+        return f.code;
+    }
 }
 
 }  // namespace hyowon::tree

@@ -247,6 +247,26 @@ class PMSolver:
             self._h, base.ctypes.data_as(nat.P_i64), nat.dptr(frac)), "cell_coords")
         return base.reshape(3, n), frac.reshape(3, n)
 
+    def set_treepm_short_range(self, theta: float, softening: float, cutoff: float):
+        """TreePM force method: every solve adds the octree short range (theta,
+        Plummer softening, cutoff < L/2) to the long range; cutoff = 0 turns it
+        off (hyowon_pm_set_treepm_short_range)."""
+        self._check(nat.lib().hyowon_pm_set_treepm_short_range(self._h, theta, softening, cutoff),
+                    "set_treepm_short_range")
+
+    def treepm_short_forces(self, theta: float, softening: float, cutoff: float):
+        """Short-range accelerations of every particle of the device state in
+        original order: (ax, ay, az, stats) (hyowon_pm_treepm_short_forces)."""
+        n = self.info()[0]
+        out = [np.empty(n) for _ in range(3)]
+        stats = np.zeros(6)
+        self._check(nat.lib().hyowon_pm_treepm_short_forces(
+            self._h, theta, softening, cutoff, *(nat.dptr(o) for o in out), nat.dptr(stats)),
+            "treepm_short_forces")
+        info = dict(zip(("nodes", "depth", "visits_per_target", "interactions_per_target",
+                         "build_ms", "walk_ms"), stats.tolist()))
+        return out[0], out[1], out[2], info
+
     def set_sort_interval(self, steps: int):
         self._check(nat.lib().hyowon_pm_set_sort_interval(self._h, int(steps)), "set_sort_interval")
 

@@ -25,6 +25,8 @@
 
 #include <stdint.h>
 
+#include "hyowon_pm.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -58,6 +60,17 @@ int hyowon_vjp_1lpt_pm(const hyowon_vjp_config* cfg, const double* noise,
                        double* final_delta, double* timings);
 
 const char* hyowon_vjp_last_error(void);
+
+/* The same VJP on a PM handle (the drop-in's vjp(handle, ...)): the handle
+ * supplies the box, the mesh and the arithmetic form (cfg->box_size,
+ * mesh_size and precision are ignored), runs on the handle's stream and keeps
+ * the adjoint's FFT plans and work arrays between calls with the same
+ * geometry (freed by hyowon_pm_destroy). The handle's particle state is not
+ * touched. The handle must use HYOWON_PURE_PM. Errors go to
+ * hyowon_pm_last_error(h). */
+int hyowon_pm_vjp(hyowon_pm_t h, const hyowon_vjp_config* cfg, const double* noise,
+                  const double* target_delta, double* loss, double* grad_noise,
+                  double* final_delta, double* timings);
 
 #ifdef __cplusplus
 }

@@ -21,6 +21,8 @@
 
 #include <stdint.h>
 
+#include "hyowon_pm.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -47,6 +49,31 @@ int hyowon_treepm_short_forces(const hyowon_treepm_params* params, uint64_t n,
                                double* ay, double* az, double* stats);
 
 const char* hyowon_treepm_last_error(void);
+
+/* ---- TreePM on a PM handle ------------------------------------------------
+ * The handle must be created with HYOWON_TREEPM_LONG_RANGE (its split_scale is
+ * r_s). Sources are the handle's device-resident particles with their masses
+ * (per-particle in the binary64 form, uniform in the precision form); the
+ * short-range sum is the same as hyowon_treepm_short_forces's. */
+/* Makes every force solve of the handle (compute_forces, kdk_step, run) the
+ * TreePM force of TreePMSolver::compute_forces (src/gravity/treepm_solver.cpp:
+ * 631-717): the PM long range (Gaussian split at r_s, spectral -ik) plus the
+ * octree short range with opening angle theta, Plummer softening and cutoff
+ * r_cut < L/2, summed per particle before the K2 kick. cutoff = 0 returns the
+ * handle to the long range alone. HYOWON_EINVAL for a pure-PM handle or
+ * invalid parameters. Invalidates the current accelerations. */
+int hyowon_pm_set_treepm_short_range(hyowon_pm_t h, double theta, double softening,
+                                     double cutoff);
+
+/* The short-range accelerations of every particle of the handle's current
+ * state (TreeWalk::compute_force per target, src/gravity/tree_walk.cpp:
+ * 203-464, on Octree::build of all sources, src/gravity/octree.cpp:169-440),
+ * written to host ax/ay/az[n] in the caller's original particle order (any may
+ * be NULL). stats as hyowon_treepm_short_forces (may be NULL). Leaves the
+ * handle's accelerations untouched. */
+int hyowon_pm_treepm_short_forces(hyowon_pm_t h, double theta, double softening,
+                                  double cutoff, double* ax, double* ay, double* az,
+                                  double* stats);
 
 #ifdef __cplusplus
 }

@@ -415,6 +415,23 @@ class Reference:
             out.update(st)
         return out
 
+    def treepm_kdk_run(self, L, n_side, n_mesh, split_scale_cells, cutoff_multiplier, eps, theta,
+                       state, a_start, a_final, delta_ln_a, steps, masses=None, uniform_mass=1.0):
+        """TreePMSolver-driven KDK steps in place on state (x..pz); fills ax..az."""
+        s = state
+        for k in ("ax", "ay", "az"):
+            s.setdefault(k, np.zeros_like(s["x"]))
+        m = None if masses is None else np.ascontiguousarray(masses, dtype=np.float64)
+        self.lib.ref_treepm_kdk_run.argtypes = None
+        rc = self.lib.ref_treepm_kdk_run(
+            _c_double(L), _c_u64(n_side), _c_u64(n_mesh), _c_double(split_scale_cells),
+            _c_double(cutoff_multiplier), _c_double(eps), _c_double(theta), _c_double(a_start),
+            _c_double(a_final), _c_double(delta_ln_a), _c_u64(steps),
+            *(_dp(s[k]) for k in ("x", "y", "z", "px", "py", "pz")), _dp(m),
+            _c_double(uniform_mass), _dp(s["ax"]), _dp(s["ay"]), _dp(s["az"]))
+        self._check(rc, "ref_treepm_kdk_run")
+        return s
+
     def lpt_white_noise(self, L, N, noise, pk_path, z_pk, z_start):
         """1LPT state from white noise through the reference's LinearPowerSpectrum,
         FFTBackend and LPTDisplacement (ref_lpt_white_noise). Returns a dict

@@ -19,6 +19,7 @@
 #include "cosmo_nbody/gravity/force_split.hpp"
 #include "cosmo_nbody/gravity/octree.hpp"
 #include "cosmo_nbody/gravity/tree_walk.hpp"
+#include "cosmo_nbody/gravity/treepm_solver.hpp"
 #include "cosmo_nbody/gravity/pm_solver.hpp"
 #include "cosmo_nbody/ic/linear_power_spectrum.hpp"
 #include "cosmo_nbody/ic/lpt_displacement.hpp"
@@ -775,5 +776,86 @@ int ref_lpt_white_noise(double L, std::uint64_t N, const double* noise, const ch
     });
 }
 
+// TreePM evolution: TimeStepper + LeapfrogIntegrator with the force callback of
+// the runner's TreePM branch (src/runtime/simulation_runner.cpp:1105-1109:
+// TreePMSolver::compute_forces on the particle store, PM long range with the
+// Gaussian split plus the octree short range, src/gravity/treepm_solver.cpp:
+// 631-717). n = n_side^3 particles; masses (n) or, when null, uniform_mass;
+// r_s = split_scale_cells * L / n_mesh, r_cut = cutoff_multiplier * r_s.
+// Runs `steps_to_run` steps on x..pz (in/out) and returns the accelerations of
+// the last force solve.
+int ref_treepm_kdk_run(double L, std::uint64_t n_side, std::uint64_t n_mesh,
+                       double split_scale_cells, double cutoff_multiplier, double eps,
+                       double theta, double a_start, double a_final, double delta_ln_a,
+                       std::uint64_t steps_to_run, double* x, double* y, double* z, double* px,
+                       double* py, double* pz, const double* masses, double uniform_mass,
+                       double* ax, double* ay, double* az) {
+    return guarded([&] {
+        config::GravityParams g;
+        g.solver = "TreePM";
+        g.eps = eps;
+        g.theta = theta;
+        g.split_scale_cells = split_scale_cells;
+        g.cutoff_multiplier = cutoff_multiplier;
+        g.deconvolve_cic = core::ExplicitBoolean(true);
+        config::BoxParams b;
+        b.L = L;
+        b.N = n_side;
+        b.N_mesh = n_mesh;
+        config::TimeParams t;
+        t.z_start = 1.0 / a_start - 1.0;
+        t.z_final = 1.0 / a_final - 1.0;
+        t.delta_ln_a = delta_ln_a;
+        config::ICParams ic;
+        ic.mode = "snapshot";
+        ic.snapshot_file = "unused.hdf5";
+        config::OutputParams o;
+        config::SimulationParameters cfg(flat_lcdm(0.3, 0.7), b, g, t, ic, o);
+        const std::uint64_t n = n_side * n_side * n_side;
+        core::ParticleStore store;
+        store.set_uniform_mass(masses ? 1.0 : uniform_mass);
+        store.resize(n);
+        if (masses) {
+            store.set_uniform_mass(std::nullopt);
+            std::memcpy(store.get_masses().data(), masses, sizeof(double) * n);
+        }
+        std::memcpy(store.get_positions_x().data(), x, sizeof(double) * n);
+        std::memcpy(store.get_positions_y().data(), y, sizeof(double) * n);
+        std::memcpy(store.get_positions_z().data(), z, sizeof(double) * n);
+        std::memcpy(store.get_momenta_x().data(), px, sizeof(double) * n);
+        std::memcpy(store.get_momenta_y().data(), py, sizeof(double) * n);
+        std::memcpy(store.get_momenta_z().data(), pz, sizeof(double) * n);
+
+        cosmology::CosmologyModel model(flat_lcdm(0.3, 0.7));
+        cosmology::DriftKickIntegrator factors(model);
+        mesh::MeshGeometry geom(L, n_mesh);
+        domain::DomainBounds bounds{0.0, L, 0.0, L, 0.0, L};
+        gravity::TreePMSolver solver(cfg, geom, bounds);
+        auto force = [&](std::span<const double>, std::span<const double>,
+                         std::span<const double>, std::span<const double>, std::span<double>,
+                         std::span<double>, std::span<double>, double) {
+            solver.compute_forces(store);
+        };
+        time::LeapfrogIntegrator integrator(store, factors, force, L, 1);
+        time::TimeStepper stepper(a_start, a_final, delta_ln_a);
+        integrator.ensure_force_at(a_start);
+        for (std::uint64_t k = 0; k < steps_to_run; ++k) {
+            auto step = stepper.next_step();
+            if (!step) break;
+            integrator.step(*step);
+        }
+        std::memcpy(x, store.get_positions_x().data(), sizeof(double) * n);
+        std::memcpy(y, store.get_positions_y().data(), sizeof(double) * n);
+        std::memcpy(z, store.get_positions_z().data(), sizeof(double) * n);
+        std::memcpy(px, store.get_momenta_x().data(), sizeof(double) * n);
+        std::memcpy(py, store.get_momenta_y().data(), sizeof(double) * n);
+        std::memcpy(pz, store.get_momenta_z().data(), sizeof(double) * n);
+        std::memcpy(ax, store.get_accelerations_x().data(), sizeof(double) * n);
+        std::memcpy(ay, store.get_accelerations_y().data(), sizeof(double) * n);
+        std::memcpy(az, store.get_accelerations_z().data(), sizeof(double) * n);
+    });
+}
+
 }  // extern "C"
+
 

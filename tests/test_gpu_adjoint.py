@@ -3,12 +3,16 @@
 Stated tolerances:
 * forward loss of the binary64 form vs the oracle (1LPT + KDK + CIC deposit on
   the CPU): relative 1e-8;
-* gradient vs central finite differences of the same forward model
+* gradient vs central finite differences of the binary64 forward model
   (eps = 1e-3 in the noise, 64 random cells of the 128^3 configuration): the
-  relative error ||g - g_fd|| / ||g_fd|| <= 1e-3 (binary64), 1e-2 (FP32
-  gradient against the binary64 finite differences);
-* FP32 gradient vs binary64 gradient: relative 1e-2;
-* checkpoint interval: gradients with ckpt_every 1 / 4 / 16 agree to 1e-9.
+  relative error ||g - g_fd|| / ||g_fd|| <= 1e-3, for the binary64 gradient
+  and for the FP32 gradient (whose own FP32 losses are too noisy for central
+  differences at this eps);
+* FP32 gradient vs binary64 gradient: relative 1e-3;
+* checkpoint interval: gradients with ckpt_every 1 / 4 / 16 agree to 1e-9;
+* cost: (forward + adjoint) / forward <= 3 with the module's own forward
+  (the best of three evaluations); bench.py --workload adjoint reports it
+  against the production forward as well.
 """
 import math
 
@@ -70,33 +74,36 @@ def c4_problem(precision, ckpt=4):
     return dpm, noise, target
 
 
-def test_gradient_vs_finite_differences_c4_fp64():
+@pytest.fixture(scope="module")
+def c4_fd():
+    """Binary64 gradient and central differences on 64 random noise cells."""
     dpm, noise, target = c4_problem("fp64")
     cells = np.random.default_rng(12).choice(noise.size, 64, replace=False)
     grad, g, fd = fd_check(dpm, noise, target, cells)
-    err = np.linalg.norm(g - fd) / np.linalg.norm(fd)
-    t = dpm.last_timings
-    print(f"c4 FP64: |g - fd| / |fd| = {err:.3e}; ")
+    return noise, target, cells, grad, fd
+
+
+def test_gradient_vs_finite_differences_c4_fp64(c4_fd):
+    _, _, cells, grad, fd = c4_fd
+    err = np.linalg.norm(grad[cells] - fd) / np.linalg.norm(fd)
+    print(f"c4 FP64: |g - fd| / |fd| = {err:.3e} (64 cells)")
     assert err <= 1e-3
     assert np.all(np.isfinite(grad))
 
 
-def test_gradient_fp32_vs_fp64_and_fd_c4():
-    d64, noise, target = c4_problem("fp64")
+def test_gradient_fp32_vs_fp64_and_fd_c4(c4_fd):
+    noise, target, cells, g64, fd = c4_fd
+    d64, _, _ = c4_problem("fp64")
     d32, _, _ = c4_problem("fp32")
-    l64, g64 = d64.loss_and_grad(noise, target)
+    l64 = d64.loss(noise, target)
     l32, g32 = d32.loss_and_grad(noise, target)
     rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
     print(f"c4 FP32 vs FP64: loss rel {abs(l32 / l64 - 1):.3e}, gradient rel {rel:.3e}")
     assert abs(l32 / l64 - 1) <= 1e-3
-    assert rel <= 1e-2
-    # FP32 gradient against finite differences of the binary64 forward model
-    # (FP32 losses are too noisy for their own central differences).
-    cells = np.random.default_rng(13).choice(noise.size, 16, replace=False)
-    _, _, fd = fd_check(d64, noise, target, cells)
+    assert rel <= 1e-3
     err = np.linalg.norm(g32[cells] - fd) / np.linalg.norm(fd)
-    print(f"c4 FP32 gradient vs binary64 FD: {err:.3e}")
-    assert err <= 1e-2
+    print(f"c4 FP32 gradient vs binary64 FD: {err:.3e} (64 cells)")
+    assert err <= 1e-3
 
 
 def test_checkpoint_interval_does_not_change_gradient():
@@ -111,10 +118,35 @@ def test_checkpoint_interval_does_not_change_gradient():
 def test_adjoint_cost_ratio_c4():
     dpm, noise, target = c4_problem("fp64")
     dpm.loss_and_grad(noise, target)
-    dpm.loss_and_grad(noise, target)
-    t = dpm.last_timings
-    ratio = (t["forward_ms"] + t["reverse_ms"]) / t["forward_ms"]
+    ratios = []
+    for _ in range(3):
+        dpm.loss_and_grad(noise, target)
+        t = dpm.last_timings
+        ratios.append((t["forward_ms"] + t["reverse_ms"]) / t["forward_ms"])
+    ratio = min(ratios)
     print(f"c4 (forward + adjoint) / forward = {ratio:.2f} "
           f"(forward {t['forward_ms']:.1f} ms, reverse {t['reverse_ms']:.1f} ms)")
-    # target <= 3 (measured 2.83 on B200); the bound leaves room for timing noise
-    assert ratio <= 3.15
+    assert ratio <= 3.0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_handle_vjp_equals_standalone_vjp(precision):
+    """hyowon_pm_vjp on a PM handle (the drop-in's vjp(handle, ...)) gives the
+    standalone call's loss and gradient, and a second call on the same handle
+    (reusing its adjoint plans and work arrays) the same again. Tolerance 1e-12
+    relative (binary64; 1e-6 FP32): the adjoint's deposit and scatter sum with
+    atomics, so the last bits may move between calls."""
+    import hyowon_b200 as hb
+    cfg = ic.CONFIGS["c4"]
+    noise = ic.white_noise(32, 3)
+    target = ic.white_noise(32, 4) * 0.1
+    ref = DifferentiablePM(64.0, 32, 32, 1 / 20, 8, precision)
+    l0, g0 = ref.loss_and_grad(noise, target)
+    with hb.PMSolver(hb.MeshGeometry(64.0, 32), hb.PMForceMethod.pure_pm(False), precision) as s:
+        dpm = DifferentiablePM(64.0, 32, 32, 1 / 20, 8, precision, solver=s)
+        tol = 1e-12 if precision == "fp64" else 1e-6
+        for _ in range(2):
+            l1, g1 = dpm.loss_and_grad(noise, target)
+            assert abs(l1 / l0 - 1) <= tol
+            assert np.linalg.norm(g1 - g0) <= tol * np.linalg.norm(g0)
+    assert cfg["n_side"] == 128  # the c4 sizes are exercised by the tests above
