@@ -185,16 +185,18 @@ __global__ void k_deposit(uint32_t n, const double* __restrict__ x,
 //
 // Owner-computes tiles: one block per tile of TY mesh rows (x0, y0 .. y0+TY-1,
 // all z). Each particle term t = m*wx*wy*wz (the reference's product order, in
-// binary64) is converted exactly in scale to fixed point, q = rint(t 2^(62-e))
-// with m_max < 2^e, so q <= 2^62; q is split at bit W into hi = q >> W and
-// lo = q mod 2^W, and both halves are summed by integer atomics into two
-// shared-memory arrays. W = 63 - floor(log2(8 max_bucket)) keeps every lo sum
-// below 2^64 (a cell's contributors lie in 8 buckets), so no carry is lost and
-// the cell holds the exact integer sum hi_sum 2^W + lo_sum of its quantised
-// terms, independent of atomic order. Each cell is written once, that sum
-// correctly rounded to binary64 and scaled by 2^(e-62) (exact). Quantisation:
-// at most 2^(e-63) per term, below the rounding of one binary64 add of a
-// typical cell.
+// binary64) is converted exactly in scale to fixed point. A cell's contributors
+// lie in 8 buckets, so W = 63 - floor(log2(8 max_bucket)) bounds their count by
+// 2^(64-W). Two forms, chosen on the device from W (kOneWordMinW below):
+//  * one word: q = rint(t 2^(W-1-e)) with m_max < 2^e, summed into one 64-bit
+//    shared-memory word per cell (sums below 2^63), quantum 2^(e+1-W) <=
+//    2^(e-54) per term;
+//  * two words: q = rint(t 2^(62-e)) <= 2^62, split at bit W into hi = q >> W
+//    and lo = q mod 2^W, both halves summed into two arrays; every lo sum stays
+//    below 2^64, so the cell holds the exact integer sum hi 2^W + lo of its
+//    terms, quantum 2^(e-62) per term.
+// Integer sums do not depend on the order atomics land in. Each cell is written
+// once: the sum correctly rounded to binary64 and scaled by a power of two.
 //
 // Contributors are the particles whose base cell lies in plane x0 (weight
 // 1 - fx) or x0-1 (weight fx) and rows y0-1 .. y0+TY-1: at most four contiguous
@@ -205,8 +207,16 @@ __global__ void k_deposit(uint32_t n, const double* __restrict__ x,
 // (plane, row), so every contributor counts once.
 constexpr int kTileThreads = 256;
 #ifndef HYOWON_DEPOSIT64_TILE_CELLS
-#define HYOWON_DEPOSIT64_TILE_CELLS 2048
+#define HYOWON_DEPOSIT64_TILE_CELLS 4096
 #endif
+// One-word accumulators: while the densest bucket is small enough that
+// W >= kOneWordMinW, a single 64-bit word per cell holds the sum of terms
+// quantised to q = rint(t 2^(W-1-e)): a quantum of 2^(e+1-W) <= 2^(e-54), below
+// half the binary64 spacing of a full-weight term (t < 2^e). Cell sums stay
+// below 2^63. Denser states use the exact two-word (hi/lo) sums. Both kernels
+// are launched; the one that does not apply returns at once, so the choice
+// needs no host synchronisation and depends only on the bucket counts.
+constexpr int kOneWordMinW = 55;
 
 __device__ __forceinline__ int fixed_split_bits(const uint32_t* max_count) {
     const unsigned long long c = 8ull * (*max_count > 0u ? *max_count : 1u);
@@ -229,6 +239,7 @@ __device__ __forceinline__ double fixed_to_double(unsigned long long hi, unsigne
     return ldexp(__ull2double_rn(top), 64 - lz);
 }
 
+template <int kDepositWords>
 __global__ void __launch_bounds__(kTileThreads)
 k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
                 const double* __restrict__ z, const double* __restrict__ mass,
@@ -241,6 +252,8 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
     __shared__ int seg_plane[4], seg_row_lo[4], seg_row_hi[4], seg_own[4];
     __shared__ int seg_n;
     if (*status & ST_BLOCKS_PUBLISH) return;
+    const int W = fixed_split_bits(max_count);
+    if ((kDepositWords == 1) != (W >= kOneWordMinW)) return;
     const int N = a.N;
     const int tid = threadIdx.x;
     const int x0 = blockIdx.y;
@@ -249,7 +262,7 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
     const int halo = ty == N ? 0 : 1;
     const int tcells = ty * N;
     unsigned long long* acc_lo = acc;
-    unsigned long long* acc_hi = acc + static_cast<size_t>(TY) * N;
+    unsigned long long* acc_hi = acc + (kDepositWords == 2 ? static_cast<size_t>(TY) * N : 0);
     if (tid == 0) {
         int ns = 0;
         for (int own = 1; own >= 0; --own) {
@@ -279,12 +292,14 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
     }
     for (int e = tid; e < tcells; e += kTileThreads) {
         acc_lo[e] = 0ull;
-        acc_hi[e] = 0ull;
+        if (kDepositWords == 2) acc_hi[e] = 0ull;
     }
     __syncthreads();
-    const int W = fixed_split_bits(max_count);
     const unsigned long long lo_mask = (1ull << W) - 1ull;
-    const int to_fixed = 62 - e_max;
+    // 2^(62 - e_max) (one word: 2^(W-1-e_max)): a multiplication by it is
+    // exact (the product is at most 2^62, and below 2^-1022 it rounds to the
+    // integer 0 either way)
+    const double to_fixed = ldexp(1.0, kDepositWords == 2 ? 62 - e_max : W - 1 - e_max);
     const int ns = seg_n;
     for (int g = 0; g < ns; ++g) {
         const uint32_t p0 = seg_p0[g];
@@ -316,20 +331,30 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
 #pragma unroll
                 for (int oz = 0; oz < 2; ++oz) {
                     const unsigned long long q =
-                        static_cast<unsigned long long>(llrint(ldexp(mxy * wz[oz], to_fixed)));
+                        static_cast<unsigned long long>(__double2ll_rn(mxy * wz[oz] * to_fixed));
                     if (q == 0ull) continue;
-                    atomicAdd(rlo + gz[oz], q & lo_mask);
-                    const unsigned long long qh = q >> W;
-                    if (qh) atomicAdd(rhi + gz[oz], qh);
+                    if (kDepositWords == 1) {
+                        atomicAdd(rlo + gz[oz], q);
+                    } else {
+                        atomicAdd(rlo + gz[oz], q & lo_mask);
+                        const unsigned long long qh = q >> W;
+                        if (qh) atomicAdd(rhi + gz[oz], qh);
+                    }
                 }
             }
         }
     }
     __syncthreads();
     double* out = mesh + (static_cast<uint64_t>(x0) * N + y0) * N;
-    const int from_fixed = e_max - 62;
-    for (int e = tid; e < tcells; e += kTileThreads)
-        out[e] = ldexp(fixed_to_double(acc_hi[e], acc_lo[e], W), from_fixed);
+    if (kDepositWords == 1) {
+        const double from_fixed = ldexp(1.0, e_max + 1 - W);
+        for (int e = tid; e < tcells; e += kTileThreads)
+            out[e] = __ull2double_rn(acc_lo[e]) * from_fixed;
+    } else {
+        const double from_fixed = ldexp(1.0, e_max - 62);
+        for (int e = tid; e < tcells; e += kTileThreads)
+            out[e] = fixed_to_double(acc_hi[e], acc_lo[e], W) * from_fixed;
+    }
 }
 
 __global__ void k_max_count64(uint32_t nb, const uint32_t* __restrict__ count,
@@ -756,8 +781,10 @@ void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,
                                                  mesh, status);
 }
 
-int deposit_tile_rows_f64(int N) {
-    int ty = HYOWON_DEPOSIT64_TILE_CELLS / N;
+// Tile rows for 8-byte-per-cell accumulators of HYOWON_DEPOSIT64_TILE_CELLS
+// cells, halved for the two-word form (same shared memory per tile).
+int deposit_tile_rows_f64(int N, int words) {
+    int ty = HYOWON_DEPOSIT64_TILE_CELLS / words / N;
     if (ty < 1) ty = 1;
     return ty > N ? N : ty;
 }
@@ -768,22 +795,34 @@ int deposit_mass_exponent_f64(double max_mass) {
     return e;
 }
 
+template <int WORDS>
+cudaError_t launch_tiles(const ParticlesF64& p, const double* mass, double uniform_mass,
+                         const uint32_t* order, const SortWork& w, Axis a,
+                         const uint32_t* max_count, int e_max, double* mesh,
+                         const unsigned int* status, cudaStream_t s) {
+    const int N = a.N;
+    const int TY = deposit_tile_rows_f64(N, WORDS);
+    const size_t smem = 8 * WORDS * static_cast<size_t>(TY) * N;
+    cudaError_t e = cudaFuncSetAttribute(k_deposit_tiles<WORDS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const dim3 grid(static_cast<unsigned>((N + TY - 1) / TY), static_cast<unsigned>(N));
+    k_deposit_tiles<WORDS><<<grid, kTileThreads, smem, s>>>(p.x, p.y, p.z, mass, uniform_mass,
+                                                            order, w.offset, w.shift, a, TY,
+                                                            max_count, e_max, mesh, status);
+    return cudaPeekAtLastError();
+}
+
 cudaError_t launch_deposit_tiles_f64(const ParticlesF64& p, const double* mass,
                                      double uniform_mass, const uint32_t* order,
                                      const SortWork& w, Axis a, const uint32_t* max_count,
                                      int e_max, double* mesh, const unsigned int* status,
                                      cudaStream_t s) {
-    const int N = a.N;
-    const int TY = deposit_tile_rows_f64(N);
-    const size_t smem = 16 * static_cast<size_t>(TY) * N;
-    cudaError_t e = cudaFuncSetAttribute(k_deposit_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    cudaError_t e = launch_tiles<1>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh,
+                                    status, s);
     if (e != cudaSuccess) return e;
-    const dim3 grid(static_cast<unsigned>((N + TY - 1) / TY), static_cast<unsigned>(N));
-    k_deposit_tiles<<<grid, kTileThreads, smem, s>>>(p.x, p.y, p.z, mass, uniform_mass, order,
-                                                     w.offset, w.shift, a, TY, max_count, e_max,
-                                                     mesh, status);
-    return cudaPeekAtLastError();
+    return launch_tiles<2>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh, status, s);
 }
 
 void launch_max_count_f64(uint32_t n_buckets, const uint32_t* count, uint32_t* max_count,

@@ -389,7 +389,7 @@ int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2,
     const ParticlesF64 p = set_view(h, pset, mset);
     (void)cells;
     record(h, 1);
-    ++h->launches;
+    h->launches += 2;   // the one-word and two-word tile kernels (one returns at once)
     CK(launch_deposit_tiles_f64(p, h->has_masses ? h->mass[h->ic] : nullptr, h->uniform_mass,
                                 order, h->sort, h->axis, h->d_max_count,
                                 deposit_mass_exponent_f64(h->max_mass), h->mesh, h->d_status,
@@ -1360,7 +1360,7 @@ int hyowon_pm_download_mass_mesh(hyowon_pm_t h, double* mesh) {
         if (rc) return rc;
     }
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
-    ++h->launches;
+    h->launches += 2;
     CK(launch_deposit_tiles_f64(set_view(h, h->pc, h->mc), h->has_masses ? h->mass[h->ic] : nullptr,
                                 h->uniform_mass, current_order(h), h->sort, h->axis,
                                 h->d_max_count, deposit_mass_exponent_f64(h->max_mass), h->mesh,

@@ -72,7 +72,6 @@ void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,
 // no zeroing needed. Needs the bucket offsets of the deposited set in w, the
 // cell order `order` (or null when the arrays are in cell order), the largest
 // bucket count in *max_count and e_max = deposit_mass_exponent_f64(max mass).
-int deposit_tile_rows_f64(int N);
 int deposit_mass_exponent_f64(double max_mass);
 cudaError_t launch_deposit_tiles_f64(const ParticlesF64& p, const double* mass,
                                      double uniform_mass, const uint32_t* order,
