@@ -29,6 +29,11 @@ opening angle 0.5, softening 1/30 of the mean spacing, the clustered z = 0
 state of a 64-step PM run of seed 5): a "step" is one KDK step with the TreePM
 force (long range plus the octree short range of every particle).
 
+`--workload cufft` times cuFFT (through torch.fft) on the data of the c3
+potential solve, for comparison with the five-pass transforms: 1-D transforms
+along x and y of the chunked FP32 half spectrum (65 x 1024 x 1024 x 8
+complex) and the 3-D r2c / c2r of the 1024^3 FP32 mesh.
+
 `--workload ic` times HYOWON's generated initial conditions instead (the
 Philox Fourier field and 2LPT of the 512^3 lattice on the automatic 1024^3 IC
 mesh, L = 1000, z = 49): a "step" is one whole generation through
@@ -76,7 +81,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="step", choices=["step", "ic", "adjoint", "treepm"])
+    ap.add_argument("--workload", default="step",
+                    choices=["step", "ic", "adjoint", "treepm", "cufft"])
     ap.add_argument("--no-side-workloads", action="store_true",
                     help="skip the adjoint (c4) and TreePM (c5) measurements the default step "
                          "line carries")
@@ -563,6 +569,45 @@ def run_treepm(args, rank, emit=True):
     return line
 
 
+def run_cufft(args, rank):
+    """cuFFT on the c3 potential solve's data (see the module docstring)."""
+    if rank != 0:
+        return
+    import torch
+    N, CC = 1024, 8
+    KC = (N // 2 + 1 + CC - 1) // CC
+    x = torch.randn(KC, N, N, CC, dtype=torch.complex64, device="cuda")
+
+    def timed(f):
+        for _ in range(max(1, args.warmup)):
+            f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    res = {"fft_x_ms": timed(lambda: torch.fft.fft(x, dim=1)),
+           "fft_y_ms": timed(lambda: torch.fft.fft(x, dim=2)),
+           "fft_ifft_x_ms": timed(lambda: torch.fft.ifft(torch.fft.fft(x, dim=1), dim=1))}
+    del x
+    torch.cuda.empty_cache()
+    r = torch.randn(N, N, N, dtype=torch.float32, device="cuda")
+    res["rfftn_ms"] = timed(lambda: torch.fft.rfftn(r))
+    h = torch.fft.rfftn(r)
+    res["irfftn_ms"] = timed(lambda: torch.fft.irfftn(h, s=(N, N, N)))
+    line = {"metric": "cuFFT time on the c3 solve's data", "value": res["rfftn_ms"] + res["irfftn_ms"],
+            "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "cuFFT via torch.fft: 1024^3 r2c + c2r, and 1-D transforms of "
+                                   "the 65 x 1024 x 1024 x 8 chunked half spectrum"},
+            "timings": res, "e2e": None}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = setup_dist()
@@ -574,6 +619,9 @@ def main():
         return
     if args.workload == "treepm":
         run_treepm(args, rank)
+        return
+    if args.workload == "cufft":
+        run_cufft(args, rank)
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

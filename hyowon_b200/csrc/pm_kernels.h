@@ -76,7 +76,7 @@ int deposit_mass_exponent_f64(double max_mass);
 cudaError_t launch_deposit_tiles_f64(const ParticlesF64& p, const double* mass,
                                      double uniform_mass, const uint32_t* order,
                                      const SortWork& w, Axis a, const uint32_t* max_count,
-                                     int e_max, double* mesh, const unsigned int* status,
+                                     int e_max, double* mesh, unsigned int* status,
                                      cudaStream_t s);
 void launch_max_count_f64(uint32_t n_buckets, const uint32_t* count, uint32_t* max_count,
                           cudaStream_t s);

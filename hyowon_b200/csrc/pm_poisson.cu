@@ -73,6 +73,13 @@ using fft::mk;
 #ifndef HYOWON_FFT_MINB_C64
 #define HYOWON_FFT_MINB_C64 1
 #endif
+// Column passes on meshes of 256 and more: each tile's CC columns are split
+// into HYOWON_FFT_SPLIT blocks of CC / SPLIT columns (half-width TMA boxes of
+// the same 64-byte rows), so that SPLIT independent blocks share an SM and one
+// block's barrier waits overlap the other's arithmetic.
+#ifndef HYOWON_FFT_SPLIT
+#define HYOWON_FFT_SPLIT 1
+#endif
 
 template <typename T, int LOG2N> struct Shape;
 template <int LOG2N> struct Shape<float, LOG2N> {
@@ -94,7 +101,6 @@ template <typename T, int LOG2N> struct Geo {
     static constexpr int CC = Shape<T, LOG2N>::CC;
     static constexpr int SZ = CZ + 1;
     static constexpr int TZ = CZ * M / 16;   // threads of a z-pass block
-    static constexpr int TC = CC * N / 16;   // threads of a y/x-pass block
     static constexpr int PZ = CZ * M / TZ;   // row pairs each z-pass thread loads (16)
     static constexpr int KC = (Hz + CC - 1) / CC;        // kz chunks
     static constexpr int QZ = (KC * CZ * CC + TZ - 1) / TZ;  // chunked values per z-pass thread
@@ -105,11 +111,17 @@ template <typename T, int LOG2N> struct Geo {
     }
     static constexpr size_t smem_zf = sizeof(C) * M * SZ;
     static constexpr size_t smem_zi = sizeof(C) * Hz * SZ;
-    static constexpr unsigned tile_bytes = sizeof(C) * N * CC;   // one y/x-pass tile
-    // tile buffers of the y/x passes: HYOWON_FFT_NBUF deep where shared memory allows
-    static constexpr int nbuf = (HYOWON_FFT_NBUF * tile_bytes <= 200u * 1024u) ? HYOWON_FFT_NBUF : 2;
-    static constexpr size_t smem_c = static_cast<size_t>(nbuf) * tile_bytes;
     static constexpr int box = N < 256 ? N : 256;                 // TMA box rows
+    // column passes: a tile is N rows of CC columns, split into SP blocks of
+    // CB columns; each block keeps nbuf_b of its parts in shared memory
+    // (HYOWON_FFT_NBUF deep where shared memory allows)
+    static constexpr int SP = (LOG2N >= 8 && CC % HYOWON_FFT_SPLIT == 0) ? HYOWON_FFT_SPLIT : 1;
+    static constexpr int CB = CC / SP;
+    static constexpr int TCB = CB * N / 16;                       // threads of a column block
+    static constexpr unsigned tile_bytes_b = sizeof(C) * N * CB;  // one block's part of a tile
+    static constexpr int nbuf_b = (HYOWON_FFT_NBUF * tile_bytes_b <= 200u * 1024u) ? HYOWON_FFT_NBUF : 2;
+    static constexpr size_t smem_cb = static_cast<size_t>(nbuf_b) * tile_bytes_b;
+    static constexpr int units_b = CB * static_cast<int>(sizeof(C)) / 8;  // 8-byte units per part row
     static constexpr int units = CC * static_cast<int>(sizeof(C)) / 8;  // 8-byte units per row
 };
 
@@ -357,14 +369,16 @@ constexpr unsigned kWaitLimit = 1u << 24;
 // inverse transform (the x pass of the potential solve); 2: the symbol
 // `green` applied to the untransformed tile, then one transform (SIGN).
 template <typename T, int LOG2N, int AXIS, int SIGN, int MODE, typename GF>
-__global__ void __launch_bounds__(Geo<T, LOG2N>::TC, sizeof(T) == 4 ? HYOWON_FFT_MINB_C32 : HYOWON_FFT_MINB_C64)
+__global__ void __launch_bounds__(Geo<T, LOG2N>::TCB,
+                                  Geo<T, LOG2N>::SP * (sizeof(T) == 4 ? HYOWON_FFT_MINB_C32 : HYOWON_FFT_MINB_C64))
 k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
           const cx_t<T>* __restrict__ tw, GF green, unsigned int* status, unsigned wait_limit) {
     using G = Geo<T, LOG2N>;
     using C = cx_t<T>;
     constexpr int P = G::N / 16;
-    constexpr int S = G::CC;
-    constexpr int NB = G::nbuf;
+    constexpr int CB = G::CB;     // columns of this block's part of a tile
+    constexpr int S = CB;
+    constexpr int NB = G::nbuf_b;
     constexpr size_t axis_stride = AXIS == 1 ? static_cast<size_t>(G::CC)
                                              : static_cast<size_t>(G::N) * G::CC;
     constexpr size_t seq_stride = AXIS == 1 ? static_cast<size_t>(G::N) * G::CC
@@ -372,21 +386,25 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
     extern __shared__ __align__(1024) unsigned char smem_tiles[];
     __shared__ __align__(8) uint64_t full[NB];
     const int tid = threadIdx.x;
-    const int c = tid % G::CC;
-    const int j = tid / G::CC;
-    const unsigned tiles = static_cast<unsigned>(G::KC) * G::N;
-    auto tile_buf = [&](int b) { return reinterpret_cast<C*>(smem_tiles + b * G::tile_bytes); };
-    auto issue = [&](unsigned tile, int b) {
+    const int c = tid % CB;
+    const int j = tid / CB;
+    // work items: (tile, part) with tile = kc * N + seq and part the column block
+    const unsigned tiles = static_cast<unsigned>(G::KC) * G::N * G::SP;
+    auto tile_buf = [&](int b) { return reinterpret_cast<C*>(smem_tiles + b * G::tile_bytes_b); };
+    auto issue = [&](unsigned item, int b) {
+        const unsigned tile = item / G::SP;
+        const int part = static_cast<int>(item % G::SP);
         const int kc = static_cast<int>(tile / G::N);
         const int sq = static_cast<int>(tile % G::N);
         C* dst = tile_buf(b);
-        tma::mbar_arrive_expect_tx(&full[b], G::tile_bytes);
+        tma::mbar_arrive_expect_tx(&full[b], G::tile_bytes_b);
+        const int c0 = part * G::units_b;   // 8-byte units: a multiple of 16 bytes
 #pragma unroll
         for (int g = 0; g < G::N / G::box; ++g) {
             if (AXIS == 1)
-                tma::load_3d(dst + g * G::box * G::CC, &map, 0, g * G::box, kc * G::N + sq, &full[b]);
+                tma::load_3d(dst + g * G::box * CB, &map, c0, g * G::box, kc * G::N + sq, &full[b]);
             else
-                tma::load_3d(dst + g * G::box * G::CC, &map, 0, sq, kc * G::N + g * G::box, &full[b]);
+                tma::load_3d(dst + g * G::box * CB, &map, c0, sq, kc * G::N + g * G::box, &full[b]);
         }
     };
     if (tid == 0) {
@@ -427,9 +445,11 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
             return;
         }
         C* sm = tile_buf(b);
-        const int kc = static_cast<int>(t / G::N);
-        const int seq = static_cast<int>(t % G::N);
-        const int kz = kc * G::CC + c;
+        const unsigned tile = t / G::SP;
+        const int col = static_cast<int>(t % G::SP) * CB + c;   // column within the chunk
+        const int kc = static_cast<int>(tile / G::N);
+        const int seq = static_cast<int>(tile % G::N);
+        const int kz = kc * G::CC + col;
         C v[16];
         if constexpr (MODE == 2) {
             // element j + q P of column c, untransformed
@@ -441,10 +461,10 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
                     v[q] = AXIS == 0 ? green(j + q * P, seq, kz, v[q]) : green(seq, j + q * P, kz, v[q]);
             }
             __syncthreads();
-            fft::first_stage_to_smem<LOG2N, SIGN, G::CC, S>(v, sm, c, j);
-            fft::rest_to_registers<LOG2N, SIGN, G::CC, S>(sm, tw, G::N, c, j, v);
+            fft::first_stage_to_smem<LOG2N, SIGN, CB, S>(v, sm, c, j);
+            fft::rest_to_registers<LOG2N, SIGN, CB, S>(sm, tw, G::N, c, j, v);
         } else {
-            fft::smem_to_registers<LOG2N, SIGN, G::CC, S>(sm, tw, G::N, c, j, v);
+            fft::smem_to_registers<LOG2N, SIGN, CB, S>(sm, tw, G::N, c, j, v);
         }
         if constexpr (MODE == 1) {
             if (kz < G::Hz) {
@@ -453,11 +473,11 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
                     v[q] = AXIS == 0 ? green(j + q * P, seq, kz, v[q]) : green(seq, j + q * P, kz, v[q]);
             }
             __syncthreads();
-            fft::first_stage_to_smem<LOG2N, -SIGN, G::CC, S>(v, sm, c, j);
-            fft::rest_to_registers<LOG2N, -SIGN, G::CC, S>(sm, tw, G::N, c, j, v);
+            fft::first_stage_to_smem<LOG2N, -SIGN, CB, S>(v, sm, c, j);
+            fft::rest_to_registers<LOG2N, -SIGN, CB, S>(sm, tw, G::N, c, j, v);
         }
         if (kz < G::Hz) {
-            C* dst = H + static_cast<size_t>(kc) * G::chunk + static_cast<size_t>(seq) * seq_stride + c;
+            C* dst = H + static_cast<size_t>(kc) * G::chunk + static_cast<size_t>(seq) * seq_stride + col;
 #pragma unroll
             for (int q = 0; q < 16; ++q) __stcs(&dst[static_cast<size_t>(j + q * P) * axis_stride], v[q]);
         }
@@ -532,17 +552,17 @@ int columns(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF green, unsigned int
     using G = Geo<T, LOG2N>;
     if (!p || p->N != G::N) return -1;
     auto kernel = k_columns<T, LOG2N, AXIS, SIGN, MODE, GF>;
-    if (!prepare(kernel, G::smem_c)) return -1;
+    if (!prepare(kernel, G::smem_cb)) return -1;
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess
         || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess
-        || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, G::TC, G::smem_c) != cudaSuccess
+        || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, G::TCB, G::smem_cb) != cudaSuccess
         || per_sm < 1)
         return -1;
-    const unsigned tiles = static_cast<unsigned>(G::KC) * G::N;
+    const unsigned tiles = static_cast<unsigned>(G::KC) * G::N * G::SP;
     const unsigned full = static_cast<unsigned>(sms) * static_cast<unsigned>(per_sm);
     const unsigned grid = tiles < full ? tiles : full;
-    kernel<<<grid, G::TC, G::smem_c, s>>>(AXIS == 1 ? p->y : p->x, H, tw, green, status,
+    kernel<<<grid, G::TCB, G::smem_cb, s>>>(AXIS == 1 ? p->y : p->x, H, tw, green, status,
                                           p->wait_limit);
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
@@ -576,8 +596,8 @@ bool encode_maps(Plan* p, void* modes) {
     const cuuint64_t strides[2] = {static_cast<cuuint64_t>(G::units) * 8,
                                    static_cast<cuuint64_t>(G::units) * 8 * G::N};
     const cuuint32_t estr[3] = {1, 1, 1};
-    const cuuint32_t box_y[3] = {static_cast<cuuint32_t>(G::units), static_cast<cuuint32_t>(G::box), 1};
-    const cuuint32_t box_x[3] = {static_cast<cuuint32_t>(G::units), 1, static_cast<cuuint32_t>(G::box)};
+    const cuuint32_t box_y[3] = {static_cast<cuuint32_t>(G::units_b), static_cast<cuuint32_t>(G::box), 1};
+    const cuuint32_t box_x[3] = {static_cast<cuuint32_t>(G::units_b), 1, static_cast<cuuint32_t>(G::box)};
     return enc(&p->y, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, modes, dims, strides, box_y, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS

@@ -335,8 +335,11 @@ struct WalkParams {
 // Targets: sorted slots tslot[t] (null: target t is sorted slot t, every
 // source). Output of target t goes to index out_idx[t] (null: t), written, or
 // added to what is there when `add`. Source masses: sorted sm[] (null: P.m).
+#ifndef HYOWON_WALK_MINB
+#define HYOWON_WALK_MINB 1
+#endif
 template <typename R>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, HYOWON_WALK_MINB)
 k_walk(uint32_t n_targets, const uint32_t* __restrict__ tslot, const double* __restrict__ sx,
        const double* __restrict__ sy, const double* __restrict__ sz,
        const double* __restrict__ sm, const unsigned long long* __restrict__ skey,
