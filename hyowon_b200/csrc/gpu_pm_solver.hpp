@@ -15,7 +15,9 @@
 // Link with libhyowon_pm.so.
 #pragma once
 
+#include "hyowon_adjoint.h"
 #include "hyowon_pm.h"
+#include "hyowon_treepm.h"
 
 #include <cstdint>
 #include <new>
@@ -188,6 +190,37 @@ public:
         std::vector<double> drift(K1.size());
         check(hyowon_pm_run(h_, K1.size(), K1.data(), D.data(), K2.data(), drift.data()));
         return drift;
+    }
+
+    // TreePMSolver::compute_forces as the force of every later solve
+    // (src/gravity/treepm_solver.cpp:631-717): the long range of a
+    // Method::TreePMLongRange solver plus the octree short range; cutoff 0
+    // returns to the long range alone. hyowon_pm_set_treepm_short_range.
+    void set_treepm_short_range(double theta, double softening, double cutoff) {
+        check(hyowon_pm_set_treepm_short_range(h_, theta, softening, cutoff));
+    }
+
+    // Short-range accelerations of the device state in particle order (spans of
+    // the particle count, or empty to skip); stats as hyowon_treepm_short_forces.
+    void treepm_short_forces(double theta, double softening, double cutoff,
+                             std::span<double> ax, std::span<double> ay, std::span<double> az,
+                             std::span<double> stats = {}) {
+        if (!stats.empty() && stats.size() < 6)
+            throw std::invalid_argument("treepm_short_forces: stats needs 6 entries");
+        auto p = [](std::span<double> v) { return v.empty() ? nullptr : v.data(); };
+        check(hyowon_pm_treepm_short_forces(h_, theta, softening, cutoff, p(ax), p(ay), p(az),
+                                            p(stats)));
+    }
+
+    // Loss and d loss / d noise of the differentiable forward model on this
+    // solver's box, mesh and form (hyowon_pm_vjp); returns the loss.
+    double vjp(const hyowon_vjp_config& cfg, std::span<const double> noise,
+               std::span<const double> target_delta, std::span<double> grad_noise) {
+        double loss = 0.0;
+        check(hyowon_pm_vjp(h_, &cfg, noise.data(),
+                            target_delta.empty() ? nullptr : target_delta.data(), &loss,
+                            grad_noise.empty() ? nullptr : grad_noise.data(), nullptr, nullptr));
+        return loss;
     }
 
     std::uint64_t particle_count() const {

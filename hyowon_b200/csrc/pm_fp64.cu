@@ -213,15 +213,20 @@ constexpr int kTileThreads = 256;
 // W >= kOneWordMinW, a single 64-bit word per cell holds the sum of terms
 // quantised to q = rint(t 2^(W-1-e)): a quantum of 2^(e+1-W) <= 2^(e-54), below
 // half the binary64 spacing of a full-weight term (t < 2^e). Cell sums stay
-// below 2^63. Denser states use the exact two-word (hi/lo) sums. Both kernels
-// are launched; the one that does not apply returns at once, so the choice
-// needs no host synchronisation and depends only on the bucket counts.
+// below 2^63. Denser states use the exact two-word (hi/lo) sums. The host reads
+// the densest bucket count before the deposit and launches the form that
+// applies (the kernel checks the same condition on the device).
 constexpr int kOneWordMinW = 55;
 // Two words: a hi part is below 2^(62-W) <= c/2 for c = 8 max_bucket
 // contributors, so hi sums stay below c^2 / 2 < 2^64 while c < 2^32, i.e.
 // W >= 31 (a bucket of fewer than 2^29 particles); beyond that the deposit
 // reports ST_CAPACITY.
 constexpr int kTwoWordMinW = 31;
+// Particles each thread loads ahead per pass of the tile loop.
+#ifndef HYOWON_DEPOSIT64_BATCH
+#define HYOWON_DEPOSIT64_BATCH 2
+#endif
+constexpr int kDepositBatch = HYOWON_DEPOSIT64_BATCH;
 
 __device__ __forceinline__ int fixed_split_bits(const uint32_t* max_count) {
     const unsigned long long c = 8ull * (*max_count > 0u ? *max_count : 1u);
@@ -261,73 +266,88 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
     if ((kDepositWords == 1) != (W >= kOneWordMinW)) return;
     if (kDepositWords == 2 && W < kTwoWordMinW) {
         // more than 2^32 contributors per cell could overflow a hi sum
-        if (threadIdx.x == 0 && blockIdx.x == 0) raise_status(status, ST_CAPACITY);
+        if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0) raise_status(status, ST_CAPACITY);
         return;
     }
     const int N = a.N;
     const int tid = threadIdx.x;
-    // persistent blocks over the tiles (x0 major, row tiles of a plane
-    // consecutive), so the form that does not apply costs one short wave
-    const unsigned row_tiles = static_cast<unsigned>((N + TY - 1) / TY);
-    const unsigned n_tiles = row_tiles * static_cast<unsigned>(N);
-    for (unsigned tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        const int x0 = static_cast<int>(tile / row_tiles);
-        const int y0 = static_cast<int>(tile % row_tiles) * TY;
-        const int ty = N - y0 < TY ? N - y0 : TY;
-        const int halo = ty == N ? 0 : 1;
-        const int tcells = ty * N;
-        unsigned long long* acc_lo = acc;
-        unsigned long long* acc_hi = acc + (kDepositWords == 2 ? static_cast<size_t>(TY) * N : 0);
-        if (tid == 0) {
-            int ns = 0;
-            for (int own = 1; own >= 0; --own) {
-                const int p = own ? x0 : (x0 == 0 ? N - 1 : x0 - 1);
-                int lo[2], hi[2], nr = 0;
-                if (halo && y0 == 0) {
-                    lo[nr] = N - 1; hi[nr++] = N - 1;
-                    lo[nr] = 0; hi[nr++] = ty - 1;
-                } else {
-                    lo[nr] = y0 - halo; hi[nr++] = y0 + ty - 1;
-                }
-                for (int k = 0; k < nr; ++k) {
-                    const uint64_t c_lo = (static_cast<uint64_t>(p) * N + lo[k]) * N;
-                    const uint64_t c_hi = (static_cast<uint64_t>(p) * N + hi[k]) * N + (N - 1);
-                    const uint32_t b0 = offset[c_lo >> shift];
-                    const uint32_t b1 = offset[(c_hi >> shift) + 1];
-                    seg_p0[ns] = b0;
-                    seg_len[ns] = b1 - b0;
-                    seg_plane[ns] = p;
-                    seg_row_lo[ns] = lo[k];
-                    seg_row_hi[ns] = hi[k];
-                    seg_own[ns] = own;
-                    ++ns;
+    const int x0 = blockIdx.y;
+    const int y0 = blockIdx.x * TY;
+    const int ty = N - y0 < TY ? N - y0 : TY;
+    const int halo = ty == N ? 0 : 1;
+    const int tcells = ty * N;
+    unsigned long long* acc_lo = acc;
+    unsigned long long* acc_hi = acc + (kDepositWords == 2 ? static_cast<size_t>(TY) * N : 0);
+    if (tid == 0) {
+        int ns = 0;
+        for (int own = 1; own >= 0; --own) {
+            const int p = own ? x0 : (x0 == 0 ? N - 1 : x0 - 1);
+            int lo[2], hi[2], nr = 0;
+            if (halo && y0 == 0) {
+                lo[nr] = N - 1; hi[nr++] = N - 1;
+                lo[nr] = 0; hi[nr++] = ty - 1;
+            } else {
+                lo[nr] = y0 - halo; hi[nr++] = y0 + ty - 1;
+            }
+            for (int k = 0; k < nr; ++k) {
+                const uint64_t c_lo = (static_cast<uint64_t>(p) * N + lo[k]) * N;
+                const uint64_t c_hi = (static_cast<uint64_t>(p) * N + hi[k]) * N + (N - 1);
+                const uint32_t b0 = offset[c_lo >> shift];
+                const uint32_t b1 = offset[(c_hi >> shift) + 1];
+                seg_p0[ns] = b0;
+                seg_len[ns] = b1 - b0;
+                seg_plane[ns] = p;
+                seg_row_lo[ns] = lo[k];
+                seg_row_hi[ns] = hi[k];
+                seg_own[ns] = own;
+                ++ns;
+            }
+        }
+        seg_n = ns;
+    }
+    for (int e = tid; e < tcells; e += kTileThreads) {
+        acc_lo[e] = 0ull;
+        if (kDepositWords == 2) acc_hi[e] = 0ull;
+    }
+    __syncthreads();
+    const unsigned long long lo_mask = (1ull << W) - 1ull;
+    // 2^(62 - e_max) (one word: 2^(W-1-e_max)): a multiplication by it is
+    // exact (the product is at most 2^62, and below 2^-1022 it rounds to the
+    // integer 0 either way)
+    const double to_fixed = ldexp(1.0, kDepositWords == 2 ? 62 - e_max : W - 1 - e_max);
+    const int ns = seg_n;
+    for (int g = 0; g < ns; ++g) {
+        const uint32_t p0 = seg_p0[g];
+        const uint32_t len = seg_len[g];
+        const int plane = seg_plane[g];
+        const int row_lo = seg_row_lo[g], row_hi = seg_row_hi[g];
+        const bool own = seg_own[g] != 0;
+        // kDepositBatch particles per thread and pass: their index and
+        // position loads are all issued before the first is used
+        for (uint32_t v0 = tid; v0 < len; v0 += kDepositBatch * kTileThreads) {
+            uint32_t idx[kDepositBatch];
+#pragma unroll
+            for (int k = 0; k < kDepositBatch; ++k) {
+                const uint32_t v = v0 + k * kTileThreads;
+                idx[k] = v < len ? (order ? order[p0 + v] : p0 + v) : 0xffffffffu;
+            }
+            double px[kDepositBatch], py[kDepositBatch], pz[kDepositBatch];
+#pragma unroll
+            for (int k = 0; k < kDepositBatch; ++k) {
+                if (idx[k] != 0xffffffffu) {
+                    px[k] = x[idx[k]];
+                    py[k] = y[idx[k]];
+                    pz[k] = z[idx[k]];
                 }
             }
-            seg_n = ns;
-        }
-        for (int e = tid; e < tcells; e += kTileThreads) {
-            acc_lo[e] = 0ull;
-            if (kDepositWords == 2) acc_hi[e] = 0ull;
-        }
-        __syncthreads();
-        const unsigned long long lo_mask = (1ull << W) - 1ull;
-        // 2^(62 - e_max) (one word: 2^(W-1-e_max)): a multiplication by it is
-        // exact (the product is at most 2^62, and below 2^-1022 it rounds to the
-        // integer 0 either way)
-        const double to_fixed = ldexp(1.0, kDepositWords == 2 ? 62 - e_max : W - 1 - e_max);
-        const int ns = seg_n;
-        for (int g = 0; g < ns; ++g) {
-            const uint32_t p0 = seg_p0[g];
-            const uint32_t len = seg_len[g];
-            const int plane = seg_plane[g];
-            const int row_lo = seg_row_lo[g], row_hi = seg_row_hi[g];
-            const bool own = seg_own[g] != 0;
-            for (uint32_t v = tid; v < len; v += kTileThreads) {
-                const uint32_t i = order ? order[p0 + v] : p0 + v;
+#pragma unroll
+            for (int k = 0; k < kDepositBatch; ++k) {
+                if (idx[k] == 0xffffffffu) continue;
+                const uint32_t i = idx[k];
                 int ix, iy, iz;
                 double tx, ty_, tz;
-                if (!(cic_coord_f64(x[i], a, ix, tx) & cic_coord_f64(y[i], a, iy, ty_)
-                      & cic_coord_f64(z[i], a, iz, tz)))
+                if (!(cic_coord_f64(px[k], a, ix, tx) & cic_coord_f64(py[k], a, iy, ty_)
+                      & cic_coord_f64(pz[k], a, iz, tz)))
                     continue;   // never in cell order: the key pass raised the status
                 if (ix != plane || iy < row_lo || iy > row_hi) continue;
                 const double m = mass ? mass[i] : uniform_mass;
@@ -335,7 +355,7 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
                 const double wy[2] = {1.0 - ty_, ty_};
                 const double wz[2] = {1.0 - tz, tz};
                 const int gz[2] = {iz, iz + 1 == N ? 0 : iz + 1};
-    #pragma unroll
+#pragma unroll
                 for (int oy = 0; oy < 2; ++oy) {
                     const int row = iy + oy == N ? 0 : iy + oy;
                     const int ly = row - y0;
@@ -343,10 +363,10 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
                     const double mxy = mx * wy[oy];
                     unsigned long long* rlo = acc_lo + ly * N;
                     unsigned long long* rhi = acc_hi + ly * N;
-    #pragma unroll
+#pragma unroll
                     for (int oz = 0; oz < 2; ++oz) {
-                        const unsigned long long q =
-                            static_cast<unsigned long long>(__double2ll_rn(mxy * wz[oz] * to_fixed));
+                        const unsigned long long q = static_cast<unsigned long long>(
+                            __double2ll_rn(mxy * wz[oz] * to_fixed));
                         if (q == 0ull) continue;
                         if (kDepositWords == 1) {
                             atomicAdd(rlo + gz[oz], q);
@@ -359,18 +379,17 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
                 }
             }
         }
-        __syncthreads();
-        double* out = mesh + (static_cast<uint64_t>(x0) * N + y0) * N;
-        if (kDepositWords == 1) {
-            const double from_fixed = ldexp(1.0, e_max + 1 - W);
-            for (int e = tid; e < tcells; e += kTileThreads)
-                out[e] = __ull2double_rn(acc_lo[e]) * from_fixed;
-        } else {
-            const double from_fixed = ldexp(1.0, e_max - 62);
-            for (int e = tid; e < tcells; e += kTileThreads)
-                out[e] = fixed_to_double(acc_hi[e], acc_lo[e], W) * from_fixed;
-        }
-        __syncthreads();   // the next tile reuses the accumulators and segment table
+    }
+    __syncthreads();
+    double* out = mesh + (static_cast<uint64_t>(x0) * N + y0) * N;
+    if (kDepositWords == 1) {
+        const double from_fixed = ldexp(1.0, e_max + 1 - W);
+        for (int e = tid; e < tcells; e += kTileThreads)
+            out[e] = __ull2double_rn(acc_lo[e]) * from_fixed;
+    } else {
+        const double from_fixed = ldexp(1.0, e_max - 62);
+        for (int e = tid; e < tcells; e += kTileThreads)
+            out[e] = fixed_to_double(acc_hi[e], acc_lo[e], W) * from_fixed;
     }
 }
 
@@ -824,15 +843,7 @@ cudaError_t launch_tiles(const ParticlesF64& p, const double* mass, double unifo
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0, per_sm = 0;
-    if ((e = cudaGetDevice(&dev)) != cudaSuccess
-        || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess
-        || (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deposit_tiles<WORDS>,
-                                                               kTileThreads, smem)) != cudaSuccess)
-        return e;
-    const uint64_t n_tiles = static_cast<uint64_t>((N + TY - 1) / TY) * static_cast<uint64_t>(N);
-    const uint64_t full = static_cast<uint64_t>(sms) * static_cast<uint64_t>(per_sm > 0 ? per_sm : 1);
-    const unsigned grid = static_cast<unsigned>(n_tiles < full ? n_tiles : full);
+    const dim3 grid(static_cast<unsigned>((N + TY - 1) / TY), static_cast<unsigned>(N));
     k_deposit_tiles<WORDS><<<grid, kTileThreads, smem, s>>>(p.x, p.y, p.z, mass, uniform_mass,
                                                             order, w.offset, w.shift, a, TY,
                                                             max_count, e_max, mesh, status);
@@ -842,11 +853,15 @@ cudaError_t launch_tiles(const ParticlesF64& p, const double* mass, double unifo
 cudaError_t launch_deposit_tiles_f64(const ParticlesF64& p, const double* mass,
                                      double uniform_mass, const uint32_t* order,
                                      const SortWork& w, Axis a, const uint32_t* max_count,
-                                     int e_max, double* mesh, unsigned int* status,
-                                     cudaStream_t s) {
-    cudaError_t e = launch_tiles<1>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh,
-                                    status, s);
-    if (e != cudaSuccess) return e;
+                                     uint32_t max_count_host, int e_max, double* mesh,
+                                     unsigned int* status, cudaStream_t s) {
+    // the same W the kernels derive from *max_count (they check it again)
+    const unsigned long long c = 8ull * (max_count_host > 0u ? max_count_host : 1u);
+    int lg = 0;
+    while ((c >> (lg + 1)) != 0ull) ++lg;
+    const int W = 63 - lg;
+    if (W >= kOneWordMinW)
+        return launch_tiles<1>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh, status, s);
     return launch_tiles<2>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh, status, s);
 }
 

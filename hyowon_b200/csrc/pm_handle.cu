@@ -121,6 +121,7 @@ struct hyowon_pm_s {
     unsigned long long* d_maxdrift = nullptr;
     double* d_diag = nullptr;                   // diagnostics scratch (pm_diag.h)
     unsigned int* h_status = nullptr;           // pinned
+    uint32_t* h_max_count = nullptr;            // pinned
     unsigned long long* h_maxdrift = nullptr;   // pinned
 
     fp32::State* f32 = nullptr;  // precision form (pm_fp32.cu)
@@ -302,6 +303,16 @@ int read_status(hyowon_pm_t h, unsigned int* st) {
     return HYOWON_OK;
 }
 
+// The densest bucket count of the last keying (it picks the deposit form);
+// waits for the work before it.
+int read_max_count(hyowon_pm_t h, uint32_t* out) {
+    CK(cudaMemcpyAsync(h->h_max_count, h->d_max_count, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *out = *h->h_max_count;
+    return HYOWON_OK;
+}
+
 // Permutes the current particle state into bucket order (used after upload).
 int sort_current(hyowon_pm_t h) {
     const uint32_t n = h->n;
@@ -388,10 +399,13 @@ int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2,
     }
     const ParticlesF64 p = set_view(h, pset, mset);
     (void)cells;
+    uint32_t max_count = 0;
+    int rc0 = read_max_count(h, &max_count);
+    if (rc0) return rc0;
     record(h, 1);
-    h->launches += 2;   // the one-word and two-word tile kernels (one returns at once)
+    ++h->launches;
     CK(launch_deposit_tiles_f64(p, h->has_masses ? h->mass[h->ic] : nullptr, h->uniform_mass,
-                                order, h->sort, h->axis, h->d_max_count,
+                                order, h->sort, h->axis, h->d_max_count, max_count,
                                 deposit_mass_exponent_f64(h->max_mass), h->mesh, h->d_status,
                                 h->stream));
     record(h, 2);
@@ -759,6 +773,7 @@ int hyowon_pm_create(double box_size, uint64_t mesh_size, int method, int deconv
     }
     if (cudaMallocHost(reinterpret_cast<void**>(&h->h_status), sizeof(unsigned int)) != cudaSuccess
         || cudaMallocHost(reinterpret_cast<void**>(&h->h_maxdrift), sizeof(unsigned long long)) != cudaSuccess
+        || cudaMallocHost(reinterpret_cast<void**>(&h->h_max_count), sizeof(uint32_t)) != cudaSuccess
         || dalloc(&h->d_status, 1) != cudaSuccess || dalloc(&h->d_maxdrift, 1) != cudaSuccess
         || dalloc(&h->d_max_count, 1) != cudaSuccess
         || dalloc(&h->d_diag, diag::scratch_doubles()) != cudaSuccess)
@@ -879,6 +894,7 @@ int hyowon_pm_destroy(hyowon_pm_t h) {
     cudaFree(h->d_max_count);
     cudaFree(h->d_diag);
     if (h->h_status) cudaFreeHost(h->h_status);
+    if (h->h_max_count) cudaFreeHost(h->h_max_count);
     if (h->h_maxdrift) cudaFreeHost(h->h_maxdrift);
     for (auto& e : h->ev) {
         if (e) cudaEventDestroy(e);
@@ -1360,11 +1376,14 @@ int hyowon_pm_download_mass_mesh(hyowon_pm_t h, double* mesh) {
         if (rc) return rc;
     }
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned int), h->stream));
-    h->launches += 2;
+    uint32_t max_count = 0;
+    int rc0 = read_max_count(h, &max_count);
+    if (rc0) return rc0;
+    ++h->launches;
     CK(launch_deposit_tiles_f64(set_view(h, h->pc, h->mc), h->has_masses ? h->mass[h->ic] : nullptr,
                                 h->uniform_mass, current_order(h), h->sort, h->axis,
-                                h->d_max_count, deposit_mass_exponent_f64(h->max_mass), h->mesh,
-                                h->d_status, h->stream));
+                                h->d_max_count, max_count, deposit_mass_exponent_f64(h->max_mass),
+                                h->mesh, h->d_status, h->stream));
     unsigned int st = 0;
     int rc = read_status(h, &st);
     if (rc) return rc;

@@ -71,13 +71,14 @@ void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,
 // Deterministic owner-computes deposit (k_deposit_tiles): mesh written whole,
 // no zeroing needed. Needs the bucket offsets of the deposited set in w, the
 // cell order `order` (or null when the arrays are in cell order), the largest
-// bucket count in *max_count and e_max = deposit_mass_exponent_f64(max mass).
+// bucket count in *max_count (and its value on the host, which picks the
+// kernel) and e_max = deposit_mass_exponent_f64(max mass).
 int deposit_mass_exponent_f64(double max_mass);
 cudaError_t launch_deposit_tiles_f64(const ParticlesF64& p, const double* mass,
                                      double uniform_mass, const uint32_t* order,
                                      const SortWork& w, Axis a, const uint32_t* max_count,
-                                     int e_max, double* mesh, unsigned int* status,
-                                     cudaStream_t s);
+                                     uint32_t max_count_host, int e_max, double* mesh,
+                                     unsigned int* status, cudaStream_t s);
 void launch_max_count_f64(uint32_t n_buckets, const uint32_t* count, uint32_t* max_count,
                           cudaStream_t s);
 void launch_green_f64(int N, double2* modes, const double* lap, const double* win,
