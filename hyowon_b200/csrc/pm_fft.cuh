@@ -139,61 +139,91 @@ template <int LOG2L> struct Plan {
     static_assert(LOG2L >= 4, "transform length must be at least 16");
 };
 
-// One shared-memory stage of radix R (R <= 16) on C interleaved sequences of
-// length L: each thread does 16/R butterflies (groups j + P b). The caller has
-// synchronised since the last writes to sm; the stage ends synchronised.
-template <int LOG2L, int R, int SIGN, int C, int S, typename Cplx>
+// Row order of the first stage's output in the dense column tiles: row rho is
+// kept at rho ^ ((rho >> 4) & 1). A radix-16 first stage writes rows 16 j + r
+// for the lanes' consecutive j, which all fall in the same half of a 128-byte
+// bank row when a row is 64 bytes (CC columns); swapping row pairs in every
+// other group of 16 rows spreads them over both halves (4- and 8-way bank
+// conflicts become none), while the next stage's reads of consecutive rows
+// stay consecutive. Every access to that stage's output applies it (PIN /
+// POUT below); other layouts are untouched.
+#ifndef HYOWON_FFT_ROWPERM
+#define HYOWON_FFT_ROWPERM 1
+#endif
+template <bool PERMUTED>
+__device__ __forceinline__ int row_at(int row) {
+    return (PERMUTED && HYOWON_FFT_ROWPERM) ? (row ^ ((row >> 4) & 1)) : row;
+}
+
+// One shared-memory stage of radix R (R <= E) on C interleaved sequences of
+// length L, E elements per thread: each thread does E/R butterflies (groups
+// j + P b, P = L/E). The caller has synchronised since the last writes to sm;
+// the stage ends synchronised. Threads with `active` false only take part in
+// the barriers.
+template <int LOG2L, int R, int SIGN, int C, int S, int E = 16, bool PIN = false, bool POUT = false,
+          typename Cplx>
 __device__ __forceinline__ void smem_stage(Cplx* sm, int Ns, const Cplx* __restrict__ tw, int NT,
-                                           int c, int j) {
+                                           int c, int j, bool active = true) {
     constexpr int L = 1 << LOG2L;
-    constexpr int P = L / 16;
-    constexpr int NB = 16 / R;
+    constexpr int P = L / E;
+    constexpr int NB = E / R;
     Cplx v[NB][R];
+    if (active) {
 #pragma unroll
-    for (int b = 0; b < NB; ++b) {
-        const int jb = j + P * b;
+        for (int b = 0; b < NB; ++b) {
+            const int jb = j + P * b;
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[b][r] = sm[(jb + r * (L / R)) * S + c];
+            for (int r = 0; r < R; ++r) v[b][r] = sm[row_at<PIN>(jb + r * (L / R)) * S + c];
+        }
     }
     __syncthreads();
+    if (active) {
 #pragma unroll
-    for (int b = 0; b < NB; ++b) {
-        const int jb = j + P * b;
-        const int k = jb & (Ns - 1);
-        twiddle<R, SIGN>(v[b], k, Ns, tw, NT);
-        dft<R, SIGN>(v[b]);
-        const int base = (jb - k) * R + k;
+        for (int b = 0; b < NB; ++b) {
+            const int jb = j + P * b;
+            const int k = jb & (Ns - 1);
+            twiddle<R, SIGN>(v[b], k, Ns, tw, NT);
+            dft<R, SIGN>(v[b]);
+            const int base = (jb - k) * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) sm[(base + r * Ns) * S + c] = v[b][r];
+            for (int r = 0; r < R; ++r) sm[row_at<POUT>(base + r * Ns) * S + c] = v[b][r];
+        }
     }
     __syncthreads();
 }
 
-// Whole transform in shared memory (natural order in and out).
-template <int LOG2L, int SIGN, int C, int S, typename Cplx>
-__device__ __forceinline__ void smem_fft(Cplx* sm, const Cplx* __restrict__ tw, int NT, int c, int j) {
-    using PL = Plan<LOG2L>;
+// Whole transform in shared memory (natural order in and out): radix-E
+// stages, then one stage of the remaining radix, E (8 or 16) elements per
+// thread, thread (c, j) for j < L/E.
+template <int LOG2L, int SIGN, int C, int S, int E = 16, typename Cplx>
+__device__ __forceinline__ void smem_fft(Cplx* sm, const Cplx* __restrict__ tw, int NT, int c, int j,
+                                         bool active = true) {
+    constexpr int LE = ilog2<E>();
+    constexpr int nE = LOG2L / LE;
+    constexpr int rem = LOG2L % LE;
+    static_assert(LOG2L >= LE, "transform shorter than the elements per thread");
     int Ns = 1;
 #pragma unroll 1
-    for (int s = 0; s < PL::n16; ++s) {
-        smem_stage<LOG2L, 16, SIGN, C, S>(sm, Ns, tw, NT, c, j);
-        Ns *= 16;
+    for (int s = 0; s < nE; ++s) {
+        smem_stage<LOG2L, E, SIGN, C, S, E>(sm, Ns, tw, NT, c, j, active);
+        Ns *= E;
     }
-    if constexpr (PL::rem != 0) smem_stage<LOG2L, PL::RF, SIGN, C, S>(sm, Ns, tw, NT, c, j);
+    if constexpr (rem != 0) smem_stage<LOG2L, (1 << rem), SIGN, C, S, E>(sm, Ns, tw, NT, c, j, active);
 }
 
 // First stage (radix 16, no twiddles) from 16 values already in registers,
-// v[r] = element j + r P, written to shared memory.
+// v[r] = element j + r P, written to shared memory in the permuted row order
+// (row_at) that rest_to_registers reads.
 template <int LOG2L, int SIGN, int C, int S, typename Cplx>
 __device__ __forceinline__ void first_stage_to_smem(Cplx (&v)[16], Cplx* sm, int c, int j) {
     dft<16, SIGN>(v);
 #pragma unroll
-    for (int r = 0; r < 16; ++r) sm[(j * 16 + r) * S + c] = v[r];
+    for (int r = 0; r < 16; ++r) sm[row_at<true>(j * 16 + r) * S + c] = v[r];
 }
 
 // The last stage (stride Ns = L / RF), read from shared memory and returned in
 // registers: out[q] = element j + q P of the transform (q < 16).
-template <int LOG2L, int SIGN, int C, int S, typename Cplx>
+template <int LOG2L, int SIGN, int C, int S, bool PIN = false, typename Cplx>
 __device__ __forceinline__ void final_to_registers(const Cplx* sm, int Ns, const Cplx* __restrict__ tw,
                                                    int NT, int c, int j, Cplx (&out)[16]) {
     using PL = Plan<LOG2L>;
@@ -206,7 +236,7 @@ __device__ __forceinline__ void final_to_registers(const Cplx* sm, int Ns, const
     for (int b = 0; b < NB; ++b) {
         const int jb = j + P * b;
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[b][r] = sm[(jb + r * (L / R)) * S + c];
+        for (int r = 0; r < R; ++r) v[b][r] = sm[row_at<PIN>(jb + r * (L / R)) * S + c];
     }
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
@@ -228,14 +258,21 @@ __device__ __forceinline__ void rest_to_registers(Cplx* sm, const Cplx* __restri
     int Ns = 16;
     // the first stage's shared-memory writes must land before anyone reads
     __syncthreads();
-    // radix-16 stages after the first, except a final radix-16 one
+    // radix-16 stages after the first, except a final radix-16 one; the
+    // first of them reads the first stage's permuted rows
     constexpr int mid = PL::rem ? PL::n16 - 1 : PL::n16 - 2;
-#pragma unroll 1
-    for (int s = 0; s < mid; ++s) {
-        smem_stage<LOG2L, 16, SIGN, C, S>(sm, Ns, tw, NT, c, j);
+    if constexpr (mid >= 1) {
+        smem_stage<LOG2L, 16, SIGN, C, S, 16, true, false>(sm, Ns, tw, NT, c, j);
         Ns *= 16;
+#pragma unroll 1
+        for (int s = 1; s < mid; ++s) {
+            smem_stage<LOG2L, 16, SIGN, C, S>(sm, Ns, tw, NT, c, j);
+            Ns *= 16;
+        }
+        final_to_registers<LOG2L, SIGN, C, S>(sm, Ns, tw, NT, c, j, out);
+    } else {
+        final_to_registers<LOG2L, SIGN, C, S, true>(sm, Ns, tw, NT, c, j, out);
     }
-    final_to_registers<LOG2L, SIGN, C, S>(sm, Ns, tw, NT, c, j, out);
 }
 
 // Whole transform from natural order in shared memory (the caller has
@@ -245,14 +282,27 @@ __device__ __forceinline__ void smem_to_registers(Cplx* sm, const Cplx* __restri
                                                   int j, Cplx (&out)[16]) {
     using PL = Plan<LOG2L>;
     int Ns = 1;
-    // every radix-16 stage but a final radix-16 one
+    // every radix-16 stage but a final radix-16 one; the first writes its rows
+    // permuted (row_at) and the stage after it reads them so
     constexpr int n = PL::rem ? PL::n16 : PL::n16 - 1;
+    if constexpr (n == 0) {
+        final_to_registers<LOG2L, SIGN, C, S>(sm, Ns, tw, NT, c, j, out);
+    } else {
+        smem_stage<LOG2L, 16, SIGN, C, S, 16, false, true>(sm, Ns, tw, NT, c, j);
+        Ns = 16;
+        if constexpr (n >= 2) {
+            smem_stage<LOG2L, 16, SIGN, C, S, 16, true, false>(sm, Ns, tw, NT, c, j);
+            Ns = 256;
 #pragma unroll 1
-    for (int s = 0; s < n; ++s) {
-        smem_stage<LOG2L, 16, SIGN, C, S>(sm, Ns, tw, NT, c, j);
-        Ns *= 16;
+            for (int s = 2; s < n; ++s) {
+                smem_stage<LOG2L, 16, SIGN, C, S>(sm, Ns, tw, NT, c, j);
+                Ns *= 16;
+            }
+            final_to_registers<LOG2L, SIGN, C, S>(sm, Ns, tw, NT, c, j, out);
+        } else {
+            final_to_registers<LOG2L, SIGN, C, S, true>(sm, Ns, tw, NT, c, j, out);
+        }
     }
-    final_to_registers<LOG2L, SIGN, C, S>(sm, Ns, tw, NT, c, j, out);
 }
 
 // Asynchronous global -> shared copies (cp.async) of BYTES = 8 or 16 bytes;

@@ -30,6 +30,7 @@
 #include "hyowon_pm.h"
 #include "pm_diag.h"
 #include "pm_fp32.h"
+#include "pm_chunk.cuh"
 #include "pm_poisson.h"
 #include "pm_kernels.h"
 
@@ -270,10 +271,9 @@ __device__ __forceinline__ void shared_add_u64(unsigned long long* a, unsigned l
 #ifndef HYOWON_DEPOSIT_TILE_CELLS
 #define HYOWON_DEPOSIT_TILE_CELLS 4096
 #endif
-inline int deposit_rows(int N) {
-    int ty = HYOWON_DEPOSIT_TILE_CELLS / N;
-    if (ty < 1) ty = 1;
-    return ty > N ? N : ty;
+__host__ __device__ constexpr int deposit_rows(int N) {
+    return HYOWON_DEPOSIT_TILE_CELLS / N < 1 ? 1
+         : (HYOWON_DEPOSIT_TILE_CELLS / N > N ? N : HYOWON_DEPOSIT_TILE_CELLS / N);
 }
 
 #ifndef HYOWON_DEPOSIT_MINB
@@ -284,13 +284,19 @@ inline int deposit_rows(int N) {
 #else
 #define HYOWON_DEPOSIT_BOUNDS __launch_bounds__(kDepositThreads)
 #endif
-template <typename OUT>
+//
+// ZLOG > 0 (N = 2^ZLOG, a power-of-two mesh of the five-pass solve): instead of
+// the real cells the tile's rows are transformed along z in shared memory
+// (chunked::rows_r2c) and stored to the chunked half spectrum H, the first
+// pass of the potential solve done while the tile is on chip.
+template <typename OUT, int ZLOG>
 __global__ void HYOWON_DEPOSIT_BOUNDS
 k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy,
                 const uint32_t* __restrict__ uz, const uint32_t* __restrict__ order,
                 const uint32_t* __restrict__ offset, int shift, int N, int TY,
                 const FixedPlan* plan, OUT* __restrict__ out, unsigned long long* qsum,
-                const unsigned int* status) {
+                const unsigned int* status, float2* __restrict__ H,
+                const float2* __restrict__ tw) {
     extern __shared__ __align__(16) unsigned long long qtile[];
     __shared__ uint32_t seg_p0[4], seg_len[4];
     __shared__ int seg_plane[4], seg_row_lo[4], seg_row_hi[4], seg_xr[4];
@@ -400,6 +406,41 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
     }
     __syncthreads();
     const long long mean = plan->mean_q;
+    if constexpr (ZLOG > 0) {
+        // N = 2^ZLOG and TY = deposit_rows(N) divides N, so ty == TY here
+        using Lz = chunked::Layout<float, ZLOG>;
+        constexpr int TYc = deposit_rows(Lz::N);
+        constexpr int S = TYc + 1;
+        constexpr int PAIRS = TYc * Lz::M;   // cell pairs of the tile
+        constexpr int PT = (PAIRS + kDepositThreads - 1) / kDepositThreads;
+        const ulonglong2* q2 = reinterpret_cast<const ulonglong2*>(qtile);
+        float2 v[PT];
+        unsigned long long local = 0;
+#pragma unroll
+        for (int i = 0; i < PT; ++i) {
+            const int e = tid + i * kDepositThreads;
+            if (e < PAIRS) {
+                const ulonglong2 q = q2[e];
+                const long long a0 = static_cast<long long>(q.x) - mean;
+                const long long a1 = static_cast<long long>(q.y) - mean;
+                local += static_cast<unsigned long long>(a0) + static_cast<unsigned long long>(a1);
+                v[i] = make_float2(__ll2float_rn(a0), __ll2float_rn(a1));
+            }
+        }
+        if (qsum) block_sum_to(local, qsum);
+        __syncthreads();
+        // the accumulators are consumed: reuse their shared memory as rows of
+        // packed complex values, sm[k S + r] = (cell 2k, cell 2k+1) of row r
+        float2* sm = reinterpret_cast<float2*>(qtile);
+#pragma unroll
+        for (int i = 0; i < PT; ++i) {
+            const int e = tid + i * kDepositThreads;
+            if (e < PAIRS) sm[(e % Lz::M) * S + e / Lz::M] = v[i];
+        }
+        __syncthreads();
+        chunked::rows_r2c<float, ZLOG, TYc, S, 8>(sm, tw, H, x0, y0, tid, kDepositThreads);
+        return;
+    }
     OUT* o = out + (static_cast<uint64_t>(x0) * N + y0) * N;
     unsigned long long local = 0;
     if ((tcells & 1) == 0 && (N & 1) == 0) {
@@ -1006,22 +1047,44 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
                        cudaEvent_t* ev, int P, int M, const uint32_t* order);
 
 // Owner-computes deposit of position set P into `out` (FP32 offsets for the
-// transform, or exact int64), see k_deposit_tiles.
-template <typename OUT>
+// transform, or exact int64), see k_deposit_tiles. With ZLOG > 0 the tiles go
+// to the chunked half spectrum `H` transformed along z instead.
+template <typename OUT, int ZLOG = 0>
 int deposit_tiles(State* st, int P, const uint32_t* order, OUT* out, unsigned long long* qsum,
-                  const unsigned int* d_status, cudaStream_t s) {
+                  const unsigned int* d_status, cudaStream_t s, float2* H = nullptr) {
     const int N = st->N;
     const int TY = deposit_rows(N);
-    const size_t smem = 8 * static_cast<size_t>(TY) * N;
-    CK(cudaFuncSetAttribute(k_deposit_tiles<OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    size_t smem = 8 * static_cast<size_t>(TY) * N;
+    if constexpr (ZLOG > 0) {
+        // the packed rows of the z transform reuse the accumulators' memory
+        const size_t rows = sizeof(float2) * static_cast<size_t>(N / 2) * (TY + 1);
+        if (rows > smem) smem = rows;
+    }
+    CK(cudaFuncSetAttribute(k_deposit_tiles<OUT, ZLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(smem)));
     const dim3 grid((N + TY - 1) / TY, N);
     ++st->launches;
-    k_deposit_tiles<OUT><<<grid, kDepositThreads, smem, s>>>(st->pos[P][0], st->pos[P][1], st->pos[P][2],
-                                                 order, st->sort.offset, st->sort.shift, N, TY,
-                                                 st->d_plan, out, qsum, d_status);
+    k_deposit_tiles<OUT, ZLOG><<<grid, kDepositThreads, smem, s>>>(
+        st->pos[P][0], st->pos[P][1], st->pos[P][2], order, st->sort.offset, st->sort.shift, N, TY,
+        st->d_plan, out, qsum, d_status, H, st->tw);
     CK(cudaPeekAtLastError());
     return HYOWON_OK;
+}
+
+// The deposit of the five-pass solve: tiles transformed along z into st->modes.
+int deposit_spectrum(State* st, int P, const uint32_t* order, unsigned long long* qsum,
+                     const unsigned int* d_status, cudaStream_t s) {
+    float* const none = nullptr;
+    switch (st->N) {
+    case 32: return deposit_tiles<float, 5>(st, P, order, none, qsum, d_status, s, st->modes);
+    case 64: return deposit_tiles<float, 6>(st, P, order, none, qsum, d_status, s, st->modes);
+    case 128: return deposit_tiles<float, 7>(st, P, order, none, qsum, d_status, s, st->modes);
+    case 256: return deposit_tiles<float, 8>(st, P, order, none, qsum, d_status, s, st->modes);
+    case 512: return deposit_tiles<float, 9>(st, P, order, none, qsum, d_status, s, st->modes);
+    case 1024: return deposit_tiles<float, 10>(st, P, order, none, qsum, d_status, s, st->modes);
+    case 2048: return deposit_tiles<float, 11>(st, P, order, none, qsum, d_status, s, st->modes);
+    default: return fail(st, HYOWON_ELOGIC, "five-pass deposit on a mesh the solve does not support");
+    }
 }
 }
 
@@ -1046,7 +1109,8 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
     ++st->launches;
     k_plan<<<1, 32, 0, s>>>(n, cells, st->d_max_count, green_c0(st), 1, st->d_plan);
     CK(cudaMemsetAsync(st->d_qsum, 0, sizeof(unsigned long long), s));
-    int rc = deposit_tiles<float>(st, P, order, st->rmesh, st->d_qsum, d_status, s);
+    int rc = st->five_pass ? deposit_spectrum(st, P, order, st->d_qsum, d_status, s)
+                           : deposit_tiles<float>(st, P, order, st->rmesh, st->d_qsum, d_status, s);
     if (rc) return rc;
     ++st->launches;
     k_check_mass<<<1, 32, 0, s>>>(st->d_qsum, st->d_plan, st->mass_check_offset, d_status);
@@ -1056,7 +1120,7 @@ int enqueue_force_sets(State* st, cudaStream_t s, unsigned int* d_status, bool k
     const float K2f = static_cast<float>(K2);
     if (st->five_pass) {
         rec(ev, 2, s);
-        int k = poisson::forward_f32(st->fft_plan, N, st->rmesh, st->modes, st->tw, d_status, s);
+        int k = poisson::forward_columns_f32(st->fft_plan, N, st->modes, st->tw, d_status, s);
         if (k < 0) return fail(st, HYOWON_ECUDA, "potential solve: forward pass launch failed");
         st->launches += k;
         rec(ev, 3, s);

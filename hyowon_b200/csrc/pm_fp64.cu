@@ -12,6 +12,7 @@
 
 #include <cmath>
 
+#include "pm_chunk.cuh"
 #include "pm_kernels.h"
 
 namespace hyowon {
@@ -228,6 +229,13 @@ constexpr int kTwoWordMinW = 31;
 #endif
 constexpr int kDepositBatch = HYOWON_DEPOSIT64_BATCH;
 
+// Tile rows for 8-byte-per-cell accumulators of HYOWON_DEPOSIT64_TILE_CELLS
+// cells, halved for the two-word form (same shared memory per tile).
+__host__ __device__ constexpr int tile_rows_f64(int N, int words) {
+    return HYOWON_DEPOSIT64_TILE_CELLS / words / N < 1 ? 1
+         : (HYOWON_DEPOSIT64_TILE_CELLS / words / N > N ? N : HYOWON_DEPOSIT64_TILE_CELLS / words / N);
+}
+
 __device__ __forceinline__ int fixed_split_bits(const uint32_t* max_count) {
     const unsigned long long c = 8ull * (*max_count > 0u ? *max_count : 1u);
     return 63 - (63 - __clzll(c));   // 63 - floor(log2 c)
@@ -249,14 +257,18 @@ __device__ __forceinline__ double fixed_to_double(unsigned long long hi, unsigne
     return ldexp(__ull2double_rn(top), 64 - lz);
 }
 
-template <int kDepositWords>
-__global__ void __launch_bounds__(kTileThreads)
+//
+// ZLOG > 0 (N = 2^ZLOG, a mesh of the five-pass solve): the tile's rows are
+// transformed along z in shared memory (chunked::rows_r2c) and stored to the
+// chunked half spectrum H instead of the real mesh.
+template <int kDepositWords, int ZLOG>
+__global__ void __launch_bounds__(kTileThreads, 4)
 k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
                 const double* __restrict__ z, const double* __restrict__ mass,
                 double uniform_mass, const uint32_t* __restrict__ order,
                 const uint32_t* __restrict__ offset, int shift, Axis a, int TY,
                 const uint32_t* __restrict__ max_count, int e_max, double* __restrict__ mesh,
-                unsigned int* status) {
+                unsigned int* status, double2* __restrict__ H, const double2* __restrict__ tw) {
     extern __shared__ __align__(16) unsigned long long acc[];
     __shared__ uint32_t seg_p0[4], seg_len[4];
     __shared__ int seg_plane[4], seg_row_lo[4], seg_row_hi[4], seg_own[4];
@@ -381,6 +393,41 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
         }
     }
     __syncthreads();
+    if constexpr (ZLOG > 0) {
+        // N = 2^ZLOG and TY = tile_rows_f64(N, words) divides N, so ty == TY
+        using Lz = chunked::Layout<double, ZLOG>;
+        constexpr int TYc = tile_rows_f64(Lz::N, kDepositWords);
+        constexpr int S = TYc + 1;
+        constexpr int PAIRS = TYc * Lz::M;   // cell pairs of the tile
+        constexpr int PT = (PAIRS + kTileThreads - 1) / kTileThreads;
+        const double from_fixed = ldexp(1.0, kDepositWords == 1 ? e_max + 1 - W : e_max - 62);
+        double2 v[PT];
+#pragma unroll
+        for (int i = 0; i < PT; ++i) {
+            const int e = tid + i * kTileThreads;
+            if (e < PAIRS) {
+                if (kDepositWords == 1)
+                    v[i] = make_double2(__ull2double_rn(acc_lo[2 * e]) * from_fixed,
+                                        __ull2double_rn(acc_lo[2 * e + 1]) * from_fixed);
+                else
+                    v[i] = make_double2(fixed_to_double(acc_hi[2 * e], acc_lo[2 * e], W) * from_fixed,
+                                        fixed_to_double(acc_hi[2 * e + 1], acc_lo[2 * e + 1], W)
+                                            * from_fixed);
+            }
+        }
+        __syncthreads();
+        // the accumulators are consumed: reuse their shared memory as rows of
+        // packed complex values, sm[k S + r] = (cell 2k, cell 2k+1) of row r
+        double2* sm = reinterpret_cast<double2*>(acc);
+#pragma unroll
+        for (int i = 0; i < PT; ++i) {
+            const int e = tid + i * kTileThreads;
+            if (e < PAIRS) sm[(e % Lz::M) * S + e / Lz::M] = v[i];
+        }
+        __syncthreads();
+        chunked::rows_r2c<double, ZLOG, TYc, S, 8>(sm, tw, H, x0, y0, tid, kTileThreads);
+        return;
+    }
     double* out = mesh + (static_cast<uint64_t>(x0) * N + y0) * N;
     if (kDepositWords == 1) {
         const double from_fixed = ldexp(1.0, e_max + 1 - W);
@@ -817,13 +864,6 @@ void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,
                                                  mesh, status);
 }
 
-// Tile rows for 8-byte-per-cell accumulators of HYOWON_DEPOSIT64_TILE_CELLS
-// cells, halved for the two-word form (same shared memory per tile).
-int deposit_tile_rows_f64(int N, int words) {
-    int ty = HYOWON_DEPOSIT64_TILE_CELLS / words / N;
-    if (ty < 1) ty = 1;
-    return ty > N ? N : ty;
-}
 
 int deposit_mass_exponent_f64(double max_mass) {
     int e = 0;
@@ -831,38 +871,67 @@ int deposit_mass_exponent_f64(double max_mass) {
     return e;
 }
 
-template <int WORDS>
+template <int WORDS, int ZLOG>
 cudaError_t launch_tiles(const ParticlesF64& p, const double* mass, double uniform_mass,
                          const uint32_t* order, const SortWork& w, Axis a,
-                         const uint32_t* max_count, int e_max, double* mesh,
-                         unsigned int* status, cudaStream_t s) {
+                         const uint32_t* max_count, int e_max, double* mesh, double2* modes,
+                         const double2* tw, unsigned int* status, cudaStream_t s) {
     const int N = a.N;
-    const int TY = deposit_tile_rows_f64(N, WORDS);
-    const size_t smem = 8 * WORDS * static_cast<size_t>(TY) * N;
-    cudaError_t e = cudaFuncSetAttribute(k_deposit_tiles<WORDS>,
+    const int TY = tile_rows_f64(N, WORDS);
+    size_t smem = 8 * WORDS * static_cast<size_t>(TY) * N;
+    if constexpr (ZLOG > 0) {
+        // the packed rows of the z transform reuse the accumulators' memory
+        const size_t rows = sizeof(double2) * static_cast<size_t>(N / 2) * (TY + 1);
+        if (rows > smem) smem = rows;
+    }
+    cudaError_t e = cudaFuncSetAttribute(k_deposit_tiles<WORDS, ZLOG>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     const dim3 grid(static_cast<unsigned>((N + TY - 1) / TY), static_cast<unsigned>(N));
-    k_deposit_tiles<WORDS><<<grid, kTileThreads, smem, s>>>(p.x, p.y, p.z, mass, uniform_mass,
-                                                            order, w.offset, w.shift, a, TY,
-                                                            max_count, e_max, mesh, status);
+    k_deposit_tiles<WORDS, ZLOG><<<grid, kTileThreads, smem, s>>>(
+        p.x, p.y, p.z, mass, uniform_mass, order, w.offset, w.shift, a, TY, max_count, e_max, mesh,
+        status, modes, tw);
     return cudaPeekAtLastError();
+}
+
+template <int WORDS>
+cudaError_t launch_tiles_n(const ParticlesF64& p, const double* mass, double uniform_mass,
+                           const uint32_t* order, const SortWork& w, Axis a,
+                           const uint32_t* max_count, int e_max, double* mesh, double2* modes,
+                           const double2* tw, unsigned int* status, cudaStream_t s) {
+#define HYOWON_TILES(LG) \
+    launch_tiles<WORDS, LG>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh, modes, tw, status, s)
+    if (!modes) return HYOWON_TILES(0);
+    switch (a.N) {
+    case 32: return HYOWON_TILES(5);
+    case 64: return HYOWON_TILES(6);
+    case 128: return HYOWON_TILES(7);
+    case 256: return HYOWON_TILES(8);
+    case 512: return HYOWON_TILES(9);
+    case 1024: return HYOWON_TILES(10);
+    case 2048: return HYOWON_TILES(11);
+    default: return cudaErrorInvalidValue;
+    }
+#undef HYOWON_TILES
 }
 
 cudaError_t launch_deposit_tiles_f64(const ParticlesF64& p, const double* mass,
                                      double uniform_mass, const uint32_t* order,
                                      const SortWork& w, Axis a, const uint32_t* max_count,
                                      uint32_t max_count_host, int e_max, double* mesh,
-                                     unsigned int* status, cudaStream_t s) {
+                                     double2* modes, const double2* tw, unsigned int* status,
+                                     cudaStream_t s) {
     // the same W the kernels derive from *max_count (they check it again)
     const unsigned long long c = 8ull * (max_count_host > 0u ? max_count_host : 1u);
     int lg = 0;
     while ((c >> (lg + 1)) != 0ull) ++lg;
     const int W = 63 - lg;
     if (W >= kOneWordMinW)
-        return launch_tiles<1>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh, status, s);
-    return launch_tiles<2>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh, status, s);
+        return launch_tiles_n<1>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh, modes,
+                                 tw, status, s);
+    return launch_tiles_n<2>(p, mass, uniform_mass, order, w, a, max_count, e_max, mesh, modes, tw,
+                             status, s);
 }
 
 void launch_max_count_f64(uint32_t n_buckets, const uint32_t* count, uint32_t* max_count,

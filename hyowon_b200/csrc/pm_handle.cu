@@ -404,16 +404,18 @@ int enqueue_force(hyowon_pm_t h, int pset, int mset, bool kick, double K2,
     if (rc0) return rc0;
     record(h, 1);
     ++h->launches;
+    // five-pass solve: the deposit writes its tiles transformed along z
     CK(launch_deposit_tiles_f64(p, h->has_masses ? h->mass[h->ic] : nullptr, h->uniform_mass,
                                 order, h->sort, h->axis, h->d_max_count, max_count,
-                                deposit_mass_exponent_f64(h->max_mass), h->mesh, h->d_status,
+                                deposit_mass_exponent_f64(h->max_mass), h->mesh,
+                                h->five_pass ? h->modes : nullptr, h->tw, h->d_status,
                                 h->stream));
     record(h, 2);
     double* const pxo = h->mom[1 - mset][0];
     double* const pyo = h->mom[1 - mset][1];
     double* const pzo = h->mom[1 - mset][2];
     if (h->five_pass) {
-        int k = poisson::forward_f64(h->fft_plan, N, h->mesh, h->modes, h->tw, h->d_status, h->stream);
+        int k = poisson::forward_columns_f64(h->fft_plan, N, h->modes, h->tw, h->d_status, h->stream);
         if (k < 0) return fail(h, HYOWON_ECUDA, "potential solve: forward pass launch failed");
         h->launches += k;
         record(h, 3);
@@ -1383,7 +1385,7 @@ int hyowon_pm_download_mass_mesh(hyowon_pm_t h, double* mesh) {
     CK(launch_deposit_tiles_f64(set_view(h, h->pc, h->mc), h->has_masses ? h->mass[h->ic] : nullptr,
                                 h->uniform_mass, current_order(h), h->sort, h->axis,
                                 h->d_max_count, max_count, deposit_mass_exponent_f64(h->max_mass),
-                                h->mesh, h->d_status, h->stream));
+                                h->mesh, nullptr, nullptr, h->d_status, h->stream));
     unsigned int st = 0;
     int rc = read_status(h, &st);
     if (rc) return rc;

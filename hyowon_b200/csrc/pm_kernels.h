@@ -74,11 +74,15 @@ void launch_deposit_f64(uint32_t n, const ParticlesF64& p, const double* mass,
 // bucket count in *max_count (and its value on the host, which picks the
 // kernel) and e_max = deposit_mass_exponent_f64(max mass).
 int deposit_mass_exponent_f64(double max_mass);
+// With `modes` non-null (a power-of-two mesh of 32 to 2048), the tiles are
+// transformed along z and stored to that chunked half spectrum (twiddles `tw`)
+// instead of `mesh`: the five-pass solve then continues with its column passes.
 cudaError_t launch_deposit_tiles_f64(const ParticlesF64& p, const double* mass,
                                      double uniform_mass, const uint32_t* order,
                                      const SortWork& w, Axis a, const uint32_t* max_count,
                                      uint32_t max_count_host, int e_max, double* mesh,
-                                     unsigned int* status, cudaStream_t s);
+                                     double2* modes, const double2* tw, unsigned int* status,
+                                     cudaStream_t s);
 void launch_max_count_f64(uint32_t n_buckets, const uint32_t* count, uint32_t* max_count,
                           cudaStream_t s);
 void launch_green_f64(int N, double2* modes, const double* lap, const double* win,

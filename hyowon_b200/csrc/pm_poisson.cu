@@ -18,6 +18,7 @@
 // and writes the N^3 potential.
 #include "pm_poisson.h"
 
+#include "pm_chunk.cuh"
 #include "pm_common.cuh"
 #include "pm_fft.cuh"
 #include "pm_tma.cuh"
@@ -55,12 +56,6 @@ using fft::mk;
 #ifndef HYOWON_FFT_CZ64
 #define HYOWON_FFT_CZ64 8
 #endif
-#ifndef HYOWON_FFT_CC32
-#define HYOWON_FFT_CC32 8
-#endif
-#ifndef HYOWON_FFT_CC64
-#define HYOWON_FFT_CC64 4
-#endif
 #ifndef HYOWON_FFT_MINB_Z
 #define HYOWON_FFT_MINB_Z 2
 #endif
@@ -84,31 +79,26 @@ using fft::mk;
 template <typename T, int LOG2N> struct Shape;
 template <int LOG2N> struct Shape<float, LOG2N> {
     static constexpr int CZ = LOG2N >= 11 ? (HYOWON_FFT_CZ32 > 8 ? 8 : HYOWON_FFT_CZ32) : HYOWON_FFT_CZ32;
-    static constexpr int CC = LOG2N >= 11 ? (HYOWON_FFT_CC32 > 4 ? 4 : HYOWON_FFT_CC32) : HYOWON_FFT_CC32;
 };
 template <int LOG2N> struct Shape<double, LOG2N> {
     static constexpr int CZ = LOG2N >= 11 ? (HYOWON_FFT_CZ64 > 4 ? 4 : HYOWON_FFT_CZ64) : HYOWON_FFT_CZ64;
-    static constexpr int CC = LOG2N >= 11 ? (HYOWON_FFT_CC64 > 2 ? 2 : HYOWON_FFT_CC64) : HYOWON_FFT_CC64;
 };
 
-template <typename T, int LOG2N> struct Geo {
+template <typename T, int LOG2N> struct Geo : chunked::Layout<T, LOG2N> {
     using C = cx_t<T>;
-    static constexpr int N = 1 << LOG2N;
-    static constexpr int M = N / 2;          // complex length of a packed row
-    static constexpr int Hz = M + 1;         // half-complex row length
-    static constexpr int K = M / 2 + 1;      // (k, M-k) pairs of a row
+    using L = chunked::Layout<T, LOG2N>;
+    using L::N;
+    using L::M;
+    using L::Hz;
+    using L::K;
+    using L::CC;
+    using L::KC;
+    using L::chunk;
     static constexpr int CZ = Shape<T, LOG2N>::CZ;
-    static constexpr int CC = Shape<T, LOG2N>::CC;
     static constexpr int SZ = CZ + 1;
     static constexpr int TZ = CZ * M / 16;   // threads of a z-pass block
     static constexpr int PZ = CZ * M / TZ;   // row pairs each z-pass thread loads (16)
-    static constexpr int KC = (Hz + CC - 1) / CC;        // kz chunks
     static constexpr int QZ = (KC * CZ * CC + TZ - 1) / TZ;  // chunked values per z-pass thread
-    static constexpr size_t chunk = static_cast<size_t>(N) * N * CC;  // elements per kz chunk
-    // element (kx, ky, kz) of the chunked half spectrum
-    __device__ static __forceinline__ size_t at(int kx, int ky, int kz) {
-        return static_cast<size_t>(kz / CC) * chunk + (static_cast<size_t>(kx) * N + ky) * CC + (kz % CC);
-    }
     static constexpr size_t smem_zf = sizeof(C) * M * SZ;
     static constexpr size_t smem_zi = sizeof(C) * Hz * SZ;
     static constexpr int box = N < 256 ? N : 256;                 // TMA box rows
@@ -166,31 +156,8 @@ k_z_forward(const SRC* __restrict__ in, cx_t<T>* __restrict__ H, const cx_t<T>* 
         }
     }
     __syncthreads();
-    fft::smem_fft<LOG2N - 1, -1, G::CZ, G::SZ>(sm, tw, G::N, tid % G::CZ, tid / G::CZ);
-    const T half = static_cast<T>(0.5);
-    const int x = static_cast<int>(row0 / G::N);
-    const int y0 = static_cast<int>(row0 % G::N);
-    constexpr int KP = (G::K + G::CC - 1) / G::CC;   // chunks covering k = 0..M/2
-    for (int e = tid; e < KP * G::CZ * G::CC; e += G::TZ) {
-        const int ki = e % G::CC;
-        const int r = (e / G::CC) % G::CZ;
-        const int k = (e / (G::CC * G::CZ)) * G::CC + ki;
-        if (k >= G::K) continue;
-        const C zk = sm[k * S + r];
-        const C zm = sm[((G::M - k) & (G::M - 1)) * S + r];
-        const C w = __ldg(&tw[k]);
-        const C E = mk(half * (zk.x + zm.x), half * (zk.y - zm.y));
-        const T dx = zk.x - zm.x;
-        const T dy = zk.y + zm.y;
-        const C O = mk(half * dy, -half * dx);        // (zk - conj(zm)) / 2i
-        H[G::at(x, y0 + r, k)] = fft::cadd(E, fft::cmul(w, O));
-        if (G::M - k != k) {
-            const C E2 = mk(E.x, -E.y);
-            const C O2 = mk(half * dy, half * dx);    // (zm - conj(zk)) / 2i
-            const C w2 = mk(-w.x, w.y);               // W_N^(M-k) = -conj(W_N^k)
-            H[G::at(x, y0 + r, G::M - k)] = fft::cadd(E2, fft::cmul(w2, O2));
-        }
-    }
+    chunked::rows_r2c<T, LOG2N, G::CZ, S>(sm, tw, H, static_cast<int>(row0 / G::N),
+                                         static_cast<int>(row0 % G::N), tid, G::TZ);
 }
 
 // c2r of CZ rows per block: Z[k] = (X[k] + conj X[M-k]) + i W_N^-k (X[k] - conj X[M-k]),
@@ -203,26 +170,25 @@ struct StorePair {
     }
 };
 
-template <typename T, int LOG2N, typename EPI>
-__global__ void __launch_bounds__(Geo<T, LOG2N>::TZ, HYOWON_FFT_MINB_Z)
-k_z_inverse(const cx_t<T>* __restrict__ H, T* __restrict__ out, const cx_t<T>* __restrict__ tw,
-            EPI epi) {
+// The rows (x, y0 .. y0+CZ-1) of the c2r: loads their half-complex values from
+// H (LOAD(p) reads one element), transforms in sm, hands each output pair to
+// epi. Every thread of the TZ-thread block calls it; it ends with sm in use
+// (the caller synchronises before refilling it).
+template <typename T, int LOG2N, typename EPI, typename LOAD>
+__device__ __forceinline__ void z_inverse_rows(const cx_t<T>* __restrict__ H, T* __restrict__ out,
+                                               const cx_t<T>* __restrict__ tw, EPI epi, LOAD load,
+                                               cx_t<T>* sm, int x, int y0, int tid) {
     using G = Geo<T, LOG2N>;
     using C = cx_t<T>;
     constexpr int S = G::SZ;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* sm = reinterpret_cast<C*>(smem_raw);
-    const int tid = threadIdx.x;
-    const size_t row0 = static_cast<size_t>(blockIdx.x) * G::CZ;
-    const int x = static_cast<int>(row0 / G::N);
-    const int y0 = static_cast<int>(row0 % G::N);
+    const size_t row0 = static_cast<size_t>(x) * G::N + y0;
     C v[G::QZ];
 #pragma unroll
     for (int i = 0; i < G::QZ; ++i) {
         const int e = tid + i * G::TZ;
         const int k = (e / (G::CC * G::CZ)) * G::CC + e % G::CC;
         if (e < G::KC * G::CZ * G::CC && k < G::Hz)
-            v[i] = __ldcs(&H[G::at(x, y0 + (e / G::CC) % G::CZ, k)]);
+            v[i] = load(&H[G::at(x, y0 + (e / G::CC) % G::CZ, k)]);
     }
 #pragma unroll
     for (int i = 0; i < G::QZ; ++i) {
@@ -253,6 +219,23 @@ k_z_inverse(const cx_t<T>* __restrict__ H, T* __restrict__ out, const cx_t<T>* _
         const int jj = e % G::M;
         epi(out, (row0 + r) * G::N + 2 * jj, sm[jj * S + r]);
     }
+}
+
+struct LoadStreaming {
+    template <typename C>
+    __device__ __forceinline__ C operator()(const C* p) const { return __ldcs(p); }
+};
+
+template <typename T, int LOG2N, typename EPI>
+__global__ void __launch_bounds__(Geo<T, LOG2N>::TZ, HYOWON_FFT_MINB_Z)
+k_z_inverse(const cx_t<T>* __restrict__ H, T* __restrict__ out, const cx_t<T>* __restrict__ tw,
+            EPI epi) {
+    using G = Geo<T, LOG2N>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const size_t row0 = static_cast<size_t>(blockIdx.x) * G::CZ;
+    z_inverse_rows<T, LOG2N>(H, out, tw, epi, LoadStreaming{}, reinterpret_cast<cx_t<T>*>(smem_raw),
+                             static_cast<int>(row0 / G::N), static_cast<int>(row0 % G::N),
+                             static_cast<int>(threadIdx.x));
 }
 
 struct NoGreen {
@@ -532,6 +515,12 @@ int forward_t(const Plan* p, const SRC* in, cx_t<T>* H, const cx_t<T>* tw, unsig
     return 2;
 }
 
+template <typename T, int LOG2N>
+int forward_columns_t(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, unsigned int* status,
+                      cudaStream_t s) {
+    return columns<T, LOG2N, kPlainAxis, -1, 0>(p, H, tw, NoGreen{}, status, s);
+}
+
 template <typename T, int LOG2N, typename GF>
 int green_t(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF g, unsigned int* status,
             cudaStream_t s) {
@@ -701,6 +690,12 @@ int forward_f64(const Plan* p, int N, const double* mass, double2* modes, const 
     HYOWON_DISPATCH(N, (forward_t<double, double, LG>(p, mass, modes, tw, nullptr, status, s)))
 }
 
+int forward_columns_f64(const Plan* p, int N, double2* modes, const double2* tw,
+                        unsigned int* status, cudaStream_t s) {
+    if (!supported(N) || !p || p->fp32) return -1;
+    HYOWON_DISPATCH(N, (forward_columns_t<double, LG>(p, modes, tw, status, s)))
+}
+
 int green_f64(const Plan* p, int N, double2* modes, const double2* tw, const GreenF64& g,
               cudaStream_t s) {
     if (!supported(N) || !p || p->fp32) return -1;
@@ -752,6 +747,12 @@ int forward_f32(const Plan* p, int N, const float* mesh, float2* modes, const fl
                 unsigned int* status, cudaStream_t s) {
     if (!supported(N) || !p || !p->fp32) return -1;
     HYOWON_DISPATCH(N, (forward_t<float, float, LG>(p, mesh, modes, tw, nullptr, status, s)))
+}
+
+int forward_columns_f32(const Plan* p, int N, float2* modes, const float2* tw,
+                        unsigned int* status, cudaStream_t s) {
+    if (!supported(N) || !p || !p->fp32) return -1;
+    HYOWON_DISPATCH(N, (forward_columns_t<float, LG>(p, modes, tw, status, s)))
 }
 
 int green_f32(const Plan* p, int N, float2* modes, const float2* tw, const GreenF32& g,

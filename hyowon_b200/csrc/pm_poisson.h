@@ -96,6 +96,10 @@ int hessian_source_f64(const Plan* pd, const Plan* pw, int N, double2* work, con
 // status receives ST_PIPELINE if a pipelined pass gives up waiting.
 int forward_f64(const Plan* p, int N, const double* mass, double2* modes, const double2* tw,
                 unsigned int* status, cudaStream_t s);
+// The forward pass after the z pass: for spectra whose rows the deposit already
+// transformed along z (chunked::rows_r2c in pm_chunk.cuh).
+int forward_columns_f64(const Plan* p, int N, double2* modes, const double2* tw,
+                        unsigned int* status, cudaStream_t s);
 int green_f64(const Plan* p, int N, double2* modes, const double2* tw, const GreenF64& g,
               cudaStream_t s);
 int inverse_f64(const Plan* p, int N, double2* modes, double* phi, const double2* tw,
@@ -103,6 +107,8 @@ int inverse_f64(const Plan* p, int N, double2* modes, double* phi, const double2
 
 int forward_f32(const Plan* p, int N, const float* mesh, float2* modes, const float2* tw,
                 unsigned int* status, cudaStream_t s);
+int forward_columns_f32(const Plan* p, int N, float2* modes, const float2* tw,
+                        unsigned int* status, cudaStream_t s);
 int green_f32(const Plan* p, int N, float2* modes, const float2* tw, const GreenF32& g,
               unsigned int* status, cudaStream_t s);
 int inverse_f32(const Plan* p, int N, float2* modes, float* phi, const float2* tw,
