@@ -47,22 +47,17 @@ template <typename T, int LOG2N> struct Layout {
     }
 };
 
-// r2c of R consecutive rows (x, y0 .. y0+R-1) whose N reals sit packed in
-// shared memory as N/2 complex values, sm[k * S + r] = (row r [2k], row r
-// [2k+1]): a length-N/2 forward transform, then X[k] = E[k] + W_N^k O[k] with
-// E/O the transforms of the even/odd samples, for k = 0..N/2, stored to the
-// chunked spectrum H. Every thread of the block calls it (the transform's
-// barriers); threads [0, R N/(2 EPT)) carry the transform, EPT elements each
-// (8 or 16), all `nthreads` the stores. The caller has synchronised after
-// filling sm.
-template <typename T, int LOG2N, int R, int S, int EPT = 16>
-__device__ __forceinline__ void rows_r2c(cx_t<T>* sm, const cx_t<T>* __restrict__ tw,
-                                         cx_t<T>* __restrict__ H, int x, int y0, int tid,
-                                         int nthreads) {
+// Unpacks R transformed rows, sm[k * S + r] = Z_r[k] (the length-N/2 forward
+// transform of row r's N reals read as N/2 complex values), into
+// X[k] = E[k] + W_N^k O[k] with E/O the transforms of the even/odd samples,
+// for k = 0..N/2, and stores them to the chunked spectrum H at rows
+// (x, y0 .. y0+R-1). All `nthreads` threads take part.
+template <typename T, int LOG2N, int R, int S>
+__device__ __forceinline__ void rows_unpack(const cx_t<T>* sm, const cx_t<T>* __restrict__ tw,
+                                            cx_t<T>* __restrict__ H, int x, int y0, int tid,
+                                            int nthreads) {
     using L = Layout<T, LOG2N>;
     using C = cx_t<T>;
-    constexpr int P = L::M / EPT;   // butterfly groups per row
-    fft::smem_fft<LOG2N - 1, -1, R, S, EPT>(sm, tw, L::N, tid % R, tid / R, tid < R * P);
     const T half = static_cast<T>(0.5);
     constexpr int KP = (L::K + L::CC - 1) / L::CC;   // chunks covering k = 0..M/2
     for (int e = tid; e < KP * R * L::CC; e += nthreads) {
@@ -85,6 +80,82 @@ __device__ __forceinline__ void rows_r2c(cx_t<T>* sm, const cx_t<T>* __restrict_
             H[L::at(x, y0 + r, L::M - k)] = fft::cadd(E2, fft::cmul(w2, O2));
         }
     }
+}
+
+// r2c of R consecutive rows (x, y0 .. y0+R-1) whose N reals sit packed in
+// shared memory as N/2 complex values, sm[k * S + r] = (row r [2k], row r
+// [2k+1]): a length-N/2 forward transform, then rows_unpack. Every thread of
+// the block calls it (the transform's barriers); threads [0, R N/(2 EPT))
+// carry the transform, EPT elements each (8 or 16), all `nthreads` the
+// stores. The caller has synchronised after filling sm.
+template <typename T, int LOG2N, int R, int S, int EPT = 16>
+__device__ __forceinline__ void rows_r2c(cx_t<T>* sm, const cx_t<T>* __restrict__ tw,
+                                         cx_t<T>* __restrict__ H, int x, int y0, int tid,
+                                         int nthreads) {
+    using L = Layout<T, LOG2N>;
+    constexpr int P = L::M / EPT;   // butterfly groups per row
+    fft::smem_fft<LOG2N - 1, -1, R, S, EPT>(sm, tw, L::N, tid % R, tid / R, tid < R * P);
+    rows_unpack<T, LOG2N, R, S>(sm, tw, H, x, y0, tid, nthreads);
+}
+
+// The r2c of a finished deposit tile of TY rows (x, y0 .. y0+TY-1): the
+// first radix-8 stage reads its inputs straight from the tile's accumulators
+// (pair(r, k) returns cells 2k and 2k+1 of row r as one complex value, each
+// pair read once), every thread's reads end before the first write, and the
+// transform then runs in place in the accumulators' shared memory `sm` (at
+// least N/2 TY complex values): rows of TY dense columns, the first stage's
+// output rows permuted so that no stage has bank conflicts, then rows_unpack.
+// Every thread of the block calls it; threads [0, TY N/16) carry the transform.
+template <typename T, int LOG2N, int TY, typename PAIR>
+__device__ __forceinline__ void tile_r2c(PAIR pair, cx_t<T>* sm, const cx_t<T>* __restrict__ tw,
+                                         cx_t<T>* __restrict__ H, int x, int y0, int tid,
+                                         int nthreads) {
+    using L = Layout<T, LOG2N>;
+    using C = cx_t<T>;
+    constexpr int E = 8;
+    constexpr int LOG2M = LOG2N - 1;
+    constexpr int M = L::M;
+    constexpr int P = M / E;
+    constexpr int S = TY;
+    // row groups a 128-byte bank row holds: the first stage's lanes write rows
+    // 8 j + r, spread over them by the permutation
+    constexpr int Q = 128 / (TY * static_cast<int>(sizeof(C))) > 1
+                          ? 128 / (TY * static_cast<int>(sizeof(C))) : 1;
+    constexpr int MASK = Q - 1;
+    constexpr int nE = LOG2M / 3;
+    constexpr int rem = LOG2M % 3;
+    static_assert(LOG2M >= 3, "rows of at least 16 cells");
+    const bool active = tid < TY * P;
+    const int c = tid % TY;
+    const int j = tid / TY;
+    C v[E];
+    if (active) {
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[r] = pair(c, j + r * (M / E));
+    }
+    __syncthreads();
+    if (active) {
+        fft::dft<E, -1>(v);
+#pragma unroll
+        for (int r = 0; r < E; ++r) sm[fft::row_at<true, 3, MASK>(j * E + r) * S + c] = v[r];
+    }
+    __syncthreads();
+    int Ns = E;
+    if constexpr (nE >= 2) {
+        fft::smem_stage<LOG2M, E, -1, TY, S, E, true, false, MASK>(sm, Ns, tw, L::N, c, j, active);
+        Ns *= E;
+#pragma unroll 1
+        for (int s = 2; s < nE; ++s) {
+            fft::smem_stage<LOG2M, E, -1, TY, S, E>(sm, Ns, tw, L::N, c, j, active);
+            Ns *= E;
+        }
+        if constexpr (rem != 0)
+            fft::smem_stage<LOG2M, (1 << rem), -1, TY, S, E>(sm, Ns, tw, L::N, c, j, active);
+    } else if constexpr (rem != 0) {
+        fft::smem_stage<LOG2M, (1 << rem), -1, TY, S, E, true, false, MASK>(sm, Ns, tw, L::N, c, j,
+                                                                           active);
+    }
+    rows_unpack<T, LOG2N, TY, S>(sm, tw, H, x, y0, tid, nthreads);
 }
 
 }  // namespace chunked

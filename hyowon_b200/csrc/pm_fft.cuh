@@ -127,32 +127,35 @@ __device__ __forceinline__ void twiddle(C (&v)[R], int k, int Ns, const C* __res
     }
 }
 
-// Stage geometry for a length L = 2^LOG2L transform: radix-16 stages, then
-// one stage of radix 2^(LOG2L mod 4) if that is not zero.
-template <int LOG2L> struct Plan {
+// Stage geometry for a length L = 2^LOG2L transform with E (8 or 16)
+// elements per thread: radix-E stages, then one stage of radix 2^(LOG2L mod
+// log2 E) if that is not zero.
+template <int LOG2L, int E = 16> struct Plan {
     static constexpr int L = 1 << LOG2L;
-    static constexpr int n16 = LOG2L / 4;
-    static constexpr int rem = LOG2L % 4;
-    static constexpr int RF = rem ? (1 << rem) : 16;   // radix of the last stage
-    static constexpr int stages = n16 + (rem ? 1 : 0);
-    static constexpr int P = L / 16;                    // butterfly groups per sequence
-    static_assert(LOG2L >= 4, "transform length must be at least 16");
+    static constexpr int LE = ilog2<E>();
+    static constexpr int nE = LOG2L / LE;
+    static constexpr int rem = LOG2L % LE;
+    static constexpr int RF = rem ? (1 << rem) : E;    // radix of the last stage
+    static constexpr int P = L / E;                     // butterfly groups per sequence
+    static_assert(LOG2L >= LE, "transform shorter than the elements per thread");
 };
 
 // Row order of the first stage's output in the dense column tiles: row rho is
-// kept at rho ^ ((rho >> 4) & 1). A radix-16 first stage writes rows 16 j + r
-// for the lanes' consecutive j, which all fall in the same half of a 128-byte
-// bank row when a row is 64 bytes (CC columns); swapping row pairs in every
-// other group of 16 rows spreads them over both halves (4- and 8-way bank
-// conflicts become none), while the next stage's reads of consecutive rows
-// stay consecutive. Every access to that stage's output applies it (PIN /
-// POUT below); other layouts are untouched.
+// kept at rho ^ ((rho >> LE) & 1) for a radix-2^LE first stage. That stage
+// writes rows 2^LE j + r for the lanes' consecutive j, which all fall in the
+// same half of a 128-byte bank row when a row is 64 bytes (CC columns);
+// swapping row pairs in every other group of 2^LE rows spreads them over both
+// halves (4- and 8-way bank conflicts become none), while the next stage's
+// reads of consecutive rows stay consecutive. Every access to that stage's
+// output applies it (PIN / POUT below); other layouts are untouched.
 #ifndef HYOWON_FFT_ROWPERM
 #define HYOWON_FFT_ROWPERM 1
 #endif
-template <bool PERMUTED>
+// MASK widens the swap to the low log2(MASK + 1) bits (rows narrower than 64
+// bytes need more row groups spread over a 128-byte bank row).
+template <bool PERMUTED, int LE = 4, int MASK = 1>
 __device__ __forceinline__ int row_at(int row) {
-    return (PERMUTED && HYOWON_FFT_ROWPERM) ? (row ^ ((row >> 4) & 1)) : row;
+    return (PERMUTED && HYOWON_FFT_ROWPERM) ? (row ^ ((row >> LE) & MASK)) : row;
 }
 
 // One shared-memory stage of radix R (R <= E) on C interleaved sequences of
@@ -161,7 +164,7 @@ __device__ __forceinline__ int row_at(int row) {
 // the stage ends synchronised. Threads with `active` false only take part in
 // the barriers.
 template <int LOG2L, int R, int SIGN, int C, int S, int E = 16, bool PIN = false, bool POUT = false,
-          typename Cplx>
+          int PMASK = 1, typename Cplx>
 __device__ __forceinline__ void smem_stage(Cplx* sm, int Ns, const Cplx* __restrict__ tw, int NT,
                                            int c, int j, bool active = true) {
     constexpr int L = 1 << LOG2L;
@@ -173,7 +176,8 @@ __device__ __forceinline__ void smem_stage(Cplx* sm, int Ns, const Cplx* __restr
         for (int b = 0; b < NB; ++b) {
             const int jb = j + P * b;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[b][r] = sm[row_at<PIN>(jb + r * (L / R)) * S + c];
+            for (int r = 0; r < R; ++r)
+                v[b][r] = sm[row_at<PIN, ilog2<E>(), PMASK>(jb + r * (L / R)) * S + c];
         }
     }
     __syncthreads();
@@ -186,7 +190,7 @@ __device__ __forceinline__ void smem_stage(Cplx* sm, int Ns, const Cplx* __restr
             dft<R, SIGN>(v[b]);
             const int base = (jb - k) * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) sm[row_at<POUT>(base + r * Ns) * S + c] = v[b][r];
+            for (int r = 0; r < R; ++r) sm[row_at<POUT, ilog2<E>(), PMASK>(base + r * Ns) * S + c] = v[b][r];
         }
     }
     __syncthreads();
@@ -211,32 +215,32 @@ __device__ __forceinline__ void smem_fft(Cplx* sm, const Cplx* __restrict__ tw, 
     if constexpr (rem != 0) smem_stage<LOG2L, (1 << rem), SIGN, C, S, E>(sm, Ns, tw, NT, c, j, active);
 }
 
-// First stage (radix 16, no twiddles) from 16 values already in registers,
+// First stage (radix E, no twiddles) from E values already in registers,
 // v[r] = element j + r P, written to shared memory in the permuted row order
 // (row_at) that rest_to_registers reads.
-template <int LOG2L, int SIGN, int C, int S, typename Cplx>
-__device__ __forceinline__ void first_stage_to_smem(Cplx (&v)[16], Cplx* sm, int c, int j) {
-    dft<16, SIGN>(v);
+template <int LOG2L, int SIGN, int C, int S, int E = 16, typename Cplx>
+__device__ __forceinline__ void first_stage_to_smem(Cplx (&v)[E], Cplx* sm, int c, int j) {
+    dft<E, SIGN>(v);
 #pragma unroll
-    for (int r = 0; r < 16; ++r) sm[row_at<true>(j * 16 + r) * S + c] = v[r];
+    for (int r = 0; r < E; ++r) sm[row_at<true, ilog2<E>()>(j * E + r) * S + c] = v[r];
 }
 
 // The last stage (stride Ns = L / RF), read from shared memory and returned in
-// registers: out[q] = element j + q P of the transform (q < 16).
-template <int LOG2L, int SIGN, int C, int S, bool PIN = false, typename Cplx>
+// registers: out[q] = element j + q P of the transform (q < E).
+template <int LOG2L, int SIGN, int C, int S, int E = 16, bool PIN = false, typename Cplx>
 __device__ __forceinline__ void final_to_registers(const Cplx* sm, int Ns, const Cplx* __restrict__ tw,
-                                                   int NT, int c, int j, Cplx (&out)[16]) {
-    using PL = Plan<LOG2L>;
+                                                   int NT, int c, int j, Cplx (&out)[E]) {
+    using PL = Plan<LOG2L, E>;
     constexpr int L = PL::L;
     constexpr int P = PL::P;
     constexpr int R = PL::RF;
-    constexpr int NB = 16 / R;
+    constexpr int NB = E / R;
     Cplx v[NB][R];
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
         const int jb = j + P * b;
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[b][r] = sm[row_at<PIN>(jb + r * (L / R)) * S + c];
+        for (int r = 0; r < R; ++r) v[b][r] = sm[row_at<PIN, PL::LE>(jb + r * (L / R)) * S + c];
     }
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
@@ -251,56 +255,56 @@ __device__ __forceinline__ void final_to_registers(const Cplx* sm, int Ns, const
 }
 
 // Middle stages plus the last stage, after first_stage_to_smem.
-template <int LOG2L, int SIGN, int C, int S, typename Cplx>
+template <int LOG2L, int SIGN, int C, int S, int E = 16, typename Cplx>
 __device__ __forceinline__ void rest_to_registers(Cplx* sm, const Cplx* __restrict__ tw, int NT, int c,
-                                                  int j, Cplx (&out)[16]) {
-    using PL = Plan<LOG2L>;
-    int Ns = 16;
+                                                  int j, Cplx (&out)[E]) {
+    using PL = Plan<LOG2L, E>;
+    int Ns = E;
     // the first stage's shared-memory writes must land before anyone reads
     __syncthreads();
-    // radix-16 stages after the first, except a final radix-16 one; the
-    // first of them reads the first stage's permuted rows
-    constexpr int mid = PL::rem ? PL::n16 - 1 : PL::n16 - 2;
+    // radix-E stages after the first, except a final radix-E one; the first
+    // of them reads the first stage's permuted rows
+    constexpr int mid = PL::rem ? PL::nE - 1 : PL::nE - 2;
     if constexpr (mid >= 1) {
-        smem_stage<LOG2L, 16, SIGN, C, S, 16, true, false>(sm, Ns, tw, NT, c, j);
-        Ns *= 16;
+        smem_stage<LOG2L, E, SIGN, C, S, E, true, false>(sm, Ns, tw, NT, c, j);
+        Ns *= E;
 #pragma unroll 1
         for (int s = 1; s < mid; ++s) {
-            smem_stage<LOG2L, 16, SIGN, C, S>(sm, Ns, tw, NT, c, j);
-            Ns *= 16;
+            smem_stage<LOG2L, E, SIGN, C, S, E>(sm, Ns, tw, NT, c, j);
+            Ns *= E;
         }
-        final_to_registers<LOG2L, SIGN, C, S>(sm, Ns, tw, NT, c, j, out);
+        final_to_registers<LOG2L, SIGN, C, S, E>(sm, Ns, tw, NT, c, j, out);
     } else {
-        final_to_registers<LOG2L, SIGN, C, S, true>(sm, Ns, tw, NT, c, j, out);
+        final_to_registers<LOG2L, SIGN, C, S, E, true>(sm, Ns, tw, NT, c, j, out);
     }
 }
 
 // Whole transform from natural order in shared memory (the caller has
 // synchronised after filling it) to registers, out[q] = element j + q P.
-template <int LOG2L, int SIGN, int C, int S, typename Cplx>
+template <int LOG2L, int SIGN, int C, int S, int E = 16, typename Cplx>
 __device__ __forceinline__ void smem_to_registers(Cplx* sm, const Cplx* __restrict__ tw, int NT, int c,
-                                                  int j, Cplx (&out)[16]) {
-    using PL = Plan<LOG2L>;
+                                                  int j, Cplx (&out)[E]) {
+    using PL = Plan<LOG2L, E>;
     int Ns = 1;
-    // every radix-16 stage but a final radix-16 one; the first writes its rows
+    // every radix-E stage but a final radix-E one; the first writes its rows
     // permuted (row_at) and the stage after it reads them so
-    constexpr int n = PL::rem ? PL::n16 : PL::n16 - 1;
+    constexpr int n = PL::rem ? PL::nE : PL::nE - 1;
     if constexpr (n == 0) {
-        final_to_registers<LOG2L, SIGN, C, S>(sm, Ns, tw, NT, c, j, out);
+        final_to_registers<LOG2L, SIGN, C, S, E>(sm, Ns, tw, NT, c, j, out);
     } else {
-        smem_stage<LOG2L, 16, SIGN, C, S, 16, false, true>(sm, Ns, tw, NT, c, j);
-        Ns = 16;
+        smem_stage<LOG2L, E, SIGN, C, S, E, false, true>(sm, Ns, tw, NT, c, j);
+        Ns = E;
         if constexpr (n >= 2) {
-            smem_stage<LOG2L, 16, SIGN, C, S, 16, true, false>(sm, Ns, tw, NT, c, j);
-            Ns = 256;
+            smem_stage<LOG2L, E, SIGN, C, S, E, true, false>(sm, Ns, tw, NT, c, j);
+            Ns = E * E;
 #pragma unroll 1
             for (int s = 2; s < n; ++s) {
-                smem_stage<LOG2L, 16, SIGN, C, S>(sm, Ns, tw, NT, c, j);
-                Ns *= 16;
+                smem_stage<LOG2L, E, SIGN, C, S, E>(sm, Ns, tw, NT, c, j);
+                Ns *= E;
             }
-            final_to_registers<LOG2L, SIGN, C, S>(sm, Ns, tw, NT, c, j, out);
+            final_to_registers<LOG2L, SIGN, C, S, E>(sm, Ns, tw, NT, c, j, out);
         } else {
-            final_to_registers<LOG2L, SIGN, C, S, true>(sm, Ns, tw, NT, c, j, out);
+            final_to_registers<LOG2L, SIGN, C, S, E, true>(sm, Ns, tw, NT, c, j, out);
         }
     }
 }

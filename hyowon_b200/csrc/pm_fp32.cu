@@ -287,7 +287,7 @@ __host__ __device__ constexpr int deposit_rows(int N) {
 //
 // ZLOG > 0 (N = 2^ZLOG, a power-of-two mesh of the five-pass solve): instead of
 // the real cells the tile's rows are transformed along z in shared memory
-// (chunked::rows_r2c) and stored to the chunked half spectrum H, the first
+// (chunked::tile_r2c) and stored to the chunked half spectrum H, the first
 // pass of the potential solve done while the tile is on chip.
 template <typename OUT, int ZLOG>
 __global__ void HYOWON_DEPOSIT_BOUNDS
@@ -407,38 +407,22 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
     __syncthreads();
     const long long mean = plan->mean_q;
     if constexpr (ZLOG > 0) {
-        // N = 2^ZLOG and TY = deposit_rows(N) divides N, so ty == TY here
+        // N = 2^ZLOG and TY = deposit_rows(N) divides N, so ty == TY here;
+        // each cell pair is read once, by the transform's first stage
         using Lz = chunked::Layout<float, ZLOG>;
         constexpr int TYc = deposit_rows(Lz::N);
-        constexpr int S = TYc + 1;
-        constexpr int PAIRS = TYc * Lz::M;   // cell pairs of the tile
-        constexpr int PT = (PAIRS + kDepositThreads - 1) / kDepositThreads;
         const ulonglong2* q2 = reinterpret_cast<const ulonglong2*>(qtile);
-        float2 v[PT];
         unsigned long long local = 0;
-#pragma unroll
-        for (int i = 0; i < PT; ++i) {
-            const int e = tid + i * kDepositThreads;
-            if (e < PAIRS) {
-                const ulonglong2 q = q2[e];
-                const long long a0 = static_cast<long long>(q.x) - mean;
-                const long long a1 = static_cast<long long>(q.y) - mean;
-                local += static_cast<unsigned long long>(a0) + static_cast<unsigned long long>(a1);
-                v[i] = make_float2(__ll2float_rn(a0), __ll2float_rn(a1));
-            }
-        }
+        auto pair = [&](int r, int k) {
+            const ulonglong2 q = q2[r * (Lz::N / 2) + k];
+            const long long a0 = static_cast<long long>(q.x) - mean;
+            const long long a1 = static_cast<long long>(q.y) - mean;
+            local += static_cast<unsigned long long>(a0) + static_cast<unsigned long long>(a1);
+            return make_float2(__ll2float_rn(a0), __ll2float_rn(a1));
+        };
+        chunked::tile_r2c<float, ZLOG, TYc>(pair, reinterpret_cast<float2*>(qtile), tw, H, x0, y0, tid,
+                                            kDepositThreads);
         if (qsum) block_sum_to(local, qsum);
-        __syncthreads();
-        // the accumulators are consumed: reuse their shared memory as rows of
-        // packed complex values, sm[k S + r] = (cell 2k, cell 2k+1) of row r
-        float2* sm = reinterpret_cast<float2*>(qtile);
-#pragma unroll
-        for (int i = 0; i < PT; ++i) {
-            const int e = tid + i * kDepositThreads;
-            if (e < PAIRS) sm[(e % Lz::M) * S + e / Lz::M] = v[i];
-        }
-        __syncthreads();
-        chunked::rows_r2c<float, ZLOG, TYc, S, 8>(sm, tw, H, x0, y0, tid, kDepositThreads);
         return;
     }
     OUT* o = out + (static_cast<uint64_t>(x0) * N + y0) * N;
@@ -1056,8 +1040,8 @@ int deposit_tiles(State* st, int P, const uint32_t* order, OUT* out, unsigned lo
     const int TY = deposit_rows(N);
     size_t smem = 8 * static_cast<size_t>(TY) * N;
     if constexpr (ZLOG > 0) {
-        // the packed rows of the z transform reuse the accumulators' memory
-        const size_t rows = sizeof(float2) * static_cast<size_t>(N / 2) * (TY + 1);
+        // the z transform runs in the accumulators' memory
+        const size_t rows = sizeof(float2) * static_cast<size_t>(N / 2) * TY;
         if (rows > smem) smem = rows;
     }
     CK(cudaFuncSetAttribute(k_deposit_tiles<OUT, ZLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize,

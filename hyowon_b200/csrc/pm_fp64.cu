@@ -259,7 +259,7 @@ __device__ __forceinline__ double fixed_to_double(unsigned long long hi, unsigne
 
 //
 // ZLOG > 0 (N = 2^ZLOG, a mesh of the five-pass solve): the tile's rows are
-// transformed along z in shared memory (chunked::rows_r2c) and stored to the
+// transformed along z in shared memory (chunked::tile_r2c) and stored to the
 // chunked half spectrum H instead of the real mesh.
 template <int kDepositWords, int ZLOG>
 __global__ void __launch_bounds__(kTileThreads, 4)
@@ -394,38 +394,24 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
     }
     __syncthreads();
     if constexpr (ZLOG > 0) {
-        // N = 2^ZLOG and TY = tile_rows_f64(N, words) divides N, so ty == TY
+        // N = 2^ZLOG and TY = tile_rows_f64(N, words) divides N, so ty == TY;
+        // each cell pair is read once, by the transform's first stage
         using Lz = chunked::Layout<double, ZLOG>;
         constexpr int TYc = tile_rows_f64(Lz::N, kDepositWords);
-        constexpr int S = TYc + 1;
-        constexpr int PAIRS = TYc * Lz::M;   // cell pairs of the tile
-        constexpr int PT = (PAIRS + kTileThreads - 1) / kTileThreads;
         const double from_fixed = ldexp(1.0, kDepositWords == 1 ? e_max + 1 - W : e_max - 62);
-        double2 v[PT];
-#pragma unroll
-        for (int i = 0; i < PT; ++i) {
-            const int e = tid + i * kTileThreads;
-            if (e < PAIRS) {
-                if (kDepositWords == 1)
-                    v[i] = make_double2(__ull2double_rn(acc_lo[2 * e]) * from_fixed,
-                                        __ull2double_rn(acc_lo[2 * e + 1]) * from_fixed);
-                else
-                    v[i] = make_double2(fixed_to_double(acc_hi[2 * e], acc_lo[2 * e], W) * from_fixed,
-                                        fixed_to_double(acc_hi[2 * e + 1], acc_lo[2 * e + 1], W)
-                                            * from_fixed);
-            }
-        }
-        __syncthreads();
-        // the accumulators are consumed: reuse their shared memory as rows of
-        // packed complex values, sm[k S + r] = (cell 2k, cell 2k+1) of row r
-        double2* sm = reinterpret_cast<double2*>(acc);
-#pragma unroll
-        for (int i = 0; i < PT; ++i) {
-            const int e = tid + i * kTileThreads;
-            if (e < PAIRS) sm[(e % Lz::M) * S + e / Lz::M] = v[i];
-        }
-        __syncthreads();
-        chunked::rows_r2c<double, ZLOG, TYc, S, 8>(sm, tw, H, x0, y0, tid, kTileThreads);
+        const ulonglong2* lo2 = reinterpret_cast<const ulonglong2*>(acc_lo);
+        const ulonglong2* hi2 = reinterpret_cast<const ulonglong2*>(acc_hi);
+        auto pair = [&](int r, int k) {
+            const int e = r * (Lz::N / 2) + k;
+            const ulonglong2 lo = lo2[e];
+            if (kDepositWords == 1)
+                return make_double2(__ull2double_rn(lo.x) * from_fixed, __ull2double_rn(lo.y) * from_fixed);
+            const ulonglong2 hi = hi2[e];
+            return make_double2(fixed_to_double(hi.x, lo.x, W) * from_fixed,
+                                fixed_to_double(hi.y, lo.y, W) * from_fixed);
+        };
+        chunked::tile_r2c<double, ZLOG, TYc>(pair, reinterpret_cast<double2*>(acc), tw, H, x0, y0, tid,
+                                             kTileThreads);
         return;
     }
     double* out = mesh + (static_cast<uint64_t>(x0) * N + y0) * N;
@@ -880,8 +866,8 @@ cudaError_t launch_tiles(const ParticlesF64& p, const double* mass, double unifo
     const int TY = tile_rows_f64(N, WORDS);
     size_t smem = 8 * WORDS * static_cast<size_t>(TY) * N;
     if constexpr (ZLOG > 0) {
-        // the packed rows of the z transform reuse the accumulators' memory
-        const size_t rows = sizeof(double2) * static_cast<size_t>(N / 2) * (TY + 1);
+        // the z transform runs in the accumulators' memory
+        const size_t rows = sizeof(double2) * static_cast<size_t>(N / 2) * TY;
         if (rows > smem) smem = rows;
     }
     cudaError_t e = cudaFuncSetAttribute(k_deposit_tiles<WORDS, ZLOG>,

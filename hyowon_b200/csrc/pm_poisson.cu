@@ -75,6 +75,12 @@ using fft::mk;
 #ifndef HYOWON_FFT_SPLIT
 #define HYOWON_FFT_SPLIT 1
 #endif
+// Elements each thread of a column pass holds (16: radix-16 stages, CC N / 16
+// threads a tile; 8: radix-8 stages and twice the threads, measured slower on
+// B200 at N = 1024: 3.66 against 3.32 ms for the FP32 x pass).
+#ifndef HYOWON_FFT_EPT
+#define HYOWON_FFT_EPT 16
+#endif
 
 template <typename T, int LOG2N> struct Shape;
 template <int LOG2N> struct Shape<float, LOG2N> {
@@ -107,7 +113,8 @@ template <typename T, int LOG2N> struct Geo : chunked::Layout<T, LOG2N> {
     // (HYOWON_FFT_NBUF deep where shared memory allows)
     static constexpr int SP = (LOG2N >= 8 && CC % HYOWON_FFT_SPLIT == 0) ? HYOWON_FFT_SPLIT : 1;
     static constexpr int CB = CC / SP;
-    static constexpr int TCB = CB * N / 16;                       // threads of a column block
+    static constexpr int EC = HYOWON_FFT_EPT == 8 ? 8 : 16;  // elements per thread
+    static constexpr int TCB = CB * N / EC;                       // threads of a column block
     static constexpr unsigned tile_bytes_b = sizeof(C) * N * CB;  // one block's part of a tile
     static constexpr int nbuf_b = (HYOWON_FFT_NBUF * tile_bytes_b <= 200u * 1024u) ? HYOWON_FFT_NBUF : 2;
     static constexpr size_t smem_cb = static_cast<size_t>(nbuf_b) * tile_bytes_b;
@@ -358,7 +365,8 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
           const cx_t<T>* __restrict__ tw, GF green, unsigned int* status, unsigned wait_limit) {
     using G = Geo<T, LOG2N>;
     using C = cx_t<T>;
-    constexpr int P = G::N / 16;
+    constexpr int EC = G::EC;
+    constexpr int P = G::N / EC;
     constexpr int CB = G::CB;     // columns of this block's part of a tile
     constexpr int S = CB;
     constexpr int NB = G::nbuf_b;
@@ -433,36 +441,36 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
         const int kc = static_cast<int>(tile / G::N);
         const int seq = static_cast<int>(tile % G::N);
         const int kz = kc * G::CC + col;
-        C v[16];
+        C v[EC];
         if constexpr (MODE == 2) {
             // element j + q P of column c, untransformed
 #pragma unroll
-            for (int q = 0; q < 16; ++q) v[q] = sm[(j + q * P) * S + c];
+            for (int q = 0; q < EC; ++q) v[q] = sm[(j + q * P) * S + c];
             if (kz < G::Hz) {
 #pragma unroll
-                for (int q = 0; q < 16; ++q)
+                for (int q = 0; q < EC; ++q)
                     v[q] = AXIS == 0 ? green(j + q * P, seq, kz, v[q]) : green(seq, j + q * P, kz, v[q]);
             }
             __syncthreads();
-            fft::first_stage_to_smem<LOG2N, SIGN, CB, S>(v, sm, c, j);
-            fft::rest_to_registers<LOG2N, SIGN, CB, S>(sm, tw, G::N, c, j, v);
+            fft::first_stage_to_smem<LOG2N, SIGN, CB, S, EC>(v, sm, c, j);
+            fft::rest_to_registers<LOG2N, SIGN, CB, S, EC>(sm, tw, G::N, c, j, v);
         } else {
-            fft::smem_to_registers<LOG2N, SIGN, CB, S>(sm, tw, G::N, c, j, v);
+            fft::smem_to_registers<LOG2N, SIGN, CB, S, EC>(sm, tw, G::N, c, j, v);
         }
         if constexpr (MODE == 1) {
             if (kz < G::Hz) {
 #pragma unroll
-                for (int q = 0; q < 16; ++q)
+                for (int q = 0; q < EC; ++q)
                     v[q] = AXIS == 0 ? green(j + q * P, seq, kz, v[q]) : green(seq, j + q * P, kz, v[q]);
             }
             __syncthreads();
-            fft::first_stage_to_smem<LOG2N, -SIGN, CB, S>(v, sm, c, j);
-            fft::rest_to_registers<LOG2N, -SIGN, CB, S>(sm, tw, G::N, c, j, v);
+            fft::first_stage_to_smem<LOG2N, -SIGN, CB, S, EC>(v, sm, c, j);
+            fft::rest_to_registers<LOG2N, -SIGN, CB, S, EC>(sm, tw, G::N, c, j, v);
         }
         if (kz < G::Hz) {
             C* dst = H + static_cast<size_t>(kc) * G::chunk + static_cast<size_t>(seq) * seq_stride + col;
 #pragma unroll
-            for (int q = 0; q < 16; ++q) __stcs(&dst[static_cast<size_t>(j + q * P) * axis_stride], v[q]);
+            for (int q = 0; q < EC; ++q) __stcs(&dst[static_cast<size_t>(j + q * P) * axis_stride], v[q]);
         }
         __syncthreads();
     }
