@@ -225,29 +225,29 @@ def phase_bytes(form, n, N, sort_fraction):
     kick/drift: read x, p, a; write candidate x, p (+ keys / ranks, and the
       scatter of x, p, id on sort steps or the cell-order index on the other
       steps, weighted by how often they occur);
-    deposit: read positions once, write the mesh once (binary64 cells; the
-      precision form writes FP32 offsets, its int64 accumulators live in
-      shared memory);
-    fft_forward / green / fft_inverse: the five-pass transform on a power-of-two
-      mesh, each pass reading and writing its array once -- z r2c (mesh in,
-      half spectrum out) + y pass (half spectrum in and out); x pass with the
-      Green's multiply (in and out); y pass + z c2r (half spectrum in, mesh out);
+    deposit: read positions once, write the half spectrum once (each finished
+      shared-memory tile of cells is transformed along z before it is
+      written, so the r2c along z is part of this launch; int64 / fixed-point
+      accumulators never reach HBM);
+    fft_forward / green / fft_inverse: the rest of the five-pass transform on a
+      power-of-two mesh, each pass reading and writing its array once -- y pass
+      (half spectrum in and out); x pass with the Green's multiply (in and
+      out); y pass + z c2r (half spectrum in, mesh out);
     gather: read x, p and the potential once; write a and p.
     """
     G = N ** 3
     H = N * N * (N // 2 + 1)
     if form == "fp64":
         bx = bp = b = 8
-        dep = n * 3 * bx + G * 8
     else:
         bx = bp = b = 4
-        dep = n * 3 * bx + G * 4
     cplx = H * 2 * b
+    dep = n * 3 * bx + cplx
     gather = n * (3 * bx + 3 * bp + 3 * bp + 3 * bp) + G * b
     kick = n * (3 * bx + 3 * bp + 3 * bp + 3 * bx + 3 * bp + 8)
     kick += sort_fraction * n * 2 * (3 * bx + 3 * bp + 4 + 8)
     kick += (1.0 - sort_fraction) * n * (4 + 4 + 4)   # cell order: key, rank in; order out
-    return {"sort": kick, "deposit": dep, "fft_forward": G * b + cplx + 2 * cplx,
+    return {"sort": kick, "deposit": dep, "fft_forward": 2 * cplx,
             "green": 2 * cplx, "fft_inverse": 2 * cplx + cplx + G * b, "gather": gather}
 
 
@@ -256,10 +256,10 @@ def phase_bytes(form, n, N, sort_fraction):
 # 1/8 of the particles and mesh cells) times 8; each kernel's traffic scales
 # with the particles and cells it processes.
 TRAFFIC_C3 = {
-    ("fp32", "deposit"): 8 * (273 + 484) * 1e6,
-    ("fp32", "green"): 8 * (554 + 499) * 1e6,
+    ("fp32", "deposit"): 8 * (285 + 492) * 1e6,
+    ("fp32", "green"): 8 * (554 + 503) * 1e6,
     ("fp32", "gather"): 8 * (942 + 383) * 1e6,
-    ("fp64", "deposit"): 8 * (1466 + 996) * 1e6,
+    ("fp64", "deposit"): 8 * (487 + 1030) * 1e6,
     ("fp64", "green"): 8 * (1091 + 1034) * 1e6,
     ("fp64", "gather"): 8 * (1885 + 789) * 1e6,
 }
@@ -696,7 +696,7 @@ def main():
                         "frac": ach / hbm}
     single = [k for k in ("deposit", "green", "gather") if k in table]
     dom = max(single, key=lambda k: table[k]["avg_ms"])
-    kernel_name = {"deposit": "deposit", "green": "x pass + Green's multiply",
+    kernel_name = {"deposit": "deposit + r2c along z", "green": "x pass + Green's multiply",
                    "gather": "gather + K2"}[dom]
     traffic = TRAFFIC_C3.get((args.form, dom)) if args.config == "c3" else None
     roofline = {"bound": "hbm", "kernel": kernel_name, "phase": dom,

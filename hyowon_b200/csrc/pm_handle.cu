@@ -133,6 +133,7 @@ struct hyowon_pm_s {
     hyowon_treepm_params tp{};
     double* tree_buf = nullptr;       // 6 n doubles: widened positions, short-range output
     uint32_t tree_cap = 0;
+    tree::Workspace* tree_ws = nullptr;   // octree build and walk scratch, kept between solves
 
     bool timing = false;
     cudaEvent_t ev[8] = {};
@@ -518,7 +519,17 @@ struct CallTimer {
     }
 };
 
+int ensure_tree_workspace(hyowon_pm_t h) {
+    if (!h->tree_ws) {
+        h->tree_ws = tree::create_workspace();
+        if (!h->tree_ws) return fail(h, HYOWON_ENOMEM, "out of host memory");
+    }
+    return HYOWON_OK;
+}
+
 int ensure_tree_buffer(hyowon_pm_t h) {
+    const int rc = ensure_tree_workspace(h);
+    if (rc) return rc;
     if (h->tree_buf && h->tree_cap >= h->n) return HYOWON_OK;
     cudaFree(h->tree_buf);
     h->tree_buf = nullptr;
@@ -536,12 +547,14 @@ int add_short_range_f64(hyowon_pm_t h, int pset) {
     int rc = read_status(h, &st);
     if (rc) return rc;
     if (st) return HYOWON_OK;   // the status decides the outcome; K2 is gated on it
+    rc = ensure_tree_workspace(h);
+    if (rc) return rc;
     std::string err;
     hyowon_treepm_params P = h->tp;
     P.particle_mass = h->uniform_mass > 0.0 ? h->uniform_mass : 1.0;  // masses win when present
     rc = tree::device_short_forces(P, h->n, h->pos[pset][0], h->pos[pset][1], h->pos[pset][2],
                                    h->has_masses ? h->mass[h->ic] : nullptr, h->acc[0], h->acc[1],
-                                   h->acc[2], h->stream, nullptr, &err);
+                                   h->acc[2], h->stream, nullptr, &err, h->tree_ws);
     return rc ? fail(h, rc, "TreePM short range: " + err) : HYOWON_OK;
 }
 
@@ -564,7 +577,7 @@ int short_range_hook_f32(void* ctx, cudaStream_t s, int P) {
     hyowon_treepm_params Pm = h->tp;
     Pm.particle_mass = h->uniform_mass;
     rc = tree::device_short_forces(Pm, h->n, px, px + n, px + 2 * n, nullptr, out, out + n,
-                                   out + 2 * n, s, nullptr, &err);
+                                   out + 2 * n, s, nullptr, &err, h->tree_ws);
     if (rc) return fail(h, rc, "TreePM short range: " + err);
     return status_or_cuda(h, fp32::add_accelerations(h->f32, s, out, out + n, out + 2 * n));
 }
@@ -888,6 +901,7 @@ int hyowon_pm_destroy(hyowon_pm_t h) {
     cudaFree(h->win);
     free_particles(h);
     cudaFree(h->tree_buf);
+    hyowon::tree::destroy_workspace(h->tree_ws);
     cudaFree(h->sort.count);
     cudaFree(h->sort.offset);
     cudaFree(h->sort.scan_tmp);
@@ -1497,7 +1511,7 @@ int hyowon_pm_treepm_short_forces(hyowon_pm_t h, double theta, double softening,
     CK(cudaMemsetAsync(out, 0, sizeof(double) * 3 * n, h->stream));
     std::string err;
     rc = tree::device_short_forces(P, h->n, x, y, z, masses, out, out + n, out + 2 * n, h->stream,
-                                   stats, &err);
+                                   stats, &err, h->tree_ws);
     if (rc) return fail(h, rc, "TreePM short range: " + err);
     double* host[3] = {ax, ay, az};
     for (int a = 0; a < 3; ++a) {

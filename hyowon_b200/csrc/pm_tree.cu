@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -531,16 +532,57 @@ struct Fail {
                                           std::string(#call) + ": " + cudaGetErrorString(e_)}; \
     } while (0)
 
+}  // namespace
+
+// Device scratch kept between calls: one block that the buffers of a call are
+// carved from (256-byte aligned), so that repeated solves allocate nothing.
+// A call that needs more than it holds takes the rest from cudaMalloc and
+// records the total, and the next call regrows the block to that size.
+struct Workspace {
+    void* base = nullptr;
+    size_t cap = 0;
+    size_t want = 0;
+};
+
+Workspace* create_workspace() { return new (std::nothrow) Workspace(); }
+
+void destroy_workspace(Workspace* ws) {
+    if (!ws) return;
+    if (ws->base) cudaFree(ws->base);
+    delete ws;
+}
+
+namespace {
+
 struct Mem {
-    std::vector<void*> p;
+    Workspace* ws;
+    size_t off = 0;
+    std::vector<void*> p;   // buffers beyond the workspace, freed with this
+    explicit Mem(Workspace* w = nullptr) : ws(w) {
+        if (ws && ws->want > ws->cap) {
+            // the previous call finished its work before returning
+            if (ws->base) cudaFree(ws->base);
+            ws->base = nullptr;
+            ws->cap = 0;
+            TCK(cudaMalloc(&ws->base, ws->want));
+            ws->cap = ws->want;
+        }
+    }
     template <typename T>
     T* get(size_t count) {
+        const size_t bytes = (((count ? count : 1) * sizeof(T)) + 255) & ~static_cast<size_t>(255);
+        if (ws) {
+            const size_t at = off;
+            off += bytes;
+            if (off <= ws->cap) return reinterpret_cast<T*>(static_cast<char*>(ws->base) + at);
+        }
         void* q = nullptr;
-        TCK(cudaMalloc(&q, (count ? count : 1) * sizeof(T)));
+        TCK(cudaMalloc(&q, bytes));
         p.push_back(q);
         return static_cast<T*>(q);
     }
     ~Mem() {
+        if (ws && off > ws->want) ws->want = off;
         for (void* q : p) cudaFree(q);
     }
 };
@@ -578,8 +620,9 @@ thread_local std::string g_err;
 // s; the call returns after it has finished.
 int run(const hyowon_treepm_params& P, uint32_t n, const double* x, const double* y,
         const double* z, const double* masses, const uint32_t* host_targets, uint32_t nt,
-        double* ax, double* ay, double* az, cudaStream_t s, double* stats) {
-    Mem mem;
+        double* ax, double* ay, double* az, cudaStream_t s, double* stats,
+        Workspace* ws = nullptr) {
+    Mem mem(ws);
     struct Events {
         cudaEvent_t e[4] = {};
         Events() { for (auto& v : e) cudaEventCreate(&v); }
@@ -776,9 +819,10 @@ int short_forces(const hyowon_treepm_params& P, uint32_t n, const double* hx, co
 
 int device_short_forces(const hyowon_treepm_params& P, uint32_t n, const double* x,
                         const double* y, const double* z, const double* masses, double* ax,
-                        double* ay, double* az, cudaStream_t s, double* stats, std::string* err) {
+                        double* ay, double* az, cudaStream_t s, double* stats, std::string* err,
+                        Workspace* ws) {
     try {
-        return run(P, n, x, y, z, masses, nullptr, n, ax, ay, az, s, stats);
+        return run(P, n, x, y, z, masses, nullptr, n, ax, ay, az, s, stats, ws);
     } catch (const Fail& f) {
         if (err) *err = f.msg;
         return f.code;
