@@ -753,6 +753,9 @@ def main():
         v2 = whole_job_rate(world, n, args.steps, dev2)
         compare = {"form": other, "value": v2, "ms_per_step": dev2 / args.steps,
                    "ratio_fp32_over_fp64": (value / v2) if args.form == "fp32" else (v2 / value),
+                   "phases_ms_avg": {k: t2[k] / max(1.0, t2["solves"])
+                                     for k in ("sort", "deposit", "fft_forward", "green",
+                                               "fft_inverse", "gather")},
                    "e2e": e2e2}
 
     # -- the precision form's force error at the state the binary64 run reached

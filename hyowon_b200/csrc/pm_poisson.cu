@@ -120,6 +120,14 @@ template <typename T, int LOG2N> struct Geo : chunked::Layout<T, LOG2N> {
     static constexpr size_t smem_cb = static_cast<size_t>(nbuf_b) * tile_bytes_b;
     static constexpr int units_b = CB * static_cast<int>(sizeof(C)) / 8;  // 8-byte units per part row
     static constexpr int units = CC * static_cast<int>(sizeof(C)) / 8;  // 8-byte units per row
+    // column-pass blocks per SM the registers are sized for: FP32 blocks of
+    // fewer than 512 threads (N <= 512) get several per SM, as many as make
+    // 512 threads and their shared memory allows (at N = 512: 2, at most 128
+    // registers, where the compiler would take 180 and fit one)
+    static constexpr int smem_blocks = static_cast<int>((227u * 1024u) / smem_cb);
+    static constexpr int minb_want = sizeof(T) == 4 ? (512 / TCB > HYOWON_FFT_MINB_C32 ? 512 / TCB : HYOWON_FFT_MINB_C32)
+                                                    : HYOWON_FFT_MINB_C64;
+    static constexpr int minb_c = SP * (minb_want < smem_blocks ? minb_want : (smem_blocks > 0 ? smem_blocks : 1));
 };
 
 template <typename S> struct Raw;   // raw row pair of the z forward input
@@ -360,7 +368,7 @@ constexpr unsigned kWaitLimit = 1u << 24;
 // `green` applied to the untransformed tile, then one transform (SIGN).
 template <typename T, int LOG2N, int AXIS, int SIGN, int MODE, typename GF>
 __global__ void __launch_bounds__(Geo<T, LOG2N>::TCB,
-                                  Geo<T, LOG2N>::SP * (sizeof(T) == 4 ? HYOWON_FFT_MINB_C32 : HYOWON_FFT_MINB_C64))
+                                  Geo<T, LOG2N>::minb_c)
 k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
           const cx_t<T>* __restrict__ tw, GF green, unsigned int* status, unsigned wait_limit) {
     using G = Geo<T, LOG2N>;
