@@ -565,6 +565,14 @@ k_gather_kick(uint32_t n, const float* __restrict__ phi, const uint32_t* __restr
               unsigned int* status) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || (*status & ST_BLOCKS_PUBLISH)) return;
+    // the momenta load while the stencil does (2.96 -> 2.60 ms at 512^3 / 1024^3;
+    // the binary64 gather, at 48 registers with spills, was slower so)
+    float p0[3] = {0.f, 0.f, 0.f};
+    if (do_kick) {
+        p0[0] = px[i];
+        p0[1] = py[i];
+        p0[2] = pz[i];
+    }
     uint32_t fx, fy, fz;
     const int ix = static_cast<int>(cell_of(ux[i], N, fx));
     const int iy = static_cast<int>(cell_of(uy[i], N, fy));
@@ -622,9 +630,9 @@ k_gather_kick(uint32_t n, const float* __restrict__ phi, const uint32_t* __restr
     ay[i] = gy;
     az[i] = gz;
     if (do_kick) {
-        const float qx = fmaf(gx, K2, px[i]);
-        const float qy = fmaf(gy, K2, py[i]);
-        const float qz = fmaf(gz, K2, pz[i]);
+        const float qx = fmaf(gx, K2, p0[0]);
+        const float qy = fmaf(gy, K2, p0[1]);
+        const float qz = fmaf(gz, K2, p0[2]);
         if (!(isfinite(qx) && isfinite(qy) && isfinite(qz))) raise_status(status, ST_KICK2);
         pxo[i] = qx;
         pyo[i] = qy;
