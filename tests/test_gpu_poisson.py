@@ -1,9 +1,10 @@
-"""The five-pass potential solve (pm_poisson.cu: z r2c + y transforms, x
-transform with the Green's multiply, inverse y + z c2r) on power-of-two
-meshes, against the oracle's potential (its own FFT, pinned to the
-reference), for every radix layout the passes use (N = 32 .. 512 covers a
-final radix of 2, 4, 8 and 16 and one to three stages in both the row and the
-column transforms); at N = 1024 against a plain torch binary64 spectral
+"""The five-pass potential solve (the deposit's r2c along z of each finished
+tile, pm_chunk.cuh; pm_poisson.cu: y transforms, x transform with the Green's
+multiply, inverse y + z c2r) on power-of-two meshes, against the oracle's
+potential (its own FFT, pinned to the reference), for every radix layout the
+passes use (N = 32 .. 512 covers a final radix of 2, 4, 8 and 16, one to three
+stages in the row and column transforms, and deposit tiles of 128 down to 8
+rows); at N = 1024 against a plain torch binary64 spectral
 solve (torch.fft.rfftn / irfftn of the downloaded mass mesh with the same
 discrete-Laplacian Green's function).
 
