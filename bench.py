@@ -699,7 +699,16 @@ def main():
     kernel_name = {"deposit": "deposit + r2c along z", "green": "x pass + Green's multiply",
                    "gather": "gather + K2"}[dom]
     traffic = TRAFFIC_C3.get((args.form, dom)) if args.config == "c3" else None
-    roofline = {"bound": "hbm", "kernel": kernel_name, "phase": dom,
+    bound_note = {
+        "deposit": "the kernel is bound by shared memory (fixed-point atomics, tile zeroing and "
+                   "the r2c along z of each finished tile; 83% of the shared pipe's cycles in the "
+                   "ncu capture of the half-size workload), not HBM: its HBM bytes are the "
+                   "positions read and the half spectrum written once",
+        "green": "two transforms per tile (forward x, Green's multiply, inverse x), issue- and "
+                 "occupancy-bound",
+        "gather": "latency of the 32 stencil loads per particle",
+    }[dom]
+    roofline = {"bound": "hbm", "kernel": kernel_name, "phase": dom, "note": bound_note,
                 "achieved": table[dom]["achieved_GBs"], "peak": hbm, "unit": "GB/s",
                 "frac": table[dom]["frac"], "traffic": traffic,
                 "traffic_source": "ncu capture of the half-size c3 workload x 8" if traffic else None,
