@@ -51,8 +51,11 @@ template <typename T, int LOG2N> struct Layout {
 // transform of row r's N reals read as N/2 complex values), into
 // X[k] = E[k] + W_N^k O[k] with E/O the transforms of the even/odd samples,
 // for k = 0..N/2, and stores them to the chunked spectrum H at rows
-// (x, y0 .. y0+R-1). All `nthreads` threads take part.
-template <typename T, int LOG2N, int R, int S>
+// (x, y0 .. y0+R-1). All `nthreads` threads take part. Consecutive threads
+// take consecutive kz of a chunk row (ROW_FAST false: 64-byte runs of H per
+// row) or consecutive rows of one kz (ROW_FAST true: for dense rows, S = R,
+// whose shared-memory reads are then one contiguous block per warp).
+template <typename T, int LOG2N, int R, int S, bool ROW_FAST = false>
 __device__ __forceinline__ void rows_unpack(const cx_t<T>* sm, const cx_t<T>* __restrict__ tw,
                                             cx_t<T>* __restrict__ H, int x, int y0, int tid,
                                             int nthreads) {
@@ -61,8 +64,8 @@ __device__ __forceinline__ void rows_unpack(const cx_t<T>* sm, const cx_t<T>* __
     const T half = static_cast<T>(0.5);
     constexpr int KP = (L::K + L::CC - 1) / L::CC;   // chunks covering k = 0..M/2
     for (int e = tid; e < KP * R * L::CC; e += nthreads) {
-        const int ki = e % L::CC;
-        const int r = (e / L::CC) % R;
+        const int ki = ROW_FAST ? (e / R) % L::CC : e % L::CC;
+        const int r = ROW_FAST ? e % R : (e / L::CC) % R;
         const int k = (e / (L::CC * R)) * L::CC + ki;
         if (k >= L::K) continue;
         const C zk = sm[k * S + r];
@@ -155,7 +158,7 @@ __device__ __forceinline__ void tile_r2c(PAIR pair, cx_t<T>* sm, const cx_t<T>* 
         fft::smem_stage<LOG2M, (1 << rem), -1, TY, S, E, true, false, MASK>(sm, Ns, tw, L::N, c, j,
                                                                            active);
     }
-    rows_unpack<T, LOG2N, TY, S>(sm, tw, H, x, y0, tid, nthreads);
+    rows_unpack<T, LOG2N, TY, S, true>(sm, tw, H, x, y0, tid, nthreads);
 }
 
 }  // namespace chunked
