@@ -701,7 +701,7 @@ def main():
     traffic = TRAFFIC_C3.get((args.form, dom)) if args.config == "c3" else None
     bound_note = {
         "deposit": "the kernel is bound by shared memory (fixed-point atomics, tile zeroing and "
-                   "the r2c along z of each finished tile; 83% of the shared pipe's cycles in the "
+                   "the r2c along z of each finished tile; 78% of the shared pipe's cycles in the "
                    "ncu capture of the half-size workload), not HBM: its HBM bytes are the "
                    "positions read and the half spectrum written once",
         "green": "two transforms per tile (forward x, Green's multiply, inverse x), issue- and "
