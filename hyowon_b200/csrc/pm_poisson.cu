@@ -59,6 +59,9 @@ using fft::mk;
 #ifndef HYOWON_FFT_MINB_Z
 #define HYOWON_FFT_MINB_Z 2
 #endif
+#ifndef HYOWON_FFT_NBUF64
+#define HYOWON_FFT_NBUF64 2
+#endif
 #ifndef HYOWON_FFT_NBUF
 #define HYOWON_FFT_NBUF 2
 #endif
@@ -116,7 +119,8 @@ template <typename T, int LOG2N> struct Geo : chunked::Layout<T, LOG2N> {
     static constexpr int EC = HYOWON_FFT_EPT == 8 ? 8 : 16;  // elements per thread
     static constexpr int TCB = CB * N / EC;                       // threads of a column block
     static constexpr unsigned tile_bytes_b = sizeof(C) * N * CB;  // one block's part of a tile
-    static constexpr int nbuf_b = (HYOWON_FFT_NBUF * tile_bytes_b <= 200u * 1024u) ? HYOWON_FFT_NBUF : 2;
+    static constexpr int nbuf_want = sizeof(T) == 4 ? HYOWON_FFT_NBUF : HYOWON_FFT_NBUF64;
+    static constexpr int nbuf_b = (nbuf_want * tile_bytes_b <= 200u * 1024u) ? nbuf_want : 2;
     static constexpr size_t smem_cb = static_cast<size_t>(nbuf_b) * tile_bytes_b;
     static constexpr int units_b = CB * static_cast<int>(sizeof(C)) / 8;  // 8-byte units per part row
     static constexpr int units = CC * static_cast<int>(sizeof(C)) / 8;  // 8-byte units per row
@@ -128,6 +132,31 @@ template <typename T, int LOG2N> struct Geo : chunked::Layout<T, LOG2N> {
     static constexpr int minb_want = sizeof(T) == 4 ? (512 / TCB > HYOWON_FFT_MINB_C32 ? 512 / TCB : HYOWON_FFT_MINB_C32)
                                                     : HYOWON_FFT_MINB_C64;
     static constexpr int minb_c = SP * (minb_want < smem_blocks ? minb_want : (smem_blocks > 0 ? smem_blocks : 1));
+};
+
+// Buffers and blocks per SM of a column pass. The x pass (MODE 1: two
+// transforms and the Green's multiply per tile) holds one tile buffer per
+// block and runs two (N >= 1024) or three blocks per SM: more warps hide its
+// latency better than the second buffer's prefetch (c3: binary64 7.37 -> 6.31
+// ms, FP32 3.32 -> 3.11 ms; 512^3: 0.82 -> 0.75 and 0.378 -> 0.364 ms), while
+// the y passes keep two buffers and one block, which measured faster for them.
+// HYOWON_FFT_X64_NBUF / HYOWON_FFT_X32_NBUF = 2 give the x pass the y passes'
+// configuration.
+#ifndef HYOWON_FFT_X64_NBUF
+#define HYOWON_FFT_X64_NBUF 1
+#endif
+#ifndef HYOWON_FFT_X32_NBUF
+#define HYOWON_FFT_X32_NBUF 1
+#endif
+template <typename T, int LOG2N, int MODE> struct ColumnCfg {
+    using G = Geo<T, LOG2N>;
+    static constexpr bool x64 = MODE == 1 && (sizeof(T) == 8 ? HYOWON_FFT_X64_NBUF == 1
+                                                               : HYOWON_FFT_X32_NBUF == 1);
+    static constexpr int nbuf = x64 ? 1 : G::nbuf_b;
+    static constexpr size_t smem = static_cast<size_t>(nbuf) * G::tile_bytes_b;
+    static constexpr int smem_blocks = static_cast<int>((227u * 1024u) / smem);
+    static constexpr int want = LOG2N >= 10 ? 2 : 3;
+    static constexpr int minb = x64 ? G::SP * (want < smem_blocks ? want : smem_blocks) : G::minb_c;
 };
 
 template <typename S> struct Raw;   // raw row pair of the z forward input
@@ -367,8 +396,7 @@ constexpr unsigned kWaitLimit = 1u << 24;
 // inverse transform (the x pass of the potential solve); 2: the symbol
 // `green` applied to the untransformed tile, then one transform (SIGN).
 template <typename T, int LOG2N, int AXIS, int SIGN, int MODE, typename GF>
-__global__ void __launch_bounds__(Geo<T, LOG2N>::TCB,
-                                  Geo<T, LOG2N>::minb_c)
+__global__ void __launch_bounds__(Geo<T, LOG2N>::TCB, (ColumnCfg<T, LOG2N, MODE>::minb))
 k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
           const cx_t<T>* __restrict__ tw, GF green, unsigned int* status, unsigned wait_limit) {
     using G = Geo<T, LOG2N>;
@@ -377,7 +405,7 @@ k_columns(const __grid_constant__ CUtensorMap map, cx_t<T>* __restrict__ H,
     constexpr int P = G::N / EC;
     constexpr int CB = G::CB;     // columns of this block's part of a tile
     constexpr int S = CB;
-    constexpr int NB = G::nbuf_b;
+    constexpr int NB = ColumnCfg<T, LOG2N, MODE>::nbuf;
     constexpr size_t axis_stride = AXIS == 1 ? static_cast<size_t>(G::CC)
                                              : static_cast<size_t>(G::N) * G::CC;
     constexpr size_t seq_stride = AXIS == 1 ? static_cast<size_t>(G::N) * G::CC
@@ -557,17 +585,18 @@ int columns(const Plan* p, cx_t<T>* H, const cx_t<T>* tw, GF green, unsigned int
     using G = Geo<T, LOG2N>;
     if (!p || p->N != G::N) return -1;
     auto kernel = k_columns<T, LOG2N, AXIS, SIGN, MODE, GF>;
-    if (!prepare(kernel, G::smem_cb)) return -1;
+    constexpr size_t smem = ColumnCfg<T, LOG2N, MODE>::smem;
+    if (!prepare(kernel, smem)) return -1;
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess
         || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess
-        || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, G::TCB, G::smem_cb) != cudaSuccess
+        || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, G::TCB, smem) != cudaSuccess
         || per_sm < 1)
         return -1;
     const unsigned tiles = static_cast<unsigned>(G::KC) * G::N * G::SP;
     const unsigned full = static_cast<unsigned>(sms) * static_cast<unsigned>(per_sm);
     const unsigned grid = tiles < full ? tiles : full;
-    kernel<<<grid, G::TCB, G::smem_cb, s>>>(AXIS == 1 ? p->y : p->x, H, tw, green, status,
+    kernel<<<grid, G::TCB, smem, s>>>(AXIS == 1 ? p->y : p->x, H, tw, green, status,
                                           p->wait_limit);
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
