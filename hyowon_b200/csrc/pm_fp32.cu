@@ -411,6 +411,8 @@ k_deposit_tiles(const uint32_t* __restrict__ ux, const uint32_t* __restrict__ uy
         // each cell pair is read once, by the transform's first stage
         using Lz = chunked::Layout<float, ZLOG>;
         constexpr int TYc = deposit_rows(Lz::N);
+        static_assert(TYc * (Lz::M / 8) <= kDepositThreads,
+                      "the tile's z transform needs a thread per 8 values of a row set");
         const ulonglong2* q2 = reinterpret_cast<const ulonglong2*>(qtile);
         unsigned long long local = 0;
         auto pair = [&](int r, int k) {

@@ -223,6 +223,12 @@ constexpr int kOneWordMinW = 55;
 // W >= 31 (a bucket of fewer than 2^29 particles); beyond that the deposit
 // reports ST_CAPACITY.
 constexpr int kTwoWordMinW = 31;
+// Blocks per SM the deposit tiles' registers are sized for: five (48 registers,
+// spilling a little to L1) measured faster than four (64) and three (8.7-8.8 ms
+// against 8.9-9.0 and 10.4 at 512^3 / 1024^3).
+#ifndef HYOWON_DEPOSIT64_MINB
+#define HYOWON_DEPOSIT64_MINB 5
+#endif
 // Particles each thread loads ahead per pass of the tile loop.
 #ifndef HYOWON_DEPOSIT64_BATCH
 #define HYOWON_DEPOSIT64_BATCH 2
@@ -262,7 +268,7 @@ __device__ __forceinline__ double fixed_to_double(unsigned long long hi, unsigne
 // transformed along z in shared memory (chunked::tile_r2c) and stored to the
 // chunked half spectrum H instead of the real mesh.
 template <int kDepositWords, int ZLOG>
-__global__ void __launch_bounds__(kTileThreads, 4)
+__global__ void __launch_bounds__(kTileThreads, HYOWON_DEPOSIT64_MINB)
 k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
                 const double* __restrict__ z, const double* __restrict__ mass,
                 double uniform_mass, const uint32_t* __restrict__ order,
@@ -398,6 +404,8 @@ k_deposit_tiles(const double* __restrict__ x, const double* __restrict__ y,
         // each cell pair is read once, by the transform's first stage
         using Lz = chunked::Layout<double, ZLOG>;
         constexpr int TYc = tile_rows_f64(Lz::N, kDepositWords);
+        static_assert(TYc * (Lz::M / 8) <= kTileThreads,
+                      "the tile's z transform needs a thread per 8 values of a row set");
         const double from_fixed = ldexp(1.0, kDepositWords == 1 ? e_max + 1 - W : e_max - 62);
         const ulonglong2* lo2 = reinterpret_cast<const ulonglong2*>(acc_lo);
         const ulonglong2* hi2 = reinterpret_cast<const ulonglong2*>(acc_hi);
