@@ -150,13 +150,14 @@ template <typename T, int LOG2N> struct Geo : chunked::Layout<T, LOG2N> {
 #endif
 template <typename T, int LOG2N, int MODE> struct ColumnCfg {
     using G = Geo<T, LOG2N>;
-    static constexpr bool x64 = MODE == 1 && (sizeof(T) == 8 ? HYOWON_FFT_X64_NBUF == 1
-                                                               : HYOWON_FFT_X32_NBUF == 1);
-    static constexpr int nbuf = x64 ? 1 : G::nbuf_b;
+    static constexpr bool single_buffer =
+        MODE == 1 && (sizeof(T) == 8 ? HYOWON_FFT_X64_NBUF == 1 : HYOWON_FFT_X32_NBUF == 1);
+    static constexpr int nbuf = single_buffer ? 1 : G::nbuf_b;
     static constexpr size_t smem = static_cast<size_t>(nbuf) * G::tile_bytes_b;
     static constexpr int smem_blocks = static_cast<int>((227u * 1024u) / smem);
     static constexpr int want = LOG2N >= 10 ? 2 : 3;
-    static constexpr int minb = x64 ? G::SP * (want < smem_blocks ? want : smem_blocks) : G::minb_c;
+    static constexpr int minb =
+        single_buffer ? G::SP * (want < smem_blocks ? want : smem_blocks) : G::minb_c;
 };
 
 template <typename S> struct Raw;   // raw row pair of the z forward input
