@@ -468,6 +468,14 @@ k_walk(uint32_t n_targets, const uint32_t* __restrict__ tslot, const double* __r
             ay[o] = static_cast<double>(fy);
             az[o] = static_cast<double>(fz);
         }
+    }
+    // walk statistics: one atomic per warp (every lane of the warp leaves the
+    // walk loop together)
+    for (int o = 16; o > 0; o >>= 1) {
+        visits += __shfl_down_sync(0xffffffffu, visits, o);
+        pairs += __shfl_down_sync(0xffffffffu, pairs, o);
+    }
+    if (lane == 0) {
         atomicAdd(&counters[0], visits);
         atomicAdd(&counters[1], pairs);
     }
