@@ -54,6 +54,7 @@ struct Node {
     uint32_t start, end;           // sorted source range
     uint32_t first_child, n_child; // children in the node array
     uint32_t level, leaf;
+    double open2;                  // (2 half / theta + |COM - centre|_1)^2, set after the build
 };
 
 __device__ __forceinline__ unsigned long long spread3(unsigned v) {
@@ -333,6 +334,19 @@ struct WalkParams {
     double L, r_cut, eps, theta, r_s, G, m;
 };
 
+// The monopole criterion's target-independent side, once per node: a node is
+// accepted when its COM distance squared exceeds (2 half / theta + off)^2
+// with off the L1 offset of the COM from the cube centre (the expression the
+// walk would otherwise evaluate at every visit, in the same operations).
+__global__ void k_open_radius(uint32_t n_nodes, double theta, Node* __restrict__ nodes) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_nodes) return;
+    Node& nd = nodes[i];
+    const double off = fabs(nd.mx - nd.cx) + fabs(nd.my - nd.cy) + fabs(nd.mz - nd.cz);
+    const double need = 2.0 * nd.half / theta + off;
+    nd.open2 = need * need;
+}
+
 // Targets: sorted slots tslot[t] (null: target t is sorted slot t, every
 // source). Output of target t goes to index out_idx[t] (null: t), written, or
 // added to what is there when `add`. Source masses: sorted sm[] (null: P.m).
@@ -422,9 +436,7 @@ k_walk(uint32_t n_targets, const uint32_t* __restrict__ tslot, const double* __r
                     dy = min_image(nd.my - ty, P.L);
                     dz = min_image(nd.mz - tz, P.L);
                     r2 = dx * dx + dy * dy + dz * dz;
-                    const double off = fabs(nd.mx - nd.cx) + fabs(nd.my - nd.cy) + fabs(nd.mz - nd.cz);
-                    const double need = 2.0 * nd.half / P.theta + off;
-                    accept = r2 > need * need;
+                    accept = r2 > nd.open2;
                 }
                 if (accept) {
                     const R f = short_factor_impl<R>(static_cast<R>(r2), eps2, inv_rs, inv_rs3)
@@ -729,6 +741,7 @@ int run(const hyowon_treepm_params& P, uint32_t n, const double* x, const double
             k_moments<<<nb(e - b), kT, 0, s>>>(b, e, sx, sy, sz, sm, nodes);
         }
     }
+    if (node_base) k_open_radius<<<nb(node_base), kT, 0, s>>>(node_base, P.theta, nodes);
     cudaEventRecord(ev.e[1], s);
     const uint32_t* dslots = nullptr;
     const uint32_t* out_idx = nullptr;
