@@ -28,6 +28,8 @@ particles, L = 256 Mpc/h, 256^3 mesh, r_s = 1.25 cells, r_cut = 4.5 r_s,
 opening angle 0.5, softening 1/30 of the mean spacing, the clustered z = 0
 state of a 64-step PM run of seed 5): a "step" is one KDK step with the TreePM
 force (long range plus the octree short range of every particle).
+`--treepm-side S` scales it to S^3 particles, L = S Mpc/h and an S^3 mesh (the
+same density and cell size) for kernel profiles of a smaller case.
 
 `--workload cufft` times cuFFT (through torch.fft) on the data of the c3
 potential solve, for comparison with the five-pass transforms: 1-D transforms
@@ -86,6 +88,10 @@ def parse():
     ap.add_argument("--no-side-workloads", action="store_true",
                     help="skip the adjoint (c4) and TreePM (c5) measurements the default step "
                          "line carries")
+    ap.add_argument("--treepm-side", type=int, default=256,
+                    help="particles per side of the TreePM workload; box (Mpc/h) and mesh scale "
+                         "with it, so 128 is c5 at 1/8 of its particles and volume (for kernel "
+                         "profiles)")
     return ap.parse_args()
 
 
@@ -515,7 +521,8 @@ def run_treepm(args, rank, emit=True):
         return None
     import hyowon_b200 as hb
     from hyowon_b200 import ic
-    n_side, L, N, seed = 256, 256.0, 256, 5
+    n_side = args.treepm_side
+    L, N, seed = float(n_side), n_side, 5
     a0 = 1.0 / 50.0
     K1, D, K2 = hb.TimeStepper(a0, 1.0, math.log(1.0 / a0) / 64).factors()
     m = ic.particle_mass(L, n_side)
@@ -556,7 +563,7 @@ def run_treepm(args, rank, emit=True):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["fp64"]["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"c5 TreePM KDK: {n_side}^3 particles, {N}^3 mesh, L = {L}, "
+        "config": {"workload": f"{'c5' if n_side == 256 else 'c5-shaped'} TreePM KDK: {n_side}^3 particles, {N}^3 mesh, L = {L}, "
                                f"r_s = 1.25 cells, r_cut = 4.5 r_s, theta = 0.5, eps = L/{n_side}/30, "
                                "clustered z = 0 state of a 64-step PM run", "seed": seed,
                    "l2": "particle arrays and meshes >> 126 MB"},
