@@ -350,11 +350,24 @@ __global__ void k_open_radius(uint32_t n_nodes, double theta, Node* __restrict__
 // Targets: sorted slots tslot[t] (null: target t is sorted slot t, every
 // source). Output of target t goes to index out_idx[t] (null: t), written, or
 // added to what is there when `add`. Source masses: sorted sm[] (null: P.m).
-#ifndef HYOWON_WALK_MINB
-#define HYOWON_WALK_MINB 1
+//
+// Blocks per SM the registers are sized for. The binary64 walk waits mostly on
+// the FP64 pipe's fixed latencies, which more warps hide: eight 128-thread
+// blocks (64 registers, 52 bytes of spill) against the compiler's five (88
+// registers) took the c5 walk from 1444 to 1283 ms. The FP32 walk measured
+// 863 ms at the compiler's 71 registers (seven blocks), 874 at eight blocks and
+// 879 at six, so it keeps its own choice.
+#ifndef HYOWON_WALK_MINB64
+#define HYOWON_WALK_MINB64 8
 #endif
+#ifndef HYOWON_WALK_MINB32
+#define HYOWON_WALK_MINB32 1
+#endif
+template <typename R> struct WalkBlocks {
+    static constexpr int minb = sizeof(R) == 8 ? HYOWON_WALK_MINB64 : HYOWON_WALK_MINB32;
+};
 template <typename R>
-__global__ void __launch_bounds__(128, HYOWON_WALK_MINB)
+__global__ void __launch_bounds__(128, WalkBlocks<R>::minb)
 k_walk(uint32_t n_targets, const uint32_t* __restrict__ tslot, const double* __restrict__ sx,
        const double* __restrict__ sy, const double* __restrict__ sz,
        const double* __restrict__ sm, const unsigned long long* __restrict__ skey,
