@@ -798,7 +798,7 @@ def main():
     # the metric's other two figures, on their own configurations (1 GPU)
     side = {}
     if rank == 0 and world == 1 and not args.no_side_workloads:
-        side_args = argparse.Namespace(steps=3, warmup=1)
+        side_args = argparse.Namespace(steps=3, warmup=1, treepm_side=256)
         for name, fn in (("adjoint", run_adjoint), ("treepm", run_treepm)):
             try:
                 side[name] = fn(side_args, 0, emit=False)
