@@ -92,7 +92,10 @@ def parse():
                     help="particles per side of the TreePM workload; box (Mpc/h) and mesh scale "
                          "with it, so 128 is c5 at 1/8 of its particles and volume (for kernel "
                          "profiles)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.treepm_side < 32 or args.treepm_side & (args.treepm_side - 1):
+        ap.error("--treepm-side must be a power of two of at least 32")
+    return args
 
 
 def peaks():
